@@ -1,0 +1,153 @@
+/*
+ * matops_b200.h -- C ABI of the B200 (sm_100a) implementation of hrautila/matops's
+ * level-3 hot path: GEMM, SYRK and TRSM, and the blocked Cholesky / LU factorizations and
+ * solves built on them, all in IEEE double precision on device-resident column-major
+ * matrices.
+ *
+ * Every operation entry point mirrors one exported Go function of the reference package
+ * (file:line in its source tree) with the same argument meaning, flag bits and error
+ * conditions; a cgo shim keeps the Go signatures and forwards FloatMatrix views as
+ * mo_matrix values.  All calls are asynchronous on the context's stream unless noted;
+ * results that the Go function returns synchronously (the Cholesky panic index) make
+ * that entry point synchronize.
+ *
+ * Plain C: pointers, sizes and ints only.  Thread-safety: one context per host thread.
+ */
+#ifndef MATOPS_B200_H
+#define MATOPS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MO_API __attribute__((visibility("default")))
+#else
+#define MO_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Flag bits: identical values to matops.Flags (mmult.go:18-30, calgo/cmops.go:19-31). */
+#define MO_NOTRANS 0x0
+#define MO_TRANSA 0x1
+#define MO_TRANSB 0x2
+#define MO_LOWER 0x4
+#define MO_UPPER 0x8
+#define MO_LEFT 0x10
+#define MO_RIGHT 0x20
+#define MO_UNIT 0x40
+#define MO_TRANS 0x80
+
+/* Status codes.  0 = nil error.  Negative values name the Go error of the reference
+ * (message in comment) or a device-side failure.  Positive values are LAPACK-style info:
+ * for mo_decompose_chol, k+1 when column k's pivot square root is NaN (the reference
+ * panics with "illegal value at k", chol.go:33-36). */
+#define MO_OK 0
+#define MO_ESIZE (-1)        /* "Mult: size mismatch"                    mmult.go:224 */
+#define MO_ENOTSQUARE (-2)   /* "A not a square matrix"                  chol.go:119 */
+#define MO_EPIVLEN (-3)      /* "pivot array < min(A.Rows(),A.Cols())"    lu.go:424 */
+#define MO_ECNOTSQUARE (-4)  /* "C not a square matrix"                  mmult.go:428 */
+#define MO_EABSIZE (-5)      /* "A, B size mismatch"                     mmult.go:406 */
+#define MO_EINVAL (-10)      /* NULL context/pointer, negative size, ld < rows        */
+#define MO_ECUDA (-20)       /* CUDA runtime error                                    */
+#define MO_EDEVTIMEOUT (-21) /* a bounded device-side wait gave up                    */
+#define MO_ENOMEM (-22)      /* device allocation failed                              */
+#define MO_ENOKERNEL (-23)   /* no sm_100a kernel image for this device               */
+
+typedef struct mo_ctx mo_ctx;
+
+/* A device-resident column-major matrix view: element (i,j) is data[i + j*ld].  This is
+ * a FloatMatrix view (FloatArray() from the view's (0,0), LeadingIndex() = ld) with its
+ * backing array mirrored in device memory. */
+typedef struct mo_matrix {
+  double *data;
+  int64_t rows;
+  int64_t cols;
+  int64_t ld;
+} mo_matrix;
+
+/* ---- context: device, stream, workspace, package-global settings ---- */
+MO_API int mo_ctx_create(int device, mo_ctx **ctx);
+MO_API int mo_ctx_destroy(mo_ctx *ctx);
+/* stream is a cudaStream_t passed as void*; NULL selects the legacy default stream */
+MO_API int mo_set_stream(mo_ctx *ctx, void *stream);
+/* wait for all work on the context's stream; returns the first error recorded */
+MO_API int mo_sync(mo_ctx *ctx);
+MO_API const char *mo_strerror(int status);
+/* BlockingParams(mb, nb, kb), mmult.go:63-67.  Only nb changes results here: it is the
+ * diagonal block size of RankUpdateSym's beta (see mo_rank_update_sym). Returns 0. */
+MO_API int mo_blocking_params(mo_ctx *ctx, int mb, int nb, int kb);
+/* NumWorkers(n), mmult.go:69-73: kept for the shim; the GPU ignores it. Returns the old value. */
+MO_API int mo_num_workers(mo_ctx *ctx, int n);
+/* 1 = RankUpdateSym applies beta to the whole triangle (BLAS SYRK); 0 (default) = the
+ * reference's behaviour, beta only inside the nb x nb diagonal blocks (calgo/dmmat_rank.c:
+ * 28-56 vs 96-121).  Returns the old value. */
+MO_API int mo_set_syrk_blas_beta(mo_ctx *ctx, int on);
+
+/* ---- device memory helpers for shims that hold host-side matrices ---- */
+MO_API int mo_malloc(mo_ctx *ctx, void **ptr, size_t bytes);
+MO_API int mo_free(mo_ctx *ctx, void *ptr);
+/* copy a host column-major matrix (leading dim ld_src) into the device view dst */
+MO_API int mo_upload(mo_ctx *ctx, mo_matrix dst, const double *src, int64_t ld_src);
+/* copy the device view src into host memory with leading dim ld_dst */
+MO_API int mo_download(mo_ctx *ctx, double *dst, int64_t ld_dst, mo_matrix src);
+MO_API int mo_upload_bytes(mo_ctx *ctx, void *dst_dev, const void *src_host, size_t bytes);
+MO_API int mo_download_bytes(mo_ctx *ctx, void *dst_host, const void *src_dev, size_t bytes);
+
+/* ---- level 3 ---- */
+
+/* Mult(C, A, B, alpha, beta, flags), mmult.go:198-256:
+ *   C = beta*C + alpha*op(A)*op(B), op per MO_TRANSA / MO_TRANSB.
+ * Empty product (per the flag-dependent rule of mmult.go:205-222) -> MO_OK, no work.
+ * beta == 0 does not read C (calgo/vec_scale.c:118-133). */
+MO_API int mo_mult(mo_ctx *ctx, mo_matrix C, mo_matrix A, mo_matrix B, double alpha, double beta,
+            int flags);
+
+/* RankUpdateSym(C, A, alpha, beta, flags), mmult.go:426-445 (SYRK):
+ *   triangle(C) = beta*C + alpha*A*A^T   (MO_LOWER or MO_UPPER selects the triangle)
+ *   triangle(C) = beta*C + alpha*A^T*A   with MO_TRANSA.
+ * Non-square C -> MO_ECNOTSQUARE.  Rows of op(A) != rows of C -> MO_EABSIZE (the reference
+ * does not check and reads out of range). */
+MO_API int mo_rank_update_sym(mo_ctx *ctx, mo_matrix C, mo_matrix A, double alpha, double beta,
+                       int flags);
+
+/* SolveTrm(B, A, alpha, flags), mmult.go:388-422 (TRSM):
+ *   B = alpha * op(A)^-1 * B   (MO_LEFT, or neither side bit)
+ *   B = alpha * B * op(A)^-1   (MO_RIGHT)
+ * A triangular: MO_UPPER selects upper, otherwise lower; MO_UNIT = unit diagonal;
+ * MO_TRANSA = op(A) = A^T.  Size checks as mmult.go:394-407. */
+MO_API int mo_solve_trm(mo_ctx *ctx, mo_matrix B, mo_matrix A, double alpha, int flags);
+
+/* ---- factorizations and solves ---- */
+
+/* DecomposeCHOL(A, flags, nb), chol.go:116-127: A = L*L^T (MO_LOWER) or U^T*U (otherwise)
+ * in place; the opposite strict triangle is not referenced.  Non-square -> MO_ENOTSQUARE.
+ * nb is the reference's block size; the device picks its own blocking (results agree to
+ * rounding).  Synchronizes; returns k+1 > 0 when column k's pivot is not positive
+ * (sqrt gives NaN), with that pivot's value in *bad_value if non-NULL; A's contents are
+ * then unspecified. */
+MO_API int mo_decompose_chol(mo_ctx *ctx, mo_matrix A, int flags, int nb, double *bad_value);
+
+/* SolveCHOL(B, A, flags), chol.go:147-158: B = (A A^T)^-1 B with the factor from
+ * mo_decompose_chol (MO_UPPER checked first, then MO_LOWER; neither -> no-op). */
+MO_API int mo_solve_chol(mo_ctx *ctx, mo_matrix B, mo_matrix A, int flags);
+
+/* DecomposeLU(A, pivots, nb), lu.go:420-436: P*A = L*U with partial pivoting, L unit lower
+ * (diagonal not stored), in place.  pivots: device int64 array of npiv entries; on return
+ * pivots[k] is the 0-based absolute row swapped with row k (pivots[k] == k: no swap),
+ * entries >= min(rows,cols) are set to 0.  npiv < min(rows,cols) -> MO_EPIVLEN.  The pivot
+ * at each column is the first row holding the largest |value| (pivot.go:98-107). */
+MO_API int mo_decompose_lu(mo_ctx *ctx, mo_matrix A, int64_t *pivots, int64_t npiv, int nb);
+
+/* SolveLU(B, A, pivots, flags), lu.go:483-497: apply the row swaps to B in forward order
+ * (pivot.go:55-61), then B = U^-1 L^-1 B; with MO_TRANSA the same swaps followed by
+ * L^-T then U^-T, exactly the reference's sequence. */
+MO_API int mo_solve_lu(mo_ctx *ctx, mo_matrix B, mo_matrix A, const int64_t *pivots, int64_t npiv,
+                int flags);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MATOPS_B200_H */

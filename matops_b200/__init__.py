@@ -1,0 +1,12 @@
+"""matops_b200: B200 (sm_100a) implementation of hrautila/matops's level-3 hot path.
+
+GEMM / SYRK / TRSM and the blocked Cholesky / LU factorizations and solves in FP64 on
+device-resident column-major matrices, behind a C ABI (include/matops_b200.h) and this
+Go-API mirror (see matops_b200.api).
+"""
+from .api import (  # noqa: F401
+    LEFT, LOWER, NONE, NOTRANS, RIGHT, TRANS, TRANSA, TRANSB, UNIT, UPPER,
+    BlockingParams, DecomposeBlockSize, DecomposeCHOL, DecomposeLU, MatopsError, MatopsPanic,
+    Mult, NumWorkers, RankUpdateSym, SetPanicOnError, SolveCHOL, SolveLU, SolveTrm, Sync,
+    matrix, to_device, view,
+)

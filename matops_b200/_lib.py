@@ -1,0 +1,63 @@
+"""ctypes binding of libmatops_b200.so (the C ABI declared in include/matops_b200.h).
+
+The library is built in-tree by matops_b200/build.py.  There is no fallback: if the
+shared library is missing or cannot be loaded, importing the bindings raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libmatops_b200.so")
+
+
+class MoMatrix(ctypes.Structure):
+    """mo_matrix: device column-major view (data, rows, cols, ld)."""
+    _fields_ = [("data", ctypes.c_void_p), ("rows", ctypes.c_int64),
+                ("cols", ctypes.c_int64), ("ld", ctypes.c_int64)]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m matops_b200.build` "
+            "(there is no CPU fallback)")
+    L = ctypes.CDLL(LIB_PATH)
+    i, d, p, i64, sz = ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_int64, ctypes.c_size_t
+    M = MoMatrix
+    sigs = {
+        "mo_ctx_create": [i, ctypes.POINTER(p)],
+        "mo_ctx_destroy": [p],
+        "mo_set_stream": [p, p],
+        "mo_sync": [p],
+        "mo_blocking_params": [p, i, i, i],
+        "mo_num_workers": [p, i],
+        "mo_set_syrk_blas_beta": [p, i],
+        "mo_malloc": [p, ctypes.POINTER(p), sz],
+        "mo_free": [p, p],
+        "mo_upload": [p, M, p, i64],
+        "mo_download": [p, p, i64, M],
+        "mo_upload_bytes": [p, p, p, sz],
+        "mo_download_bytes": [p, p, p, sz],
+        "mo_mult": [p, M, M, M, d, d, i],
+        "mo_rank_update_sym": [p, M, M, d, d, i],
+        "mo_solve_trm": [p, M, M, d, i],
+        "mo_decompose_chol": [p, M, i, i, ctypes.POINTER(d)],
+        "mo_solve_chol": [p, M, M, i],
+        "mo_decompose_lu": [p, M, p, i64, i],
+        "mo_solve_lu": [p, M, M, p, i64, i],
+    }
+    for name, args in sigs.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = i
+    L.mo_strerror.argtypes = [i]
+    L.mo_strerror.restype = ctypes.c_char_p
+    _lib = L
+    return L

@@ -1,0 +1,173 @@
+"""Host-side mirror of the reference's Go API for the level-3 / Cholesky / LU path.
+
+Names, argument order, flag values and error behaviour follow package matops
+(mmult.go, chol.go, lu.go): functions return ``None`` for a nil error or a
+:class:`MatopsError` carrying the Go error string; a Go ``panic`` (non-SPD Cholesky,
+chol.go:33-36, or any error after ``SetPanicOnError(True)`` for the wrappers that use
+``onError``, mmult.go:46-57) raises :class:`MatopsPanic`.
+
+Matrices are CUDA float64 tensors in column-major layout (stride(0) == 1); slicing such
+a tensor gives a view with the parent's leading dimension, like FloatMatrix.SubMatrix.
+Every call goes through the C ABI of libmatops_b200.so on the current torch stream.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _lib
+
+# flags, calgo/cmops.go:19-31
+TRANSA, TRANSB, LOWER, UPPER, LEFT, RIGHT, UNIT, TRANS = 0x1, 0x2, 0x4, 0x8, 0x10, 0x20, 0x40, 0x80
+NOTRANS = NONE = 0
+
+
+class MatopsError(Exception):
+    """A Go error value returned by a matops function."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(msg)
+        self.code = code
+
+
+class MatopsPanic(RuntimeError):
+    """A Go panic in the reference (raised, not returned)."""
+
+
+_panic_on_error = False
+_contexts: dict[int, ctypes.c_void_p] = {}
+_settings = {"blocking": (68, 68, 196), "workers": 1}
+
+
+def SetPanicOnError(newval: bool) -> None:
+    """mmult.go:55-57"""
+    global _panic_on_error
+    _panic_on_error = bool(newval)
+
+
+def BlockingParams(mb: int, nb: int, kb: int) -> None:
+    """mmult.go:63-67 (nb sets RankUpdateSym's beta block; see mo_blocking_params)"""
+    _settings["blocking"] = (mb, nb, kb)
+    for c in _contexts.values():
+        _lib.lib().mo_blocking_params(c, mb, nb, kb)
+
+
+def NumWorkers(newWorkers: int) -> int:
+    """mmult.go:69-73 -- kept for drop-in compatibility; the device does not use it."""
+    old = _settings["workers"]
+    _settings["workers"] = newWorkers
+    return old
+
+
+def DecomposeBlockSize(nb: int) -> None:
+    """lu.go:35-37 -- sets a global that the reference never reads."""
+
+
+def context(device: int | None = None) -> ctypes.c_void_p:
+    dev = torch.cuda.current_device() if device is None else device
+    c = _contexts.get(dev)
+    if c is None:
+        c = ctypes.c_void_p()
+        rc = _lib.lib().mo_ctx_create(dev, ctypes.byref(c))
+        if rc != 0:
+            raise RuntimeError(f"mo_ctx_create({dev}) failed: {_lib.lib().mo_strerror(rc).decode()}")
+        _lib.lib().mo_blocking_params(c, *_settings["blocking"])
+        _contexts[dev] = c
+    _lib.lib().mo_set_stream(c, ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+    return c
+
+
+def view(t: torch.Tensor) -> _lib.MoMatrix:
+    """mo_matrix of a column-major CUDA float64 tensor view."""
+    if t.dim() != 2 or t.dtype != torch.float64 or not t.is_cuda:
+        raise TypeError("expected a 2-D float64 CUDA tensor")
+    r, c = t.shape
+    if r > 1 and t.stride(0) != 1:
+        raise TypeError("matrix view must be column-major (stride(0) == 1)")
+    ld = t.stride(1) if c > 1 else max(t.stride(1), r, 1)
+    return _lib.MoMatrix(t.data_ptr(), r, c, max(ld, r, 1))
+
+
+def matrix(rows: int, cols: int, device=None, fill=None) -> torch.Tensor:
+    """Allocate a column-major float64 matrix on the device."""
+    dev = device if device is not None else torch.device("cuda", torch.cuda.current_device())
+    t = torch.empty((cols, rows), dtype=torch.float64, device=dev).t()
+    if fill is not None:
+        t.fill_(fill)
+    return t
+
+
+def to_device(a, device=None) -> torch.Tensor:
+    """Copy a 2-D host array (numpy or torch) into a new column-major device matrix."""
+    src = torch.as_tensor(a, dtype=torch.float64)
+    t = matrix(src.shape[0], src.shape[1], device)
+    t.copy_(src)
+    return t
+
+
+def _err(rc: int, use_on_error: bool = False):
+    if rc == 0:
+        return None
+    msg = _lib.lib().mo_strerror(rc).decode()
+    if use_on_error and _panic_on_error:
+        raise MatopsPanic(msg)
+    if rc in (-20, -21, -22, -23):
+        raise RuntimeError(f"matops_b200 device failure: {msg} ({rc})")
+    return MatopsError(rc, msg)
+
+
+def Mult(C, A, B, alpha: float, beta: float, flags: int = NOTRANS):
+    """mmult.go:198 -- C = beta*C + alpha*op(A)*op(B)."""
+    return _err(_lib.lib().mo_mult(context(), view(C), view(A), view(B), alpha, beta, flags))
+
+
+def RankUpdateSym(C, A, alpha: float, beta: float, flags: int):
+    """mmult.go:426 -- triangle(C) = beta*C + alpha*A*A^T (or A^T*A with TRANSA)."""
+    return _err(_lib.lib().mo_rank_update_sym(context(), view(C), view(A), alpha, beta, flags), True)
+
+
+def SolveTrm(B, A, alpha: float, flags: int):
+    """mmult.go:388 -- B = alpha*op(A)^-1*B (LEFT) or alpha*B*op(A)^-1 (RIGHT)."""
+    return _err(_lib.lib().mo_solve_trm(context(), view(B), view(A), alpha, flags), True)
+
+
+def DecomposeCHOL(A, flags: int, nb: int):
+    """chol.go:116 -- returns (A, err); a non-positive pivot panics like the reference."""
+    bad = ctypes.c_double(0.0)
+    rc = _lib.lib().mo_decompose_chol(context(), view(A), flags, nb, ctypes.byref(bad))
+    if rc > 0:
+        raise MatopsPanic(f"illegal value at {rc - 1}: {bad.value:e}")
+    return A, _err(rc)
+
+
+def SolveCHOL(B, A, flags: int) -> None:
+    """chol.go:147 (no return value)."""
+    rc = _lib.lib().mo_solve_chol(context(), view(B), view(A), flags)
+    if rc != 0:
+        e = _err(rc, True)
+        if e is not None:
+            raise MatopsPanic(str(e))
+
+
+def DecomposeLU(A, pivots: torch.Tensor, nb: int):
+    """lu.go:420 -- returns (A, err); pivots is a CUDA int64 tensor (0-based rows)."""
+    if pivots.dtype != torch.int64 or not pivots.is_cuda or not pivots.is_contiguous():
+        raise TypeError("pivots must be a contiguous CUDA int64 tensor")
+    rc = _lib.lib().mo_decompose_lu(context(), view(A), ctypes.c_void_p(pivots.data_ptr()),
+                                    pivots.numel(), nb)
+    return A, _err(rc)
+
+
+def SolveLU(B, A, pivots: torch.Tensor, flags: int):
+    """lu.go:483 -- apply the interchanges, then the two triangular solves."""
+    if pivots.dtype != torch.int64 or not pivots.is_cuda or not pivots.is_contiguous():
+        raise TypeError("pivots must be a contiguous CUDA int64 tensor")
+    rc = _lib.lib().mo_solve_lu(context(), view(B), view(A), ctypes.c_void_p(pivots.data_ptr()),
+                                pivots.numel(), flags)
+    return _err(rc)
+
+
+def Sync() -> int:
+    """Wait for the context's stream; returns the first device-side status recorded."""
+    return _lib.lib().mo_sync(context())

@@ -1,0 +1,414 @@
+// extern "C" entry points (include/matops_b200.h): argument checking that mirrors the Go
+// wrappers of the reference, then dispatch to the device drivers.
+#include <climits>
+#include <cstddef>
+#include <cstring>
+
+#include "context.cuh"
+
+namespace mo {
+int potrf(mo_ctx *ctx, View A, bool upper, int *d_info, double *d_bad, double *inv);
+int getrf(mo_ctx *ctx, View A, int64_t *piv, int64_t npiv, int ref_nb);
+int laswp_forward(mo_ctx *ctx, View B, const int64_t *piv, int64_t npiv);
+
+namespace {
+// control block in device memory: [0] status word, [1] info, [2..3] bad pivot value
+struct Control {
+  int status;
+  int info;
+  double bad;
+};
+}  // namespace
+
+int to_view(const mo_matrix &m, View &v) {
+  if (m.rows < 0 || m.cols < 0 || m.rows > INT_MAX || m.cols > INT_MAX) return MO_EINVAL;
+  if (m.rows > 0 && m.cols > 0) {
+    if (!m.data) return MO_EINVAL;
+    if (m.ld < m.rows || m.ld < 1) return MO_EINVAL;
+  }
+  v.d = m.data;
+  v.rows = (int)m.rows;
+  v.cols = (int)m.cols;
+  v.ld = m.ld < 1 ? 1 : m.ld;
+  return MO_OK;
+}
+
+int enter(mo_ctx *ctx) {
+  if (!ctx) return MO_EINVAL;
+  MO_CUDA_TRY(cudaSetDevice(ctx->device));
+  return MO_OK;
+}
+
+int workspace(mo_ctx *ctx, size_t bytes, void **out) {
+  if (bytes > ctx->ws_bytes) {
+    MO_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (ctx->ws) cudaFree(ctx->ws);
+    ctx->ws = nullptr;
+    ctx->ws_bytes = 0;
+    size_t want = bytes < (size_t(1) << 22) ? (size_t(1) << 22) : bytes;
+    MO_CUDA_TRY(cudaMalloc(&ctx->ws, want));
+    ctx->ws_bytes = want;
+  }
+  *out = ctx->ws;
+  return MO_OK;
+}
+
+static Control *control(mo_ctx *ctx) { return reinterpret_cast<Control *>(ctx->d_status); }
+
+int gemm(mo_ctx *ctx, View C, View A, bool ta, View B, bool tb, double alpha, double beta) {
+  GemmArgs g;
+  g.M = C.rows;
+  g.N = C.cols;
+  g.K = ta ? A.rows : A.cols;
+  g.alpha = alpha;
+  g.beta = beta;
+  g.A = A.d;
+  g.lda = A.ld;
+  g.transA = ta;
+  g.B = B.d;
+  g.ldb = B.ld;
+  g.transB = tb;
+  g.C = C.d;
+  g.ldc = C.ld;
+  g.mode = kGemm;
+  g.status = &control(ctx)->status;
+  return launch_gemm(g, ctx->stream);
+}
+
+int syrk(mo_ctx *ctx, View C, View A, bool ta, bool upper, double alpha, double beta,
+         int beta_block) {
+  GemmArgs g;
+  g.M = C.rows;
+  g.N = C.cols;
+  g.K = ta ? A.rows : A.cols;
+  g.alpha = alpha;
+  g.beta = beta;
+  g.A = A.d;
+  g.lda = A.ld;
+  g.transA = ta;
+  g.B = A.d;
+  g.ldb = A.ld;
+  g.transB = !ta;
+  g.C = C.d;
+  g.ldc = C.ld;
+  g.mode = upper ? kSyrkUpper : kSyrkLower;
+  g.beta_block = beta_block;
+  g.status = &control(ctx)->status;
+  return launch_gemm(g, ctx->stream);
+}
+
+}  // namespace mo
+
+using mo::View;
+
+extern "C" {
+
+int mo_ctx_create(int device, mo_ctx **out) {
+  if (!out) return MO_EINVAL;
+  *out = nullptr;
+  int ndev = 0;
+  MO_CUDA_TRY(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return MO_EINVAL;
+  MO_CUDA_TRY(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  MO_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10) return MO_ENOKERNEL;  // sm_100a image only
+  mo_ctx *ctx = new mo_ctx();
+  ctx->device = device;
+  ctx->sms = prop.multiProcessorCount;
+  cudaError_t e = cudaMalloc(&ctx->d_status, sizeof(mo::Control));
+  if (e == cudaSuccess) e = cudaMemset(ctx->d_status, 0, sizeof(mo::Control));
+  if (e != cudaSuccess) {
+    delete ctx;
+    return mo_from_cuda_error(e);
+  }
+  *out = ctx;
+  return MO_OK;
+}
+
+int mo_ctx_destroy(mo_ctx *ctx) {
+  if (!ctx) return MO_EINVAL;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->ws) cudaFree(ctx->ws);
+  if (ctx->d_status) cudaFree(ctx->d_status);
+  delete ctx;
+  return MO_OK;
+}
+
+int mo_set_stream(mo_ctx *ctx, void *stream) {
+  if (!ctx) return MO_EINVAL;
+  ctx->stream = reinterpret_cast<cudaStream_t>(stream);
+  return MO_OK;
+}
+
+int mo_sync(mo_ctx *ctx) {
+  int rc = mo::enter(ctx);
+  if (rc) return rc;
+  MO_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  int st = 0;
+  MO_CUDA_TRY(cudaMemcpy(&st, &mo::control(ctx)->status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (st != 0) MO_CUDA_TRY(cudaMemset(&mo::control(ctx)->status, 0, sizeof(int)));
+  return st;
+}
+
+const char *mo_strerror(int s) {
+  switch (s) {
+    case MO_OK: return "ok";
+    case MO_ESIZE: return "Mult: size mismatch";
+    case MO_ENOTSQUARE: return "A not a square matrix";
+    case MO_EPIVLEN: return "pivot array < min(A.Rows(),A.Cols())";
+    case MO_ECNOTSQUARE: return "C not a square matrix";
+    case MO_EABSIZE: return "A, B size mismatch";
+    case MO_EINVAL: return "invalid argument";
+    case MO_ECUDA: return "CUDA runtime error";
+    case MO_EDEVTIMEOUT: return "device-side wait timed out";
+    case MO_ENOMEM: return "device out of memory";
+    case MO_ENOKERNEL: return "no sm_100a kernel image for this device";
+    default: return s > 0 ? "illegal value (non-positive pivot)" : "unknown error";
+  }
+}
+
+int mo_blocking_params(mo_ctx *ctx, int mb, int nb, int kb) {
+  if (!ctx) return MO_EINVAL;
+  ctx->mb = mb;
+  ctx->nb = nb;
+  ctx->kb = kb;
+  return MO_OK;
+}
+
+int mo_num_workers(mo_ctx *ctx, int n) {
+  if (!ctx) return MO_EINVAL;
+  int old = ctx->workers;
+  ctx->workers = n;
+  return old;
+}
+
+int mo_set_syrk_blas_beta(mo_ctx *ctx, int on) {
+  if (!ctx) return MO_EINVAL;
+  int old = ctx->syrk_blas_beta;
+  ctx->syrk_blas_beta = on ? 1 : 0;
+  return old;
+}
+
+int mo_malloc(mo_ctx *ctx, void **ptr, size_t bytes) {
+  int rc = mo::enter(ctx);
+  if (rc) return rc;
+  if (!ptr) return MO_EINVAL;
+  MO_CUDA_TRY(cudaMalloc(ptr, bytes ? bytes : 16));
+  return MO_OK;
+}
+
+int mo_free(mo_ctx *ctx, void *ptr) {
+  int rc = mo::enter(ctx);
+  if (rc) return rc;
+  MO_CUDA_TRY(cudaFree(ptr));
+  return MO_OK;
+}
+
+int mo_upload(mo_ctx *ctx, mo_matrix dst, const double *src, int64_t ld_src) {
+  int rc = mo::enter(ctx);
+  if (rc) return rc;
+  View v;
+  if ((rc = mo::to_view(dst, v))) return rc;
+  if (v.rows == 0 || v.cols == 0) return MO_OK;
+  if (!src || ld_src < v.rows) return MO_EINVAL;
+  MO_CUDA_TRY(cudaMemcpy2DAsync(v.d, v.ld * 8, src, ld_src * 8, (size_t)v.rows * 8, v.cols,
+                                cudaMemcpyHostToDevice, ctx->stream));
+  return MO_OK;
+}
+
+int mo_download(mo_ctx *ctx, double *dst, int64_t ld_dst, mo_matrix src) {
+  int rc = mo::enter(ctx);
+  if (rc) return rc;
+  View v;
+  if ((rc = mo::to_view(src, v))) return rc;
+  if (v.rows == 0 || v.cols == 0) return MO_OK;
+  if (!dst || ld_dst < v.rows) return MO_EINVAL;
+  MO_CUDA_TRY(cudaMemcpy2DAsync(dst, ld_dst * 8, v.d, v.ld * 8, (size_t)v.rows * 8, v.cols,
+                                cudaMemcpyDeviceToHost, ctx->stream));
+  return MO_OK;
+}
+
+int mo_upload_bytes(mo_ctx *ctx, void *dst, const void *src, size_t bytes) {
+  int rc = mo::enter(ctx);
+  if (rc) return rc;
+  if (bytes == 0) return MO_OK;
+  MO_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  return MO_OK;
+}
+
+int mo_download_bytes(mo_ctx *ctx, void *dst, const void *src, size_t bytes) {
+  int rc = mo::enter(ctx);
+  if (rc) return rc;
+  if (bytes == 0) return MO_OK;
+  MO_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  return MO_OK;
+}
+
+// mmult.go:198-256
+int mo_mult(mo_ctx *ctx, mo_matrix Cm, mo_matrix Am, mo_matrix Bm, double alpha, double beta,
+            int flags) {
+  int rc = mo::enter(ctx);
+  if (rc) return rc;
+  View C, A, B;
+  if ((rc = mo::to_view(Cm, C)) || (rc = mo::to_view(Am, A)) || (rc = mo::to_view(Bm, B)))
+    return rc;
+  const int ar = A.rows, ac = A.cols, br = B.rows, bc = B.cols, cr = C.rows, cc = C.cols;
+  bool ok, empty;
+  switch (flags & (MO_TRANSA | MO_TRANSB)) {
+    case MO_TRANSA | MO_TRANSB:
+      empty = ac == 0 || br == 0;
+      ok = cr == ac && cc == br && ar == bc;
+      break;
+    case MO_TRANSA:
+      empty = ac == 0 || bc == 0;
+      ok = cr == ac && cc == bc && ar == br;
+      break;
+    case MO_TRANSB:
+      empty = ar == 0 || br == 0;
+      ok = cr == ar && cc == br && ac == bc;
+      break;
+    default:
+      empty = ar == 0 || bc == 0;
+      ok = cr == ar && cc == bc && ac == br;
+  }
+  if (empty) return MO_OK;
+  if (!ok) return MO_ESIZE;
+  return mo::gemm(ctx, C, A, (flags & MO_TRANSA) != 0, B, (flags & MO_TRANSB) != 0, alpha, beta);
+}
+
+// mmult.go:426-445 with calgo/cmops.go:219-240 and calgo/dmmat_rank.c:62-127
+int mo_rank_update_sym(mo_ctx *ctx, mo_matrix Cm, mo_matrix Am, double alpha, double beta,
+                       int flags) {
+  int rc = mo::enter(ctx);
+  if (rc) return rc;
+  View C, A;
+  if ((rc = mo::to_view(Cm, C)) || (rc = mo::to_view(Am, A))) return rc;
+  if (C.rows != C.cols) return MO_ECNOTSQUARE;
+  const bool ta = (flags & MO_TRANSA) != 0;
+  const int P = ta ? A.rows : A.cols;
+  const int n = C.rows;
+  if (P == 0 || n == 0) return MO_OK;  // the reference returns before touching C
+  if ((ta ? A.cols : A.rows) != n) return MO_EABSIZE;
+  const bool up = (flags & MO_UPPER) != 0, lo = (flags & MO_LOWER) != 0;
+  if (up == lo) return MO_EINVAL;  // exactly one triangle must be named
+  int bb = 0;
+  if (!ctx->syrk_blas_beta && beta != 1.0) {
+    // calgo/dmmat_rank.c:75-83: NB clamped to (0, 68] and to the order of C
+    int nb = ctx->nb;
+    if (nb > 68 || nb <= 0) nb = 68;
+    if (nb > n) nb = n;
+    bb = nb;
+  }
+  return mo::syrk(ctx, C, A, ta, up, alpha, beta, bb);
+}
+
+// mmult.go:388-422
+int mo_solve_trm(mo_ctx *ctx, mo_matrix Bm, mo_matrix Am, double alpha, int flags) {
+  int rc = mo::enter(ctx);
+  if (rc) return rc;
+  View B, A;
+  if ((rc = mo::to_view(Bm, B)) || (rc = mo::to_view(Am, A))) return rc;
+  bool ok = true, empty = false;
+  switch (flags & (MO_LEFT | MO_RIGHT)) {
+    case MO_LEFT:
+      empty = B.rows == 0;
+      ok = B.rows == A.cols && A.cols == A.rows;
+      break;
+    case MO_RIGHT:
+      empty = B.cols == 0;
+      ok = B.cols == A.rows && A.cols == A.rows;
+      break;
+    default:
+      break;
+  }
+  if (empty) return MO_OK;
+  if (!ok) return MO_EABSIZE;
+  // no side check in the reference when neither or both side bits are set; the triangle
+  // order is A.Cols() (calgo/cmops.go:195-215); refuse shapes that would read out of range
+  const int N = A.cols;
+  const bool right = (flags & MO_RIGHT) != 0;
+  if (N == 0 || (right ? B.rows : B.cols) == 0) return MO_OK;
+  if (A.rows < N || (right ? B.cols : B.rows) < N) return MO_EABSIZE;
+  View Bn = right ? B.sub(0, 0, B.rows, N) : B.sub(0, 0, N, B.cols);
+  return mo::trsm(ctx, Bn, A.sub(0, 0, N, N), flags, alpha);
+}
+
+// chol.go:116-127
+int mo_decompose_chol(mo_ctx *ctx, mo_matrix Am, int flags, int nb, double *bad_value) {
+  (void)nb;
+  int rc = mo::enter(ctx);
+  if (rc) return rc;
+  View A;
+  if ((rc = mo::to_view(Am, A))) return rc;
+  if (A.rows != A.cols) return MO_ENOTSQUARE;
+  if (A.rows == 0) return MO_OK;
+  mo::Control *cb = mo::control(ctx);
+  MO_CUDA_TRY(cudaMemsetAsync(&cb->info, 0, sizeof(mo::Control) - offsetof(mo::Control, info), ctx->stream));
+  double *inv = nullptr;
+  if ((rc = mo::workspace(ctx, 128 * 128 * sizeof(double), (void **)&inv))) return rc;
+  // LOWER selects L*L^T; any other flags factor the upper triangle (chol.go:39-49, 77-87)
+  rc = mo::potrf(ctx, A, (flags & MO_LOWER) == 0, &cb->info, &cb->bad, inv);
+  if (rc) return rc;
+  MO_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  mo::Control h;
+  MO_CUDA_TRY(cudaMemcpy(&h, cb, sizeof(h), cudaMemcpyDeviceToHost));
+  if (h.status) {
+    cudaMemset(&cb->status, 0, sizeof(int));
+    return h.status;
+  }
+  if (h.info > 0 && bad_value) *bad_value = h.bad;
+  return h.info;
+}
+
+// chol.go:147-158
+int mo_solve_chol(mo_ctx *ctx, mo_matrix Bm, mo_matrix Am, int flags) {
+  int rc;
+  if (flags & MO_UPPER) {
+    rc = mo_solve_trm(ctx, Bm, Am, 1.0, MO_UPPER | MO_TRANSA);
+    if (!rc) rc = mo_solve_trm(ctx, Bm, Am, 1.0, MO_UPPER);
+    return rc;
+  }
+  if (flags & MO_LOWER) {
+    rc = mo_solve_trm(ctx, Bm, Am, 1.0, MO_LOWER);
+    if (!rc) rc = mo_solve_trm(ctx, Bm, Am, 1.0, MO_LOWER | MO_TRANSA);
+    return rc;
+  }
+  return MO_OK;
+}
+
+// lu.go:420-436
+int mo_decompose_lu(mo_ctx *ctx, mo_matrix Am, int64_t *piv, int64_t npiv, int nb) {
+  int rc = mo::enter(ctx);
+  if (rc) return rc;
+  View A;
+  if ((rc = mo::to_view(Am, A))) return rc;
+  const int mlen = A.rows < A.cols ? A.rows : A.cols;
+  if (npiv < mlen) return MO_EPIVLEN;
+  if (npiv > 0 && !piv) return MO_EINVAL;
+  if (npiv > 0) MO_CUDA_TRY(cudaMemsetAsync(piv, 0, (size_t)npiv * sizeof(int64_t), ctx->stream));
+  if (mlen == 0) return MO_OK;
+  return mo::getrf(ctx, A, piv, npiv, nb);
+}
+
+// lu.go:483-497
+int mo_solve_lu(mo_ctx *ctx, mo_matrix Bm, mo_matrix Am, const int64_t *piv, int64_t npiv,
+                int flags) {
+  int rc = mo::enter(ctx);
+  if (rc) return rc;
+  View B;
+  if ((rc = mo::to_view(Bm, B))) return rc;
+  if (npiv > 0 && !piv) return MO_EINVAL;
+  if ((rc = mo::laswp_forward(ctx, B, piv, npiv))) return rc;
+  if (flags & MO_TRANSA) {
+    rc = mo_solve_trm(ctx, Bm, Am, 1.0, MO_LOWER | MO_UNIT | MO_TRANSA);
+    if (!rc) rc = mo_solve_trm(ctx, Bm, Am, 1.0, MO_UPPER | MO_TRANSA);
+  } else {
+    rc = mo_solve_trm(ctx, Bm, Am, 1.0, MO_LOWER | MO_UNIT);
+    if (!rc) rc = mo_solve_trm(ctx, Bm, Am, 1.0, MO_UPPER);
+  }
+  return rc;
+}
+
+}  // extern "C"

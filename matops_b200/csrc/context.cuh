@@ -1,0 +1,51 @@
+// The mo_ctx object and internal entry points shared by the C-ABI translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "gemm.cuh"
+
+struct mo_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int *d_status = nullptr;  // device status word written by bounded waits
+  int mb = 68, nb = 68, kb = 196;  // BlockingParams (mmult.go:33-35)
+  int workers = 1;                 // NumWorkers (mmult.go:38)
+  int syrk_blas_beta = 0;
+  // scratch owned by the context (grown on demand, freed in mo_ctx_destroy)
+  void *ws = nullptr;
+  size_t ws_bytes = 0;
+  int sms = 148;
+};
+
+namespace mo {
+
+struct View {
+  double *d;
+  int rows, cols;
+  int64_t ld;
+  double *at(int i, int j) const { return d + i + (int64_t)j * ld; }
+  View sub(int i, int j, int r, int c) const { return View{at(i, j), r, c, ld}; }
+};
+
+// Validates a public mo_matrix: non-negative sizes that fit in int, ld >= rows, data
+// non-NULL when non-empty.  Returns MO_OK or MO_EINVAL.
+int to_view(const mo_matrix &m, View &v);
+
+// make the context's device current for this call
+int enter(mo_ctx *ctx);
+
+// grow the context workspace to at least `bytes` (stream-ordered: synchronizes first)
+int workspace(mo_ctx *ctx, size_t bytes, void **out);
+
+// C = alpha*op(A)*op(B) + beta*C on device views (sizes already checked)
+int gemm(mo_ctx *ctx, View C, View A, bool ta, View B, bool tb, double alpha, double beta);
+
+// triangle(C) = alpha*op(A)*op(A)^T + beta*C; beta_block as in GemmArgs
+int syrk(mo_ctx *ctx, View C, View A, bool ta, bool upper, double alpha, double beta,
+         int beta_block);
+
+// B = alpha*op(A)^-1*B (left) or alpha*B*op(A)^-1 (right); A n x n triangle
+int trsm(mo_ctx *ctx, View B, View A, int flags, double alpha);
+
+}  // namespace mo

@@ -1,0 +1,39 @@
+// DGEMM / DSYRK engine: host-side interface.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mo {
+
+enum GemmMode : int {
+  kGemm = 0,       // C[M,N] = alpha*op(A)*op(B) + beta*C
+  kSyrkLower = 1,  // only tiles / elements with row >= col are computed and written
+  kSyrkUpper = 2,  // only row <= col
+};
+
+struct GemmArgs {
+  int M = 0, N = 0, K = 0;
+  double alpha = 1.0, beta = 0.0;
+  const double *A = nullptr;
+  int64_t lda = 0;
+  bool transA = false;  // op(A)(m,k) = A[k + m*lda] when true, A[m + k*lda] otherwise
+  const double *B = nullptr;
+  int64_t ldb = 0;
+  bool transB = false;  // op(B)(k,n) = B[n + k*ldb] when true, B[k + n*ldb] otherwise
+  double *C = nullptr;
+  int64_t ldc = 0;
+  int mode = kGemm;
+  // > 0: beta applies only where row/beta_block == col/beta_block (elsewhere beta = 1)
+  int beta_block = 0;
+  int *status = nullptr;  // device status word (first error wins)
+  bool force_fallback = false;  // use the cp.async producer even when TMA is legal
+};
+
+// Enqueue one launch on `stream`.  Returns MO_OK or a negative MO_E* code.
+int launch_gemm(const GemmArgs &args, cudaStream_t stream);
+
+// True when the TMA producer can be used for these operands (16-byte aligned bases,
+// leading dimensions that are multiples of 2 doubles).
+bool gemm_tma_ok(const GemmArgs &args);
+
+}  // namespace mo

@@ -1,0 +1,358 @@
+// LU factorization with partial pivoting (DecomposeLU) and the row interchanges used by
+// SolveLU, on the device.
+//
+// Reference: lu.go:173-231 (blockedLUpiv, left-looking Crout variant), lu.go:103-171
+// (unblockedLUpiv), pivot.go:27-61 (swapRows/applyPivots), pivot.go:98-107 (pivotIndex:
+// first row holding the strict maximum of |x|; a NaN never wins unless it sits on the
+// diagonal, where the scan starts).  The factors do not depend on left- vs right-looking
+// order except through rounding, so the device runs the right-looking form:
+//   panel   : cooperative kernel, every CTA owns a slice of panel rows in shared memory,
+//             one grid barrier per column (candidate rows are published with the local
+//             argmax, so every CTA picks the pivot itself)
+//   laswp   : apply the panel's interchanges to the columns left and right of it
+//   trsm    : U12 = L11^-1 A12 (unit lower inverse + in-place GEMM)
+//   update  : A22 -= L21 U12 on the FP64 tensor pipe
+#include <algorithm>
+#include <climits>
+#include <utility>
+
+#include "context.cuh"
+#include "tri.cuh"
+
+namespace mo {
+int trtri_blocks(mo_ctx *ctx, View A, int N, bool trans, bool lower_eff, bool unit, double *inv);
+
+namespace {
+
+constexpr int PANEL_THREADS = 256;
+constexpr int MAX_PANEL_W = 64;
+
+struct PanelScratch {
+  // double-buffered per-CTA candidates: value, index, NaN-on-diagonal flag, row values
+  double *cand_val;   // [2][nblk]
+  int *cand_idx;      // [2][nblk]
+  double *cand_row;   // [2][nblk][W]
+  double *rowj;       // [2][W]  current contents of panel row j (published by its owner)
+  int *diag_nan;      // [2]
+  unsigned *barrier;  // monotonically increasing arrival counter
+};
+
+__device__ __forceinline__ bool better(double v, int i, double bv, int bi) {
+  return v > bv || (v == bv && i < bi);
+}
+
+// Bounded grid barrier over `nblk` co-resident CTAs (cooperative launch).  Returns false
+// after recording MO_EDEVTIMEOUT.
+__device__ bool grid_barrier(unsigned *counter, unsigned target, int *status, int *abort_flag) {
+  __syncthreads();
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(counter, 1u);
+    int ok = 1;
+    unsigned i = 0;
+    while (true) {
+      unsigned v = *(volatile unsigned *)counter;
+      if (v >= target) break;
+      if (*(volatile int *)abort_flag) {
+        ok = 0;
+        break;
+      }
+      if (++i > MO_SPIN_LIMIT) {
+        set_status(status, MO_EDEVTIMEOUT);
+        atomicExch(abort_flag, 1);
+        ok = 0;
+        break;
+      }
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Factor the m x W panel P (column-major, ld) in place; piv[j] = row0 + pivot position.
+// Each CTA owns rows [b*R, min((b+1)*R, m)) in shared memory (row-major, stride W+1).
+__global__ void __launch_bounds__(PANEL_THREADS)
+    lu_panel_kernel(double *P, int64_t ld, int m, int W, int R, int64_t *piv, int64_t row0,
+                    PanelScratch sc, int *status, int *abort_flag) {
+  extern __shared__ double S[];
+  const int nblk = gridDim.x, b = blockIdx.x;
+  const int LDW = W + 1;
+  const int rbeg = b * R, rend = min(m, rbeg + R), nr = max(0, rend - rbeg);
+  __shared__ double s_prow[MAX_PANEL_W];
+  __shared__ double s_oldj[MAX_PANEL_W];
+  __shared__ double red_v[PANEL_THREADS / 32];
+  __shared__ int red_i[PANEL_THREADS / 32];
+  __shared__ int s_p;
+
+  for (int e = threadIdx.x; e < nr * W; e += blockDim.x) {
+    const int r = e % nr, c = e / nr;
+    S[r * LDW + c] = P[(rbeg + r) + (int64_t)c * ld];
+  }
+  __syncthreads();
+
+  const int kmax = min(m, W);
+  for (int j = 0; j < kmax; ++j) {
+    const int par = j & 1;
+    // (a) local argmax of |column j| over owned positions >= j
+    double bv = -1.0;
+    int bi = INT_MAX;
+    for (int r = threadIdx.x; r < nr; r += blockDim.x) {
+      const int gi = rbeg + r;
+      if (gi < j) continue;
+      const double a = S[r * LDW + j];
+      double v = fabs(a);
+      if (isnan(v)) v = -1.0;  // NaN never wins off the diagonal
+      if (better(v, gi, bv, bi)) {
+        bv = v;
+        bi = gi;
+      }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ov = __shfl_down_sync(0xffffffffu, bv, off);
+      const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+      if (better(ov, oi, bv, bi)) {
+        bv = ov;
+        bi = oi;
+      }
+    }
+    if ((threadIdx.x & 31) == 0) {
+      red_v[threadIdx.x >> 5] = bv;
+      red_i[threadIdx.x >> 5] = bi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+        if (better(red_v[w], red_i[w], bv, bi)) {
+          bv = red_v[w];
+          bi = red_i[w];
+        }
+      sc.cand_val[par * nblk + b] = bv;
+      sc.cand_idx[par * nblk + b] = bi;
+      s_p = bi;
+    }
+    __syncthreads();
+    // (b) publish the candidate row and, if owned here, row j
+    {
+      const int ci = s_p;
+      double *crow = sc.cand_row + ((size_t)par * nblk + b) * W;
+      if (ci != INT_MAX)
+        for (int c = threadIdx.x; c < W; c += blockDim.x) crow[c] = S[(ci - rbeg) * LDW + c];
+      if (j >= rbeg && j < rend) {
+        for (int c = threadIdx.x; c < W; c += blockDim.x) sc.rowj[par * W + c] = S[(j - rbeg) * LDW + c];
+        if (threadIdx.x == 0) sc.diag_nan[par] = isnan(S[(j - rbeg) * LDW + j]) ? 1 : 0;
+      }
+    }
+    if (!grid_barrier(sc.barrier, (unsigned)(j + 1) * nblk, status, abort_flag)) return;
+    // (c) every CTA selects the pivot: largest value, lowest index; NaN on the diagonal wins
+    if (threadIdx.x == 0) {
+      double v = -2.0;
+      int p = INT_MAX, wb = -1;
+      for (int q = 0; q < nblk; ++q) {
+        const double cv = ((volatile double *)sc.cand_val)[par * nblk + q];
+        const int ci = ((volatile int *)sc.cand_idx)[par * nblk + q];
+        if (ci != INT_MAX && better(cv, ci, v, p)) {
+          v = cv;
+          p = ci;
+          wb = q;
+        }
+      }
+      if (((volatile int *)sc.diag_nan)[par]) {
+        p = j;
+        wb = -1;
+      }
+      s_p = p;
+      red_i[0] = wb;
+    }
+    __syncthreads();
+    const int p = s_p, wb = red_i[0];
+    for (int c = threadIdx.x; c < W; c += blockDim.x) {
+      const double oj = ((volatile double *)sc.rowj)[par * W + c];
+      s_oldj[c] = oj;
+      s_prow[c] = (wb >= 0) ? ((volatile double *)sc.cand_row)[((size_t)par * nblk + wb) * W + c] : oj;
+    }
+    if (b == 0 && threadIdx.x == 0) piv[j] = row0 + p;
+    __syncthreads();
+    // (d) interchange rows j and p (pivot.go:27-35 on the panel columns)
+    if (p != j) {
+      if (j >= rbeg && j < rend)
+        for (int c = threadIdx.x; c < W; c += blockDim.x) S[(j - rbeg) * LDW + c] = s_prow[c];
+      if (p >= rbeg && p < rend)
+        for (int c = threadIdx.x; c < W; c += blockDim.x) S[(p - rbeg) * LDW + c] = s_oldj[c];
+    }
+    __syncthreads();
+    // (e) l = a_ij / u_jj (true division, mvec.go:422 InvScale), then rank-1 update
+    const double ujj = s_prow[j];
+    for (int r = threadIdx.x; r < nr; r += blockDim.x) {
+      const int gi = rbeg + r;
+      if (gi <= j) continue;
+      double *row = S + r * LDW;
+      const double l = row[j] / ujj;
+      row[j] = l;
+      for (int c = j + 1; c < W; ++c) row[c] = fma(-l, s_prow[c], row[c]);
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < nr * W; e += blockDim.x) {
+    const int r = e % nr, c = e / nr;
+    P[(rbeg + r) + (int64_t)c * ld] = S[r * LDW + c];
+  }
+}
+
+// Apply interchanges rows (r0+s) <-> piv[s] (absolute rows of A), s = 0..ns-1 in order,
+// to columns [0, ncols) of A; one thread per column.  Out-of-range pivots are reported.
+__global__ void laswp_kernel(double *A, int64_t ld, int rows, int ncols, const int64_t *piv,
+                             int ns, int64_t r0, int *status) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncols) return;
+  double *col = A + (int64_t)c * ld;
+  for (int s = 0; s < ns; ++s) {
+    const int64_t p = piv[s];
+    const int64_t q = r0 + s;
+    if (p <= 0 || p == q) continue;  // pivot.go:57: entries <= 0 are skipped
+    if (p >= rows || q >= rows) {
+      if (c == 0) set_status(status, MO_EINVAL);
+      continue;
+    }
+    const double t = col[q];
+    col[q] = col[p];
+    col[p] = t;
+  }
+}
+
+// piv[i] = v for i in [lo, hi)
+__global__ void fill_pivots_kernel(int64_t *piv, int64_t lo, int64_t hi, int64_t v) {
+  const int64_t i = lo + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < hi) piv[i] = v;
+}
+
+struct CtrlView {
+  int status;
+  int info;
+  double bad;
+};
+
+}  // namespace
+
+int laswp(mo_ctx *ctx, View A, int c0, int c1, const int64_t *piv, int ns, int64_t r0) {
+  if (c1 <= c0 || ns <= 0) return MO_OK;
+  const int nc = c1 - c0;
+  laswp_kernel<<<(nc + 127) / 128, 128, 0, ctx->stream>>>(
+      A.at(0, c0), A.ld, A.rows, nc, piv, ns, r0,
+      &reinterpret_cast<CtrlView *>(ctx->d_status)->status);
+  MO_CUDA_TRY(cudaGetLastError());
+  return MO_OK;
+}
+
+// SolveLU's applyPivots(B, pivots) (lu.go:485, pivot.go:55-61)
+int laswp_forward(mo_ctx *ctx, View B, const int64_t *piv, int64_t npiv) {
+  if (B.rows == 0 || B.cols == 0 || npiv <= 0) return MO_OK;
+  if (npiv > INT_MAX) return MO_EINVAL;
+  return laswp(ctx, B, 0, B.cols, piv, (int)npiv, 0);
+}
+
+int getrf(mo_ctx *ctx, View A, int64_t *piv, int64_t npiv, int ref_nb) {
+  const int m = A.rows, n = A.cols, mn = min(m, n);
+  int *status = &reinterpret_cast<CtrlView *>(ctx->d_status)->status;
+  // panel width and rows per CTA: keep the panel slice <= ~200 KB of shared memory
+  int W = MAX_PANEL_W;
+  const int max_blocks = ctx->sms;
+  auto rows_per_block = [&](int) {
+    int nblk = min(max_blocks, max(1, (m + 63) / 64));
+    return std::pair<int, int>((m + nblk - 1) / nblk, nblk);
+  };
+  auto smem_for = [](int R, int w) { return (size_t)R * (w + 1) * sizeof(double); };
+  auto rb = rows_per_block(W);
+  while (smem_for(rb.first, W) > 200 * 1024 && W > 8) {
+    W /= 2;
+    rb = rows_per_block(W);
+  }
+  if (smem_for(rb.first, W) > 200 * 1024) return MO_EINVAL;  // > ~3.2M rows
+  const int R = rb.first, nblk = rb.second;
+  // later (shorter) panels may use up to 64 rows per CTA
+  const size_t smem = smem_for(std::max(R, 64), W);
+  MO_CUDA_TRY(cudaFuncSetAttribute(lu_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+  int occ = 0;
+  MO_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, lu_panel_kernel, PANEL_THREADS,
+                                                            smem));
+  if (occ * ctx->sms < nblk) return MO_EINVAL;
+
+  // workspace: panel scratch + L11 inverse
+  const size_t sz_val = 2 * nblk * sizeof(double), sz_idx = 2 * nblk * sizeof(int);
+  const size_t sz_row = (size_t)2 * nblk * W * sizeof(double), sz_rowj = 2 * W * sizeof(double);
+  const size_t inv_bytes = 128 * 128 * sizeof(double);
+  const size_t total = inv_bytes + sz_val + sz_row + sz_rowj + sz_idx + 64 + 64;
+  char *ws = nullptr;
+  int rc = workspace(ctx, total, (void **)&ws);
+  if (rc) return rc;
+  double *inv = (double *)ws;
+  PanelScratch sc;
+  char *q = ws + inv_bytes;
+  sc.cand_val = (double *)q;
+  q += sz_val;
+  sc.cand_row = (double *)q;
+  q += sz_row;
+  sc.rowj = (double *)q;
+  q += sz_rowj;
+  sc.cand_idx = (int *)q;
+  q += sz_idx;
+  sc.diag_nan = (int *)q;
+  q += 16;
+  sc.barrier = (unsigned *)q;
+  q += 16;
+  int *abort_flag = (int *)q;
+
+  for (int k = 0; k < mn; k += W) {
+    const int b = min(W, mn - k);
+    // panel A[k:m, k:k+b]
+    MO_CUDA_TRY(cudaMemsetAsync(sc.barrier, 0, 32, ctx->stream));  // barrier + abort flag
+    View Pv = A.sub(k, k, m - k, b);
+    const int pm = m - k;
+    int pblk = min(nblk, max(1, (pm + 63) / 64));
+    int pR = (pm + pblk - 1) / pblk;
+    int64_t *pv = piv + k;
+    int64_t row0 = k;
+    double *pd = Pv.d;
+    int64_t pld = Pv.ld;
+    int pw = b;
+    void *args[] = {&pd, &pld, (void *)&pm, &pw, &pR, &pv, &row0, &sc, &status, &abort_flag};
+    MO_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)lu_panel_kernel, dim3(pblk),
+                                            dim3(PANEL_THREADS), args, smem, ctx->stream));
+    // interchanges on the columns left and right of the panel
+    if ((rc = laswp(ctx, A, 0, k, piv + k, b, k))) return rc;
+    if ((rc = laswp(ctx, A, k + b, n, piv + k, b, k))) return rc;
+    const int rest_c = n - k - b;
+    if (rest_c > 0) {
+      View L11 = A.sub(k, k, b, b);
+      if ((rc = trtri_blocks(ctx, L11, b, false, true, true, inv))) return rc;
+      View A12 = A.sub(k, k + b, b, rest_c);
+      if ((rc = gemm(ctx, A12, View{inv, b, b, 128}, false, A12, false, 1.0, 0.0))) return rc;
+      const int rest_r = m - k - b;
+      if (rest_r > 0) {
+        if ((rc = gemm(ctx, A.sub(k + b, k + b, rest_r, rest_c), A.sub(k + b, k, rest_r, b), false,
+                       A12, false, -1.0, 1.0)))
+          return rc;
+      }
+    }
+  }
+  // The reference's blocked path (mlen > nb, nb != 0) leaves the pivot entries past
+  // min(rows, cols) inside the last block equal to that block's start row (lu.go:381-383).
+  if (ref_nb > 0 && mn > ref_nb && npiv > mn) {
+    int64_t k_last = 0;
+    for (int64_t k = 0; k < m && k < n;) {
+      k_last = k;
+      k += (k + ref_nb > n) ? n - k : ref_nb;
+    }
+    const int64_t hi = std::min<int64_t>(npiv, k_last + ref_nb);
+    if (hi > mn)
+      fill_pivots_kernel<<<(unsigned)((hi - mn + 255) / 256), 256, 0, ctx->stream>>>(piv, mn, hi,
+                                                                                     k_last);
+    MO_CUDA_TRY(cudaGetLastError());
+  }
+  return MO_OK;
+}
+
+}  // namespace mo

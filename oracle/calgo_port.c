@@ -1,0 +1,247 @@
+/*
+ * oracle/calgo_port.c -- TEST INFRASTRUCTURE ONLY (the oracle), never product code.
+ *
+ * Plain-C restatement of the arithmetic of the reference's C kernels (hrautila/matops
+ * calgo/) that lie on the GEMM / SYRK / TRSM / Cholesky / LU path.  The reference uses
+ * SSE micro-kernels with packing buffers; this restatement keeps every semantic that
+ * changes results (where beta is applied and how beta==0/1 are special-cased, alpha
+ * applied after a blocked triangular solve, true division by pivots / diagonals, the
+ * SYRK beta quirk) and replaces the micro-kernels by scalar loops.  Summation order
+ * inside a dot product therefore differs from the SSE code; results agree to rounding.
+ *
+ * Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg load this code,
+ * and only as the checker.
+ */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include "calgo_iface.h"
+
+#define MAX_VP_ROWS 196 /* calgo/cmops.h:28 */
+#define MAX_VP_COLS 68  /* calgo/cmops.h:29 */
+
+#define AT(M, i, j) ((M)->md[(long)(i) + (long)(j) * (M)->step])
+
+/* calgo/vec_scale.c:114-140 (dscale_tile): f==1 -> untouched, f==0 -> zeros, else scale */
+static void scale_tile(double *X, int ldX, double f, int M, int N) {
+  if (f == 1.0) return;
+  for (int j = 0; j < N; j++)
+    for (int i = 0; i < M; i++) X[i + (long)j * ldX] = (f == 0.0) ? 0.0 : X[i + (long)j * ldX] * f;
+}
+
+/* calgo/vec_scale.c:94-111 (dscale_vec) */
+static void scale_vec(double *X, int inc, double f, int N) {
+  if (f == 1.0) return;
+  for (int i = 0; i < N; i++) X[(long)i * inc] = (f == 0.0) ? 0.0 : X[(long)i * inc] * f;
+}
+
+static inline double opA(const mdata_t *A, int flags, int i, int p) {
+  return (flags & MTX_TRANSA) ? AT(A, p, i) : AT(A, i, p);
+}
+static inline double opB(const mdata_t *B, int flags, int p, int j) {
+  return (flags & MTX_TRANSB) ? AT(B, j, p) : AT(B, p, j);
+}
+
+/* C[R:E, S:L] += alpha * sum_{p in [p0,p1)} opA(i,p) opB(p,j), one partial sum per panel
+ * (calgo/dmmat_gemm.c:309-360, the panel step _dblock_mult_gepp) */
+static void panel_update(mdata_t *C, const mdata_t *A, const mdata_t *B, double alpha, int flags,
+                         int p0, int p1, int S, int L, int R, int E) {
+  for (int j = S; j < L; j++)
+    for (int i = R; i < E; i++) {
+      double s = 0.0;
+      for (int p = p0; p < p1; p++) s += opA(A, flags, i, p) * opB(B, flags, p, j);
+      AT(C, i, j) += alpha * s;
+    }
+}
+
+/* calgo/dmmat_gemm.c:364-415: C = beta*C + alpha*op(A)*op(B) on rows [R,E) and columns
+ * [S,L); beta is applied per NB column block before its k-panels of length vlen. */
+void dmult_mm_blocked3(mdata_t *C, const mdata_t *A, const mdata_t *B, double alpha,
+                       double beta, int flags, int P, int S, int L, int R, int E, int vlen,
+                       int NB, int MB) {
+  (void)MB;
+  if (L - S <= 0 || E - R <= 0) return;
+  if (NB > MAX_VP_ROWS || NB <= 0) NB = MAX_VP_ROWS;
+  if (vlen > MAX_VP_ROWS || vlen <= 0) vlen = MAX_VP_ROWS;
+  for (int j = S; j < L; j += NB) {
+    int nJ = L - j < NB ? L - j : NB;
+    scale_tile(&AT(C, R, j), C->step, beta, E - R, nJ);
+    for (int k = 0; k < P; k += vlen) {
+      int nP = P - k < vlen ? P - k : vlen;
+      panel_update(C, A, B, alpha, flags, k, k + nP, j, j + nJ, R, E);
+    }
+  }
+}
+
+/* calgo/dmmat_rank.c:62-127 (dmmat_rank_blk) with _dmmat_rank_diag (:18-57).
+ * Diagonal NB x NB blocks: the triangle (upper if flags&UPPER, else lower) gets
+ * beta*C + alpha*op(A)op(A)^T.  Off-diagonal blocks (left of the diagonal block when
+ * flags&LOWER, right of it otherwise) get alpha*... added WITHOUT beta: the reference
+ * applies beta only inside the diagonal blocks, so only beta==1 gives BLAS SYRK. */
+void dmmat_rank_blk(mdata_t *C, const mdata_t *A, double alpha, double beta, int flags, int P,
+                    int S, int E, int vlen, int NB) {
+  (void)vlen;
+  if (E - S <= 0 || P <= 0) return;
+  if (NB > MAX_VP_COLS || NB <= 0) NB = MAX_VP_COLS;
+  if (NB > E - S) NB = E - S;
+  /* op(A)(i,p): A(i,p) normally, A(p,i) with TRANSA; C += alpha*op(A)*op(A)^T */
+  int ta = flags & MTX_TRANSA ? MTX_TRANSA : 0;
+  for (int i = S; i < E; i += NB) {
+    int nI = E - i < NB ? E - i : NB;
+    /* 1. diagonal block, row by row (dmmat_rank.c:28-56) */
+    for (int r = 0; r < nI; r++) {
+      int c0 = (flags & MTX_UPPER) ? r : 0;
+      int c1 = (flags & MTX_UPPER) ? nI : r + 1;
+      for (int c = c0; c < c1; c++) {
+        double *cij = &AT(C, i + r, i + c);
+        *cij = (beta == 1.0) ? *cij : (beta == 0.0 ? 0.0 : *cij * beta);
+        double s = 0.0;
+        for (int p = 0; p < P; p++) s += opA(A, ta, i + r, p) * opA(A, ta, i + c, p);
+        *cij += alpha * s;
+      }
+    }
+    /* 2. off-diagonal block (dmmat_rank.c:96-104 / :113-121), no beta */
+    int cs = (flags & MTX_LOWER) ? 0 : i + nI;
+    int ce = (flags & MTX_LOWER) ? i : E;
+    for (int c = cs; c < ce; c++)
+      for (int r = 0; r < nI; r++) {
+        double s = 0.0;
+        for (int p = 0; p < P; p++) s += opA(A, ta, i + r, p) * opA(A, ta, c, p);
+        AT(C, i + r, c) += alpha * s;
+      }
+  }
+}
+
+/* Triangular solves on B's columns [S,E) (LEFT) or rows [S,E) (RIGHT) with the N x N
+ * triangle of A.  calgo/dmmat_solve.c:864-908 dispatches to eight blocked variants
+ * (:464-862) that solve with alpha == 1 and scale by alpha at the end; the diagonal
+ * is divided (not multiplied by a reciprocal) unless UNIT (e.g. :171, :203).
+ * Upper is chosen iff flags&UPPER, right side iff flags&RIGHT. */
+void dmmat_solve_blk(mdata_t *B, const mdata_t *A, double alpha, int flags, int N, int S, int E,
+                     int NB) {
+  (void)NB;
+  if (E - S <= 0) return;
+  int unit = flags & MTX_UNIT, upper = flags & MTX_UPPER, tr = flags & MTX_TRANSA;
+  /* effective triangle of op(A): lower unless (upper xor trans) */
+  int lower_eff = upper ? (tr != 0) : (tr == 0);
+#define OPA(i, j) (tr ? AT(A, j, i) : AT(A, i, j))
+  if (flags & MTX_RIGHT) {
+    /* X * op(A) = B, rows r in [S,E): x_j = (b_j - sum_{k} x_k opA(k,j)) / opA(j,j) */
+    for (int r = S; r < E; r++) {
+      if (lower_eff) {
+        /* op(A) lower: column j depends on k > j -> go backwards */
+        for (int j = N - 1; j >= 0; j--) {
+          double s = AT(B, r, j);
+          for (int k = j + 1; k < N; k++) s -= AT(B, r, k) * OPA(k, j);
+          AT(B, r, j) = unit ? s : s / OPA(j, j);
+        }
+      } else {
+        for (int j = 0; j < N; j++) {
+          double s = AT(B, r, j);
+          for (int k = 0; k < j; k++) s -= AT(B, r, k) * OPA(k, j);
+          AT(B, r, j) = unit ? s : s / OPA(j, j);
+        }
+      }
+    }
+    if (alpha != 1.0)
+      for (int j = 0; j < N; j++) scale_vec(&AT(B, S, j), 1, alpha, E - S);
+  } else {
+    /* op(A) X = B, columns c in [S,E) */
+    for (int c = S; c < E; c++) {
+      if (lower_eff) {
+        for (int i = 0; i < N; i++) {
+          double s = AT(B, i, c);
+          for (int k = 0; k < i; k++) s -= OPA(i, k) * AT(B, k, c);
+          AT(B, i, c) = unit ? s : s / OPA(i, i);
+        }
+      } else {
+        for (int i = N - 1; i >= 0; i--) {
+          double s = AT(B, i, c);
+          for (int k = i + 1; k < N; k++) s -= OPA(i, k) * AT(B, k, c);
+          AT(B, i, c) = unit ? s : s / OPA(i, i);
+        }
+      }
+    }
+    if (alpha != 1.0) scale_tile(&AT(B, 0, S), B->step, alpha, N, E - S);
+  }
+#undef OPA
+}
+
+/* calgo/dmvec_rank.c:239-262 (dmvec_symv_rank, SYR): for columns c in [S,L)
+ * lower: rows c..L-1 ; upper: rows 0..c ; A(r,c) += x(r) * (alpha*x(c)) */
+void dmvec_symv_rank(mdata_t *A, const mvec_t *X, double alpha, int flags, int S, int L,
+                     int NB) {
+  (void)NB;
+  if (L - S <= 0) return;
+  for (int c = S; c < L; c++) {
+    double cf = alpha * X->md[(long)c * X->inc];
+    int r0 = (flags & MTX_UPPER) ? 0 : c;
+    int r1 = (flags & MTX_UPPER) ? c + 1 : L;
+    for (int r = r0; r < r1; r++) AT(A, r, c) += X->md[(long)r * X->inc] * cf;
+  }
+}
+
+/* calgo/dmvec_gemv.c:353-427 (dmult_gemv_blocked), the non-transposed form used on this
+ * path: per MB row block, y = beta*y (dscale_vec semantics), then y += alpha*A[:,S:L]*x. */
+void dmult_gemv_blocked(mvec_t *Y, const mdata_t *A, const mvec_t *X, double alpha, double beta,
+                        int flags, int S, int L, int R, int E, int vlen, int MB) {
+  (void)vlen;
+  if (L - S <= 0 || E - R <= 0) return;
+  if (flags & MTX_TRANSA) {
+    fprintf(stderr, "oracle: transposed GEMV is not on the restated path\n");
+    abort();
+  }
+  if (MB <= 0) MB = E - R;
+  for (int i = R; i < E; i += MB) {
+    int nI = E - i < MB ? E - i : MB;
+    if (beta != 1.0) scale_vec(&Y->md[(long)i * Y->inc], Y->inc, beta, nI);
+    for (int r = i; r < i + nI; r++) {
+      double s = 0.0;
+      for (int c = S; c < L; c++) s += AT(A, r, c) * X->md[(long)c * X->inc];
+      Y->md[(long)r * Y->inc] += alpha * s;
+    }
+  }
+}
+
+/* calgo/dmvec_solve.c:165-222 (dmvec_solve_blocked, TRSV): forward substitution when
+ * flags&LOWER, backward otherwise; TRANSA is not consulted by the reference. */
+void dmvec_solve_blocked(mvec_t *X, const mdata_t *A, int flags, int N, int NB) {
+  (void)NB;
+  int unit = flags & MTX_UNIT;
+  double *x = X->md;
+  long inc = X->inc;
+  if (flags & MTX_LOWER) {
+    for (int i = 0; i < N; i++) {
+      double s = x[i * inc];
+      for (int k = 0; k < i; k++) s -= AT(A, i, k) * x[k * inc];
+      x[i * inc] = unit ? s : s / AT(A, i, i);
+    }
+  } else {
+    for (int i = N - 1; i >= 0; i--) {
+      double s = x[i * inc];
+      for (int k = i + 1; k < N; k++) s -= AT(A, i, k) * x[k * inc];
+      x[i * inc] = unit ? s : s / AT(A, i, i);
+    }
+  }
+}
+
+/* calgo/dvec_util.c:46-67 (dvec_dot): alpha * sum x*y */
+double dvec_dot(const mvec_t *X, const mvec_t *Y, double alpha, int N) {
+  double s = 0.0;
+  for (int i = 0; i < N; i++) s += X->md[(long)i * X->inc] * Y->md[(long)i * Y->inc];
+  return alpha * s;
+}
+
+/* calgo/dvec_util.c:230-246 (dvec_invscal): x /= alpha, true division */
+void dvec_invscal(mvec_t *X, double alpha, int N) {
+  for (int i = 0; i < N; i++) X->md[(long)i * X->inc] /= alpha;
+}
+
+/* calgo/dvec_util.c:200-225 (dvec_swap) */
+void dvec_swap(mvec_t *X, mvec_t *Y, int N) {
+  for (int i = 0; i < N; i++) {
+    double t = X->md[(long)i * X->inc];
+    X->md[(long)i * X->inc] = Y->md[(long)i * Y->inc];
+    Y->md[(long)i * Y->inc] = t;
+  }
+}

@@ -1,0 +1,446 @@
+/*
+ * oracle/drivers.c -- TEST INFRASTRUCTURE ONLY (the oracle), never product code.
+ *
+ * C restatement of the Go layer of hrautila/matops on the level-3 / Cholesky / LU path:
+ * the BLAS-3 wrappers of mmult.go (Mult with its goroutine worker split, SolveTrm,
+ * RankUpdateSym), the level-1/2 wrappers of mvec.go used inside the panels, pivot.go,
+ * chol.go and lu.go, with the FLAME partitioning of partition.go turned into index
+ * arithmetic.  The same file is linked against oracle/calgo_port.c (this repository's
+ * restatement of the C kernels) and against the reference's own calgo C files (oracle/_ref).
+ *
+ * A FloatMatrix view (hrautila/matrix, not vendored) is column-major storage with a
+ * leading index; FloatArray()[0] is the view's (0,0) (inferred from mmult.go:228-233).
+ *
+ * Return codes mirror the Go error values: 0 = nil error, negative = the error string
+ * listed at OR_E*, positive k+1 = the panic "illegal value at k" of chol.go:34-36.
+ */
+#include <math.h>
+#include <pthread.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include "calgo_iface.h"
+
+enum {
+  OR_OK = 0,
+  OR_ESIZE = -1,        /* "Mult: size mismatch"             mmult.go:224 */
+  OR_ENOTSQUARE = -2,   /* "A not a square matrix"           chol.go:119 */
+  OR_EPIVLEN = -3,      /* "pivot array < min(A.Rows(),A.Cols())" lu.go:424 */
+  OR_ECNOTSQUARE = -4,  /* "C not a square matrix"           mmult.go:428 */
+  OR_EABSIZE = -5,      /* "A, B size mismatch"              mmult.go:406 */
+  OR_ENOTVECTOR = -6    /* "X not a vector." / "Y not a vector."  mvec.go:34-37 */
+};
+
+/* package globals, mmult.go:33-41 */
+static int vpLen = 196, nB = 68, mB = 68;
+static int nWorker = 1;
+static const int64_t limitOne = 200LL * 200 * 200;
+
+typedef struct { double *d; int r, c, ld; } fm;
+
+static inline fm sub(fm A, int i, int j, int nr, int nc) {
+  fm s = {A.d + (intptr_t)i + (intptr_t)j * A.ld, nr, nc, A.ld};
+  return s;
+}
+static inline fm sub2(fm A, int i, int j) { return sub(A, i, j, A.r - i, A.c - j); }
+static inline int is_vector(fm X) { return X.r == 1 || X.c == 1; }
+static inline int imin(int a, int b) { return a < b ? a : b; }
+
+typedef struct { int64_t *p; int n; } pv;
+static inline pv pslice(pv P, int a, int b) { pv s = {P.p + a, b - a}; return s; }
+
+/* ---------------- mvec.go wrappers used by the panels ---------------- */
+
+/* mvec.go:422-436 */
+static void InvScale(fm X, double alpha) {
+  int n = X.r * X.c;
+  if (n == 0 || !is_vector(X)) return;
+  mvec_t x = {X.d, X.c != 1 ? X.ld : 1};
+  dvec_invscal(&x, alpha, n);
+}
+
+/* mvec.go:101-121 */
+static int MVRankUpdateSym(fm A, fm X, double alpha, int flags) {
+  if (A.r == 0 || A.c == 0) return OR_OK;
+  if (!is_vector(X)) return OR_ENOTVECTOR;
+  mdata_t a = {A.d, A.ld};
+  mvec_t x = {X.d, X.r == 1 ? X.ld : 1};
+  dmvec_symv_rank(&a, &x, alpha, flags, 0, A.c, nB);
+  return OR_OK;
+}
+
+/* mvec.go:203-222 (alpha is not used by the reference) */
+static int MVSolveTrm(fm X, fm A, double alpha, int flags) {
+  (void)alpha;
+  if (A.r == 0 || A.c == 0) return OR_OK;
+  if (!is_vector(X)) return OR_ENOTVECTOR;
+  mdata_t a = {A.d, A.ld};
+  mvec_t x = {X.d, X.r == 1 ? X.ld : 1};
+  dmvec_solve_blocked(&x, &a, flags, A.c, nB);
+  return OR_OK;
+}
+
+/* mvec.go:28-60 */
+static int MVMult(fm Y, fm A, fm X, double alpha, double beta, int flags) {
+  if (A.r == 0 || A.c == 0) return OR_OK;
+  if (!is_vector(Y) || !is_vector(X)) return OR_ENOTVECTOR;
+  mdata_t a = {A.d, A.ld};
+  mvec_t y = {Y.d, Y.r == 1 ? Y.ld : 1};
+  mvec_t x = {X.d, X.r == 1 ? X.ld : 1};
+  dmult_gemv_blocked(&y, &a, &x, alpha, beta, flags, 0, X.r * X.c, 0, Y.r * Y.c, vpLen, mB);
+  return OR_OK;
+}
+
+/* mvec.go:274-297 with calgo/cmops.go:517-537 (N<=0 -> 0) */
+static double Dot(fm X, fm Y, double alpha) {
+  if (!is_vector(X) || !is_vector(Y)) return NAN;
+  int n = X.r * X.c;
+  if (n <= 0) return 0.0;
+  mvec_t x = {X.d, X.c != 1 ? X.ld : 1};
+  mvec_t y = {Y.d, Y.c != 1 ? Y.ld : 1};
+  return dvec_dot(&x, &y, alpha, n);
+}
+
+/* mvec.go:456-482 */
+static void Swap(fm X, fm Y) {
+  if (X.r * X.c == 0 || Y.r * Y.c == 0) return;
+  if (!is_vector(X) || !is_vector(Y)) return;
+  mvec_t x = {X.d, X.c != 1 ? X.ld : 1};
+  mvec_t y = {Y.d, Y.c != 1 ? Y.ld : 1};
+  dvec_swap(&x, &y, X.r * X.c);
+}
+
+/* ---------------- pivot.go ---------------- */
+
+/* pivot.go:27-35 */
+static void swapRows(fm A, int src, int dst) {
+  if (src == dst || A.r == 0) return;
+  Swap(sub(A, src, 0, 1, A.c), sub(A, dst, 0, 1, A.c));
+}
+
+/* pivot.go:55-61: forward order, entries <= 0 skipped */
+static void applyPivots(fm A, pv p) {
+  for (int k = 0; k < p.n; k++)
+    if (p.p[k] > 0) swapRows(A, (int)p.p[k], k);
+}
+
+/* pivot.go:98-107: first index of the strict maximum of |x|, scanning from row 0 */
+static void pivotIndex(fm A, pv p) {
+  double max = fabs(A.d[0]);
+  for (int k = 1; k < A.r; k++) {
+    double v = fabs(A.d[k]);
+    if (v > max) {
+      p.p[0] = k;
+      max = v;
+    }
+  }
+}
+
+/* ---------------- mmult.go BLAS-3 wrappers ---------------- */
+
+/* mmult.go:105-110 */
+static int blockIndex4(int i, int r, int sz) {
+  if (i == r) return sz;
+  int v = (int)((int64_t)i * sz / r);
+  return v - (v & 0x3);
+}
+
+/* mmult.go:137-167 */
+static void divideWork(int rows, int cols, int workers, int *colW, int *rowW) {
+  int nwsqrt = (int)sqrt((double)workers);
+  int issquare = nwsqrt * nwsqrt == workers;
+  if (workers == 2 || (workers & 0x1) != 0) {
+    if (cols > rows) { *colW = workers; *rowW = 1; }
+    else { *rowW = workers; *colW = 1; }
+  } else if (issquare) {
+    *colW = nwsqrt; *rowW = nwsqrt;
+  } else {
+    if (cols > rows) { *rowW = 2; *colW = workers / 2; }
+    else { *colW = 2; *rowW = workers / 2; }
+  }
+}
+
+typedef struct {
+  mdata_t C, A, B;
+  double alpha, beta;
+  int flags, P, S, L, R, E;
+} mult_task;
+
+static void *mult_worker(void *arg) {
+  mult_task *t = (mult_task *)arg;
+  dmult_mm_blocked3(&t->C, &t->A, &t->B, t->alpha, t->beta, t->flags, t->P, t->S, t->L, t->R,
+                    t->E, vpLen, nB, mB);
+  return NULL;
+}
+
+/* mmult.go:198-256 */
+int or_mult_fm(fm C, fm A, fm B, double alpha, double beta, int flags) {
+  int ar = A.r, ac = A.c, br = B.r, bc = B.c, cr = C.r, cc = C.c, ok, empty;
+  switch (flags & (MTX_TRANSA | MTX_TRANSB)) {
+    case MTX_TRANSA | MTX_TRANSB: empty = ac == 0 || br == 0; ok = cr == ac && cc == br && ar == bc; break;
+    case MTX_TRANSA: empty = ac == 0 || bc == 0; ok = cr == ac && cc == bc && ar == br; break;
+    case MTX_TRANSB: empty = ar == 0 || br == 0; ok = cr == ar && cc == br && ac == bc; break;
+    default: empty = ar == 0 || bc == 0; ok = cr == ar && cc == bc && ac == br;
+  }
+  if (empty) return OR_OK;
+  if (!ok) return OR_ESIZE;
+  int64_t psize = (int64_t)C.r * C.c * (int64_t)A.c;
+  int P = (flags & MTX_TRANSA) ? A.r : A.c;
+  mult_task base = {{C.d, C.ld}, {A.d, A.ld}, {B.d, B.ld}, alpha, beta, flags, P, 0, C.c, 0, C.r};
+  if (nWorker <= 1 || psize <= limitOne) {
+    mult_worker(&base);
+    return OR_OK;
+  }
+  int colW, rowW;
+  divideWork(C.r, C.c, nWorker, &colW, &rowW);
+  int nt = colW * rowW;
+  mult_task *tasks = (mult_task *)malloc(sizeof(mult_task) * nt);
+  pthread_t *th = (pthread_t *)malloc(sizeof(pthread_t) * nt);
+  int t = 0;
+  /* mmult.go:171-188 (scheduleWork) */
+  for (int k = 0; k < colW; k++)
+    for (int l = 0; l < rowW; l++, t++) {
+      tasks[t] = base;
+      tasks[t].S = blockIndex4(k, colW, C.c);
+      tasks[t].L = blockIndex4(k + 1, colW, C.c);
+      tasks[t].R = blockIndex4(l, rowW, C.r);
+      tasks[t].E = blockIndex4(l + 1, rowW, C.r);
+      pthread_create(&th[t], NULL, mult_worker, &tasks[t]);
+    }
+  for (t = 0; t < nt; t++) pthread_join(th[t], NULL);
+  free(tasks);
+  free(th);
+  return OR_OK;
+}
+
+/* mmult.go:388-422 */
+int or_solve_trm_fm(fm B, fm A, double alpha, int flags) {
+  int ok = 1, empty = 0, br = B.r, bc = B.c, ar = A.r, ac = A.c;
+  switch (flags & (MTX_LEFT | MTX_RIGHT)) {
+    case MTX_LEFT: empty = br == 0; ok = br == ac && ac == ar; break;
+    case MTX_RIGHT: empty = bc == 0; ok = bc == ar && ac == ar; break;
+  }
+  if (empty) return OR_OK;
+  if (!ok) return OR_EABSIZE;
+  int E = (flags & MTX_RIGHT) ? br : bc;
+  /* calgo/cmops.go:195-215 (DSolveBlk): N == 0 or an empty range returns */
+  if (ac == 0 || E <= 0) return OR_OK;
+  mdata_t b = {B.d, B.ld}, a = {A.d, A.ld};
+  dmmat_solve_blk(&b, &a, alpha, flags, ac, 0, E, nB);
+  return OR_OK;
+}
+
+/* mmult.go:426-445 */
+int or_rank_update_sym_fm(fm C, fm A, double alpha, double beta, int flags) {
+  if (C.r != C.c) return OR_ECNOTSQUARE;
+  int P = (flags & MTX_TRANSA) ? A.r : A.c;
+  /* calgo/cmops.go:219-240 (DSymmRankBlk) */
+  if (P == 0 || C.r <= 0) return OR_OK;
+  mdata_t c = {C.d, C.ld}, a = {A.d, A.ld};
+  dmmat_rank_blk(&c, &a, alpha, beta, flags, P, 0, C.r, vpLen, nB);
+  return OR_OK;
+}
+
+/* ---------------- chol.go ---------------- */
+
+/* chol.go:17-56 (unblockedCHOL); returns k+1 for the panic at absolute column k */
+static int unblockedCHOL(fm A, int flags, int nr) {
+  for (int k = 0; k < A.r; k++) {
+    fm a11 = sub(A, k, k, 1, 1);
+    double aval = sqrt(a11.d[0]);
+    if (isnan(aval)) return nr + k + 1;
+    a11.d[0] = aval;
+    fm A22 = sub2(A, k + 1, k + 1);
+    if (flags & MTX_LOWER) {
+      fm a21 = sub(A, k + 1, k, A.r - k - 1, 1);
+      InvScale(a21, aval);
+      MVRankUpdateSym(A22, a21, -1.0, flags);
+    } else {
+      fm a12 = sub(A, k, k + 1, 1, A.c - k - 1);
+      InvScale(a12, aval);
+      MVRankUpdateSym(A22, a12, -1.0, flags);
+    }
+  }
+  return OR_OK;
+}
+
+/* chol.go:58-94 (blockedCHOL) */
+static int blockedCHOL(fm A, int flags, int nb) {
+  for (int k = 0; k < A.r && k < A.c; ) {
+    int b = (k + nb > A.c) ? A.c - k : nb;
+    fm A11 = sub(A, k, k, b, b);
+    int err = unblockedCHOL(A11, flags, k);
+    if (err > 0) return err; /* the Go code panics here */
+    fm A22 = sub2(A, k + b, k + b);
+    if (flags & MTX_LOWER) {
+      fm A21 = sub(A, k + b, k, A.r - k - b, b);
+      or_solve_trm_fm(A21, A11, 1.0, MTX_RIGHT | MTX_LOWER | MTX_TRANSA);
+      or_rank_update_sym_fm(A22, A21, -1.0, 1.0, MTX_LOWER);
+    } else {
+      fm A12 = sub(A, k, k + b, b, A.c - k - b);
+      or_solve_trm_fm(A12, A11, 1.0, MTX_UPPER | MTX_TRANSA);
+      or_rank_update_sym_fm(A22, A12, -1.0, 1.0, MTX_UPPER | MTX_TRANSA);
+    }
+    k += b;
+  }
+  return OR_OK;
+}
+
+/* chol.go:116-127 */
+int or_decompose_chol_fm(fm A, int flags, int nb) {
+  if (A.c != A.r) return OR_ENOTSQUARE;
+  if (A.c < nb || nb == 0) return unblockedCHOL(A, flags, 0);
+  return blockedCHOL(A, flags, nb);
+}
+
+/* chol.go:147-158 */
+void or_solve_chol_fm(fm B, fm A, int flags) {
+  if (flags & MTX_UPPER) {
+    or_solve_trm_fm(B, A, 1.0, MTX_UPPER | MTX_TRANSA);
+    or_solve_trm_fm(B, A, 1.0, MTX_UPPER);
+  } else if (flags & MTX_LOWER) {
+    or_solve_trm_fm(B, A, 1.0, MTX_LOWER);
+    or_solve_trm_fm(B, A, 1.0, MTX_LOWER | MTX_TRANSA);
+  }
+}
+
+/* ---------------- lu.go ---------------- */
+
+/* lu.go:103-171 (unblockedLUpiv): left-looking column step */
+static int unblockedLUpiv(fm A, pv p) {
+  int k = 0;
+  for (; k < A.r && k < A.c; k++) {
+    fm A00 = sub(A, 0, 0, k, k);
+    fm a01 = sub(A, 0, k, k, 1);
+    fm a10 = sub(A, k, 0, 1, k);
+    fm a11 = sub(A, k, k, 1, 1);
+    fm A20 = sub(A, k + 1, 0, A.r - k - 1, k);
+    fm a21 = sub(A, k + 1, k, A.r - k - 1, 1);
+    fm a1 = sub(A, 0, k, A.r, 1);
+    pv p0 = pslice(p, 0, k);
+    pv p1 = pslice(p, k, imin(k + 1, p.n));
+    if (p1.n == 0) return OR_EPIVLEN; /* the Go code would index past the slice */
+
+    applyPivots(a1, p0);
+    MVSolveTrm(a01, A00, 1.0, MTX_LOWER | MTX_UNIT);
+    a11.d[0] += Dot(a10, a01, -1.0);
+    MVMult(a21, A20, a01, -1.0, 1.0, MTX_NOTRANS);
+
+    fm aB1 = sub(A, k, k, A.r - k, 1);
+    pivotIndex(aB1, p1);
+    applyPivots(aB1, p1);
+    InvScale(a21, a11.d[0]);
+    fm AB0 = sub(A, k, 0, A.r - k, k);
+    applyPivots(AB0, p1);
+    p1.p[0] += k;
+  }
+  if (k < A.c) {
+    fm ATR = sub(A, 0, k, k, A.c - k);
+    fm ATL = sub(A, 0, 0, k, k);
+    applyPivots(ATR, p);
+    or_solve_trm_fm(ATR, ATL, 1.0, MTX_LEFT | MTX_UNIT | MTX_LOWER);
+  }
+  return OR_OK;
+}
+
+/* lu.go:173-231 (blockedLUpiv): left-looking (Crout) blocked variant */
+static int blockedLUpiv(fm A, pv p, int nb) {
+  int k = 0;
+  while (k < A.r && k < A.c) {
+    int b = (k + nb > A.c) ? A.c - k : nb;                  /* partition.go:252-254 */
+    int pb = (k + nb > p.n) ? p.n - k : nb;                  /* partition.go:386-388 */
+    fm A00 = sub(A, 0, 0, k, k);
+    fm A01 = sub(A, 0, k, k, b);
+    fm A10 = sub(A, k, 0, b, k);
+    fm A11 = sub(A, k, k, b, b);
+    fm A20 = sub(A, k + b, 0, A.r - k - b, k);
+    fm A21 = sub(A, k + b, k, A.r - k - b, b);
+    fm A1 = sub(A, 0, k, A.r, b);
+    pv p0 = pslice(p, 0, k);
+    pv p1 = pslice(p, k, k + pb);
+
+    applyPivots(A1, p0);
+    or_solve_trm_fm(A01, A00, 1.0, MTX_LOWER | MTX_UNIT);
+    or_mult_fm(A11, A10, A01, -1.0, 1.0, MTX_NOTRANS);
+    or_mult_fm(A21, A20, A01, -1.0, 1.0, MTX_NOTRANS);
+
+    fm AB1 = sub(A, k, k, A.r - k, A11.c);
+    unblockedLUpiv(AB1, p1);
+    fm AB0 = sub(A, k, 0, A.r - k, k);
+    applyPivots(AB0, p1);
+    for (int i = 0; i < p1.n; i++) p1.p[i] += k;
+    k += b;
+  }
+  if (k < A.c) {
+    fm ATR = sub(A, 0, k, k, A.c - k);
+    fm ATL = sub(A, 0, 0, k, k);
+    applyPivots(ATR, p);
+    or_solve_trm_fm(ATR, ATL, 1.0, MTX_LEFT | MTX_UNIT | MTX_LOWER);
+  }
+  return OR_OK;
+}
+
+/* lu.go:257-272 */
+int or_decompose_lu_fm(fm A, pv p, int nb) {
+  int mlen = imin(A.r, A.c);
+  if (p.n < mlen) return OR_EPIVLEN;
+  for (int k = 0; k < p.n; k++) p.p[k] = 0;
+  if (mlen <= nb || nb == 0) return unblockedLUpiv(A, p);
+  return blockedLUpiv(A, p, nb);
+}
+
+/* lu.go:320-331 */
+int or_solve_lu_fm(fm B, fm A, pv p, int flags) {
+  applyPivots(B, p);
+  if (flags & MTX_TRANSA) {
+    or_solve_trm_fm(B, A, 1.0, MTX_LOWER | MTX_UNIT | MTX_TRANSA);
+    or_solve_trm_fm(B, A, 1.0, MTX_UPPER | MTX_TRANSA);
+  } else {
+    or_solve_trm_fm(B, A, 1.0, MTX_LOWER | MTX_UNIT);
+    or_solve_trm_fm(B, A, 1.0, MTX_UPPER);
+  }
+  return OR_OK;
+}
+
+/* ---------------- flat C entry points for the ctypes harness ---------------- */
+
+#define FM(p, r, c, ld) ((fm){(p), (r), (c), (ld)})
+
+int or_mult(double *C, int cr, int cc, int ldc, double *A, int ar, int ac, int lda, double *B,
+            int br, int bc, int ldb, double alpha, double beta, int flags) {
+  return or_mult_fm(FM(C, cr, cc, ldc), FM(A, ar, ac, lda), FM(B, br, bc, ldb), alpha, beta, flags);
+}
+int or_rank_update_sym(double *C, int cr, int cc, int ldc, double *A, int ar, int ac, int lda,
+                       double alpha, double beta, int flags) {
+  return or_rank_update_sym_fm(FM(C, cr, cc, ldc), FM(A, ar, ac, lda), alpha, beta, flags);
+}
+int or_solve_trm(double *B, int br, int bc, int ldb, double *A, int ar, int ac, int lda,
+                 double alpha, int flags) {
+  return or_solve_trm_fm(FM(B, br, bc, ldb), FM(A, ar, ac, lda), alpha, flags);
+}
+int or_decompose_chol(double *A, int ar, int ac, int lda, int flags, int nb) {
+  return or_decompose_chol_fm(FM(A, ar, ac, lda), flags, nb);
+}
+int or_decompose_lu(double *A, int ar, int ac, int lda, int64_t *piv, int npiv, int nb) {
+  pv p = {piv, npiv};
+  return or_decompose_lu_fm(FM(A, ar, ac, lda), p, nb);
+}
+void or_solve_chol(double *B, int br, int bc, int ldb, double *A, int ar, int ac, int lda, int flags) {
+  or_solve_chol_fm(FM(B, br, bc, ldb), FM(A, ar, ac, lda), flags);
+}
+int or_solve_lu(double *B, int br, int bc, int ldb, double *A, int ar, int ac, int lda, int64_t *piv,
+                int npiv, int flags) {
+  pv p = {piv, npiv};
+  return or_solve_lu_fm(FM(B, br, bc, ldb), FM(A, ar, ac, lda), p, flags);
+}
+/* mmult.go:69-73 */
+int or_num_workers(int n) {
+  int old = nWorker;
+  nWorker = n;
+  return old;
+}
+/* mmult.go:63-67 */
+void or_blocking_params(int mb, int nb, int kb) {
+  vpLen = kb;
+  nB = nb;
+  mB = mb;
+}

@@ -1,0 +1,114 @@
+"""Oracle loader -- TEST INFRASTRUCTURE ONLY.
+
+ctypes access to the CPU restatement of hrautila/matops's level-3 / Cholesky / LU path
+(oracle/drivers.c over oracle/calgo_port.c) and, when it was built here, to the same
+drivers over the reference's own C kernels (oracle/_ref/libmatops_ref.so).
+
+Matrices are numpy float64 arrays in column-major (Fortran) layout; a slice of such an
+array is a view with the parent's leading dimension, exactly like a FloatMatrix view
+(hrautila/matrix SubMatrix).  Only tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline use this module, and only as the checker.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_LIB = os.path.join(HERE, "_build", "liboracle_port.so")
+REF_LIB = os.path.join(HERE, "_ref", "libmatops_ref.so")
+
+# flag values, calgo/cmops.go:19-31
+TRANSA, TRANSB, LOWER, UPPER, LEFT, RIGHT, UNIT, TRANS = 0x1, 0x2, 0x4, 0x8, 0x10, 0x20, 0x40, 0x80
+NOTRANS = 0
+
+ERRORS = {
+    -1: "Mult: size mismatch",
+    -2: "A not a square matrix",
+    -3: "pivot array < min(A.Rows(),A.Cols())",
+    -4: "C not a square matrix",
+    -5: "A, B size mismatch",
+    -6: "X not a vector.",
+}
+
+
+def build(ref: bool = False) -> None:
+    """Compile the oracle (and, with ref=True, the reference's own kernels) via make."""
+    targets = ["port"] + (["ref"] if ref else [])
+    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+
+
+def view(a: np.ndarray):
+    """(pointer, rows, cols, ld) of a column-major float64 matrix view."""
+    if a.ndim != 2 or a.dtype != np.float64:
+        raise TypeError("expected a 2-D float64 array")
+    r, c = a.shape
+    if r > 1 and a.strides[0] != 8:
+        raise TypeError("matrix view must be column-major (unit row stride)")
+    ld = a.strides[1] // 8 if c > 1 or a.strides[1] // 8 >= r else max(r, 1)
+    ld = max(ld, 1)
+    return ctypes.c_void_p(a.ctypes.data), r, c, ld
+
+
+class Oracle:
+    """The restated Go API over one of the two kernel libraries."""
+
+    def __init__(self, which: str = "port"):
+        path = PORT_LIB if which == "port" else REF_LIB
+        if not os.path.exists(path):
+            if which == "port":
+                build()
+            else:
+                raise FileNotFoundError(f"{path} not built (needs the reference sources)")
+        self.which = which
+        L = self.lib = ctypes.CDLL(path)
+        d, i, p = ctypes.c_double, ctypes.c_int, ctypes.c_void_p
+        M = [p, i, i, i]
+        L.or_mult.argtypes = M + M + M + [d, d, i]
+        L.or_rank_update_sym.argtypes = M + M + [d, d, i]
+        L.or_solve_trm.argtypes = M + M + [d, i]
+        L.or_decompose_chol.argtypes = M + [i, i]
+        L.or_decompose_lu.argtypes = M + [p, i, i]
+        L.or_solve_chol.argtypes = M + M + [i]
+        L.or_solve_chol.restype = None
+        L.or_solve_lu.argtypes = M + M + [p, i, i]
+        L.or_num_workers.argtypes = [i]
+        L.or_blocking_params.argtypes = [i, i, i]
+        L.or_blocking_params.restype = None
+
+    # each method returns the raw status code (0 = nil error)
+    def Mult(self, C, A, B, alpha, beta, flags):
+        return self.lib.or_mult(*view(C), *view(A), *view(B), alpha, beta, flags)
+
+    def RankUpdateSym(self, C, A, alpha, beta, flags):
+        return self.lib.or_rank_update_sym(*view(C), *view(A), alpha, beta, flags)
+
+    def SolveTrm(self, B, A, alpha, flags):
+        return self.lib.or_solve_trm(*view(B), *view(A), alpha, flags)
+
+    def DecomposeCHOL(self, A, flags, nb):
+        return self.lib.or_decompose_chol(*view(A), flags, nb)
+
+    def DecomposeLU(self, A, pivots: np.ndarray, nb):
+        assert pivots.dtype == np.int64 and pivots.flags.c_contiguous
+        return self.lib.or_decompose_lu(*view(A), ctypes.c_void_p(pivots.ctypes.data), len(pivots), nb)
+
+    def SolveCHOL(self, B, A, flags):
+        self.lib.or_solve_chol(*view(B), *view(A), flags)
+
+    def SolveLU(self, B, A, pivots: np.ndarray, flags):
+        assert pivots.dtype == np.int64 and pivots.flags.c_contiguous
+        return self.lib.or_solve_lu(*view(B), *view(A), ctypes.c_void_p(pivots.ctypes.data), len(pivots), flags)
+
+    def NumWorkers(self, n: int) -> int:
+        return self.lib.or_num_workers(n)
+
+    def BlockingParams(self, mb: int, nb: int, kb: int) -> None:
+        self.lib.or_blocking_params(mb, nb, kb)
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB)

@@ -1,0 +1,164 @@
+"""CPU: the oracle (restated Go drivers + restated C kernels) against the reference.
+
+1. golden.npz holds outputs of the reference's own C kernels (tests/golden/make_golden.py);
+   the restatement must reproduce them (pivots exactly, values to rounding).
+2. when oracle/_ref is built, port and reference are also compared on fresh inputs.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from util import EPS, colmajor, even_ld, fro, spd
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "golden.npz")
+TA, TB, LO, UP, LEFT, RIGHT, UNIT = 0x1, 0x2, 0x4, 0x8, 0x10, 0x20, 0x40
+
+
+@pytest.fixture(scope="module")
+def golden():
+    z = np.load(GOLDEN)
+    cases = {}
+    for k in z.files:
+        name, field = k.split("/")
+        cases.setdefault(name, {})[field] = z[k]
+    return cases
+
+
+def F(a):
+    return colmajor(a, ld=even_ld(a.shape[0]))
+
+
+def names(prefix):
+    z = np.load(GOLDEN)
+    return sorted({k.split("/")[0] for k in z.files if k.startswith(prefix)})
+
+
+def rel(a, b):
+    return fro(a - b) / max(fro(b), 1e-300)
+
+
+@pytest.mark.parametrize("name", names("mult_"))
+def test_golden_mult(oracle, golden, name):
+    c = golden[name]
+    R = F(c["C"])
+    assert oracle.Mult(R, F(c["A"]), F(c["B"]), float(c["alpha"]), float(c["beta"]), int(c["flags"])) == 0
+    assert rel(R, c["R"]) <= 1e-14
+
+
+@pytest.mark.parametrize("name", names("syrk_"))
+def test_golden_rank_update_sym(oracle, golden, name):
+    c = golden[name]
+    R = F(c["C"])
+    assert oracle.RankUpdateSym(R, F(c["A"]), float(c["alpha"]), float(c["beta"]), int(c["flags"])) == 0
+    assert rel(R, c["R"]) <= 1e-14
+
+
+@pytest.mark.parametrize("name", names("trsm_") + names("ka_trsm_"))
+def test_golden_solve_trm(oracle, golden, name):
+    c = golden[name]
+    X = F(c["B"])
+    assert oracle.SolveTrm(X, F(c["A"]), float(c["alpha"]), int(c["flags"])) == 0
+    assert rel(X, c["X"]) <= 1e-13
+
+
+@pytest.mark.parametrize("name", names("chol_") + names("ka_chol"))
+def test_golden_chol(oracle, golden, name):
+    c = golden[name]
+    L = F(c["A"])
+    assert oracle.DecomposeCHOL(L, int(c["flags"]), int(c["nb"])) == 0
+    assert rel(L, c["L"]) <= 1e-13
+    if "Lexact" in c:  # decomp_test.go:150-163: chol(L L^T) recovers L
+        assert np.allclose(np.tril(L), c["Lexact"], rtol=1e-5, atol=1e-8)
+    if "B" in c:
+        X = F(c["B"])
+        oracle.SolveCHOL(X, L, int(c["flags"]))
+        assert rel(X, c["X"]) <= 1e-12
+
+
+@pytest.mark.parametrize("name", names("lu_") + names("ka_lu"))
+def test_golden_lu(oracle, golden, name):
+    c = golden[name]
+    LU = F(c["A"])
+    p = np.zeros(len(c["piv"]), np.int64)
+    assert oracle.DecomposeLU(LU, p, int(c["nb"])) == 0
+    assert np.array_equal(p, c["piv"])
+    assert rel(LU, c["LU"]) <= 1e-12
+    for tr in (0, TA):
+        if f"B{tr}" in c:
+            X = F(c[f"B{tr}"])
+            assert oracle.SolveLU(X, LU, p, tr) == 0
+            assert rel(X, c[f"X{tr}"]) <= 1e-11
+
+
+def test_golden_lu3x3_matches_lapack(golden):
+    """decomp_test.go:85-108 compares against lapack.Getrf: pivots are LAPACK's minus one."""
+    import scipy.linalg as sl
+    c = golden["ka_lu3x3"]
+    lu, piv = sl.lu_factor(c["A"])
+    assert np.array_equal(piv, c["piv"])
+    assert np.allclose(lu, c["LU"], rtol=1e-12, atol=1e-14)
+
+
+# ---- port vs the reference's own kernels on fresh inputs ----
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_port_vs_ref_factorizations(oracle, ref_oracle, seed):
+    rng = np.random.default_rng(seed)
+    for n, nb in [(97, 16), (150, 68), (64, 0)]:
+        A = F(spd(rng, n))
+        a1, a2 = F(A), F(A)
+        assert oracle.DecomposeCHOL(a1, LO, nb) == ref_oracle.DecomposeCHOL(a2, LO, nb) == 0
+        assert rel(a1, a2) <= 1e-13
+        G = F(rng.standard_normal((n, n)))
+        g1, g2 = F(G), F(G)
+        p1, p2 = np.zeros(n, np.int64), np.zeros(n, np.int64)
+        oracle.DecomposeLU(g1, p1, nb)
+        ref_oracle.DecomposeLU(g2, p2, nb)
+        assert np.array_equal(p1, p2)
+        assert rel(g1, g2) <= 1e-11
+
+
+def test_port_vs_ref_mult_workers(oracle, ref_oracle):
+    """Mult's goroutine split (mmult.go:137-255) restated with threads: same result."""
+    rng = np.random.default_rng(7)
+    m, n, k = 300, 260, 250
+    A, B, C = F(rng.uniform(-1, 1, (m, k))), F(rng.uniform(-1, 1, (k, n))), F(rng.uniform(-1, 1, (m, n)))
+    outs = []
+    for o in (oracle, ref_oracle):
+        for w in (1, 4, 6):
+            old = o.NumWorkers(w)
+            R = F(C)
+            assert o.Mult(R, A, B, 1.5, -0.5, 0) == 0
+            o.NumWorkers(old)
+            outs.append(R)
+    for R in outs[1:]:
+        assert rel(R, outs[0]) <= 4 * k * EPS
+
+
+def test_oracle_errors(oracle):
+    assert oracle.Mult(F(np.zeros((3, 3))), F(np.zeros((3, 2))), F(np.zeros((3, 3))), 1, 1, 0) == -1
+    assert oracle.DecomposeCHOL(F(np.zeros((3, 4))), LO, 0) == -2
+    assert oracle.DecomposeLU(F(np.zeros((4, 4))), np.zeros(3, np.int64), 0) == -3
+    assert oracle.RankUpdateSym(F(np.zeros((3, 4))), F(np.zeros((3, 2))), 1, 1, LO) == -4
+    assert oracle.SolveTrm(F(np.zeros((3, 2))), F(np.eye(4)), 1, LEFT) == -5
+    A = spd(np.random.default_rng(0), 50)
+    A[20, 20] = -1.0
+    assert oracle.DecomposeCHOL(F(A), LO, 16) == 21
+
+
+def test_reference_gemv_unaligned_bug_is_real(ref_oracle, oracle):
+    """calgo/dmvec_gemv.c:241 offsets Y by R*X->inc in the unaligned path.  With an odd
+    leading dimension the reference's DecomposeLU writes outside the view at panel column
+    1 (a 1x1 a01 has inc = ld); the restatement computes the intended result."""
+    import scipy.linalg as sl
+    rng = np.random.default_rng(5)
+    n = 137
+    A = colmajor(rng.standard_normal((n, n)), ld=n)   # odd ld -> unaligned path
+    a1, a2 = colmajor(A, ld=n), colmajor(A, ld=n)
+    p1, p2 = np.zeros(n, np.int64), np.zeros(n, np.int64)
+    oracle.DecomposeLU(a1, p1, 0)
+    ref_oracle.DecomposeLU(a2, p2, 0)
+    lu, piv = sl.lu_factor(A)
+    assert np.array_equal(p1, piv) and rel(a1, lu) <= 1e-12
+    assert rel(a2, lu) > 1e-3
