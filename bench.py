@@ -1,0 +1,419 @@
+#!/usr/bin/env python
+"""Benchmark: FP64 Cholesky factor + solve at n = 16384 (64 RHS) on B200.
+
+One step = DecomposeCHOL(A, LOWER) + SolveCHOL(B, A, LOWER) on a fresh device copy of
+A = G*G^T/n + 0.5*I (G iid N(0,1), seed 2) and B iid U[-1,1] (seed 3), through the C ABI
+(libmatops_b200.so).  Every step works on its own 2 GiB copy of A, so inputs are larger
+than L2 and nothing is reused between steps.
+
+Reported on one JSON line (rank 0):
+  value / ms_per_step   device time of one step (CUDA events, max over ranks)
+  roofline              the DMMA GEMM engine (SYRK / TRSM updates) during the timed steps:
+                        algorithmic FLOPs / its summed event time vs the FP64 tensor-pipe peak
+                        measured on this device in the same run
+  e2e                   the same step through the public API with HOST buffers: upload A, B
+                        (pinned), factor, solve, download the factor and X
+  cpu_baseline          the reference's own C kernels (oracle/_ref) on this host, on a
+                        bounded sample scaled to n = 16384
+  extras                DGEMM 2048^3 (alpha 1.5, beta -0.5) as % of FP64 peak; LU + SolveLU
+
+--impl reference times the reference's CPU path alone (rank 0) and prints its line.
+Multi-GPU (torchrun): independent replicas, one system per rank, no collective in the path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Cholesky solve s at n=16384, mixed+IR vs FP64 at err≤1e-14; DGEMM % FP64 peak"
+LOWER = 0x4
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=16384)
+    ap.add_argument("--nrhs", type=int, default=64)
+    ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def workload(n, nrhs):
+    return (f"DecomposeCHOL+SolveCHOL FP64, n={n}, {nrhs} RHS, A=G*G^T/n+0.5I "
+            f"(G~N(0,1) seed 2), B~U[-1,1] seed 3")
+
+
+# --------------------------------------------------------------------------------------
+# CPU side: the reference's kernels (oracle/_ref) or, if they were not built, the oracle
+# --------------------------------------------------------------------------------------
+
+def cpu_sample(n_s: int, nrhs: int, reps: int):
+    """Time DecomposeCHOL + SolveCHOL at n_s on the host; returns (best factor s, best
+    solve s, kind, threads)."""
+    import numpy as np
+
+    from oracle.oracle import Oracle, ref_available
+    kind = "reference" if ref_available() else "port"
+    orc = Oracle("ref" if kind == "reference" else "port")
+    cores = os.cpu_count() or 1
+    orc.NumWorkers(cores)  # the reference parallelizes only Mult (mmult.go:241-255)
+    rng = np.random.default_rng(2)
+    ld = n_s + (n_s % 2)
+    g = rng.standard_normal((n_s, n_s))
+    A0 = np.zeros((ld, n_s), order="F")
+    A0[:n_s] = g @ g.T / n_s + 0.5 * np.eye(n_s)
+    B0 = np.zeros((ld, nrhs), order="F")
+    B0[:n_s] = np.random.default_rng(3).uniform(-1, 1, (n_s, nrhs))
+    tf, ts = [], []
+    for _ in range(reps):
+        A = A0.copy(order="F")[:n_s]
+        B = B0.copy(order="F")[:n_s]
+        t0 = time.perf_counter()
+        assert orc.DecomposeCHOL(A, LOWER, 64) == 0
+        t1 = time.perf_counter()
+        orc.SolveCHOL(B, A, LOWER)
+        t2 = time.perf_counter()
+        tf.append(t1 - t0)
+        ts.append(t2 - t1)
+    return min(tf), min(ts), kind, 1  # the Cholesky path runs on one thread
+
+
+def scaled_cpu_seconds(n, n_s, tf, ts):
+    return tf * (n / n_s) ** 3 + ts * (n / n_s) ** 2
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return 0
+    n_s = min(args.n, 3072)
+    times = []
+    for i in range(args.warmup + args.steps):
+        tf, ts, kind, cores = cpu_sample(n_s, args.nrhs, 1)
+        if i >= args.warmup:
+            times.append(scaled_cpu_seconds(args.n, n_s, tf, ts))
+    v = sum(times) / len(times)
+    sample = (f"DecomposeCHOL+SolveCHOL at n={n_s}, {args.nrhs} RHS per step; factor time "
+              f"scaled by (n/{n_s})^3, solve by (n/{n_s})^2 to n={args.n}")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": workload(args.n, args.nrhs), "n": args.n, "nrhs": args.nrhs,
+                   "nb": 64, "parallelism": "host cores"},
+        "cpu_baseline": {"value": v, "unit": "s", "cores": cores, "kind": kind, "sample": sample,
+                         "num_workers": os.cpu_count()},
+        "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------------------
+# clocks during the timed region (NVML, read-only)
+# --------------------------------------------------------------------------------------
+
+class ClockSampler:
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
+
+    def __init__(self, torch_dev):
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        self._h = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            import torch
+            bus = torch.cuda.get_device_properties(torch_dev).pci_bus_id
+            dom = torch.cuda.get_device_properties(torch_dev).pci_domain_id
+            dev = torch.cuda.get_device_properties(torch_dev).pci_device_id
+            pci = f"{dom:08X}:{bus:02X}:{dev:02X}.0"
+            try:
+                self._h = pynvml.nvmlDeviceGetHandleByPciBusId(pci)
+            except Exception:
+                self._h = pynvml.nvmlDeviceGetHandleByIndex(0)
+            self._nv = pynvml
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self._h = None
+
+    def _run(self):
+        nv = self._nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                for bit, name in self.REASONS.items():
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.1)
+
+    def __enter__(self):
+        if self._h is not None:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self._h is not None:
+            self._stop.set()
+            self._t.join()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": [], "samples": 0}
+        s = sorted(self.samples)
+        return {"sm_mhz": s[len(s) // 2], "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(s)}
+
+
+# --------------------------------------------------------------------------------------
+# GPU side
+# --------------------------------------------------------------------------------------
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+
+    import torch
+    import torch.distributed as dist
+
+    import matops_b200 as mo
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    n, nrhs, K, W = args.n, args.nrhs, args.steps, args.warmup
+    fp64_peak = mo.MeasureFP64Peak(300.0)
+
+    # inputs, generated on the device (G G^T costs 8.8 TFLOP)
+    g = torch.Generator(device=dev).manual_seed(2)
+    G = mo.matrix(n, n)
+    G.normal_(generator=g)
+    A0 = mo.matrix(n, n)
+    assert mo.Mult(A0, G, G, 1.0 / n, 0.0, mo.TRANSB) is None
+    A0.diagonal().add_(0.5)
+    del G
+    B0 = mo.matrix(n, nrhs)
+    B0.uniform_(-1.0, 1.0, generator=torch.Generator(device=dev).manual_seed(3))
+    nsteps = W + K
+    copies_bytes = nsteps * n * n * 8
+    free = torch.cuda.mem_get_info(dev)[0]
+    fresh = copies_bytes < 0.7 * free
+    As = [A0.clone() for _ in range(nsteps)] if fresh else [mo.matrix(n, n)]
+    Bs = [B0.clone() for _ in range(nsteps)]
+
+    def step(i):
+        A = As[i] if fresh else As[0]
+        if not fresh:
+            A.copy_(A0)
+        _, err = mo.DecomposeCHOL(A, LOWER, 64)
+        assert err is None, err
+        mo.SolveCHOL(Bs[i], A, LOWER)
+
+    for i in range(W):
+        step(i)
+    torch.cuda.synchronize()
+    barrier()
+    mo.ProfileRead()  # reset counters
+    mo.ProfileEnable(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    barrier()
+    with ClockSampler(dev) as clk:
+        e0.record()
+        for i in range(W, nsteps):
+            step(i)
+        e1.record()
+        torch.cuda.synchronize()
+    barrier()
+    prof = mo.ProfileRead()
+    mo.ProfileEnable(False)
+    ms = max_over_ranks(e0.elapsed_time(e1) / K)
+
+    # backward error of the last solve: ||B - A X|| / (||A|| ||X|| + ||B||)
+    X = Bs[nsteps - 1]
+    R = B0.clone()
+    assert mo.Mult(R, A0, X, -1.0, 1.0, 0) is None
+    berr = float(R.norm() / (A0.norm() * X.norm() + B0.norm()))
+    del As, Bs, R
+
+    g_ms = prof.ms["gemm"] / K
+    g_fl = prof.flops["gemm"] / K
+    achieved = g_fl / (g_ms * 1e-3) / 1e12 if g_ms > 0 else 0.0
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "gemm_engine_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+    roofline = {
+        "bound": "tensor", "kernel": "dgemm_tile_kernel (SYRK/GEMM updates)",
+        "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+        "frac": achieved / fp64_peak if fp64_peak else None, "traffic": traffic,
+        "peak_source": "FP64 mma.sync (DMMA) loop measured on this device in this run "
+                       "(MEASURED_PEAKS.json has no FP64 figure)",
+        "share_of_step": g_ms / ms if ms else None,
+        "per_class_ms_per_step": {k: v / K for k, v in prof.ms.items()},
+        "per_class_tflops": {k: (prof.flops[k] / (prof.ms[k] * 1e-3) / 1e12 if prof.ms[k] else None)
+                             for k in prof.ms},
+    }
+    launches = sum(prof.launches.values())
+
+    # ---- e2e: host buffers through the public API ----
+    e2e = None
+    if not args.no_e2e:
+        Ah = mo.host_matrix(n, n)
+        Bh = mo.host_matrix(n, nrhs)
+        Ah.copy_(A0.cpu())
+        Bh.copy_(B0.cpu())
+        Ad = mo.matrix(n, n)
+        Bd = mo.matrix(n, nrhs)
+        Lh = mo.host_matrix(n, n)
+        Xh = mo.host_matrix(n, nrhs)
+
+        def e2e_step():
+            mo.Upload(Ad, Ah)
+            mo.Upload(Bd, Bh)
+            _, err = mo.DecomposeCHOL(Ad, LOWER, 64)
+            assert err is None
+            mo.SolveCHOL(Bd, Ad, LOWER)
+            mo.Download(Lh, Ad)
+            mo.Download(Xh, Bd)
+
+        e2e_step()
+        torch.cuda.synchronize()
+        barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record()
+        ke = max(1, min(K, 3))
+        for _ in range(ke):
+            e2e_step()
+        f1.record()
+        torch.cuda.synchronize()
+        barrier()
+        e_ms = max_over_ranks(f0.elapsed_time(f1) / ke)
+        e2e = {"value": e_ms * 1e-3, "unit": "s", "h2d_bytes_per_step": 8 * (n * n + n * nrhs),
+               "d2h_bytes_per_step": 8 * (n * n + n * nrhs), "steps": ke,
+               "what": "pinned host A,B -> upload, DecomposeCHOL, SolveCHOL, download L and X"}
+        del Ah, Bh, Ad, Bd, Lh, Xh
+
+    # ---- extras: DGEMM 2048^3 and LU at n ----
+    extras = {"mixed_ir": None}
+    if not args.no_extras:
+        m = 2048
+        ga = torch.Generator(device=dev).manual_seed(1)
+        Ag, Bg, Cg = mo.matrix(m, m), mo.matrix(m, m), mo.matrix(m, m)
+        for t in (Ag, Bg, Cg):
+            t.uniform_(-1.0, 1.0, generator=ga)
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > L2
+        ts = []
+        for it in range(3 + 10):
+            flush.fill_(float(it))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            mo.Mult(Cg, Ag, Bg, 1.5, -0.5, 0)
+            b.record()
+            torch.cuda.synchronize()
+            if it >= 3:
+                ts.append(a.elapsed_time(b))
+        gm = sorted(ts)[len(ts) // 2]
+        gtf = 2 * m ** 3 / (gm * 1e-3) / 1e12
+        extras["dgemm_2048"] = {"ms": gm, "tflops": gtf, "frac_fp64_peak": gtf / fp64_peak,
+                                "alpha": 1.5, "beta": -0.5, "l2": "flushed (256 MiB write) between calls"}
+        del Ag, Bg, Cg, flush
+        # LU + SolveLU at n (N(0,1) seed 4; 64 RHS U[-1,1] seed 5)
+        L0 = mo.matrix(n, n)
+        L0.normal_(generator=torch.Generator(device=dev).manual_seed(4))
+        Lb0 = mo.matrix(n, nrhs)
+        Lb0.uniform_(-1.0, 1.0, generator=torch.Generator(device=dev).manual_seed(5))
+        LA, LB = mo.matrix(n, n), mo.matrix(n, nrhs)
+        piv = torch.zeros(n, dtype=torch.int64, device=dev)
+        lts = []
+        for it in range(2):
+            LA.copy_(L0)
+            LB.copy_(Lb0)
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            _, err = mo.DecomposeLU(LA, piv, 64)
+            assert err is None
+            assert mo.SolveLU(LB, LA, piv, 0) is None
+            b.record()
+            torch.cuda.synchronize()
+            lts.append(a.elapsed_time(b))
+        R = Lb0.clone()
+        mo.Mult(R, L0, LB, -1.0, 1.0, 0)
+        lberr = float(R.norm() / (L0.norm() * LB.norm() + Lb0.norm()))
+        lms = min(lts)
+        extras["lu_16384"] = {"s": lms * 1e-3, "factor_tflops": 2 * n ** 3 / 3 / (lms * 1e-3) / 1e12,
+                              "berr": lberr}
+        del L0, Lb0, LA, LB, R
+
+    # ---- CPU baseline (rank 0, one GPU only) ----
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        n_s = min(n, 4096)
+        tf, ts_, kind, cores = cpu_sample(n_s, nrhs, 2)
+        cpu = {"value": scaled_cpu_seconds(n, n_s, tf, ts_), "unit": "s", "cores": cores,
+               "kind": kind, "num_workers": os.cpu_count(),
+               "sample": f"DecomposeCHOL+SolveCHOL at n={n_s}, {nrhs} RHS, best of 2; factor "
+                         f"scaled by (n/{n_s})^3 and solve by (n/{n_s})^2 to n={n}",
+               "sample_s": tf + ts_}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": ms * 1e-3, "unit": "s", "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": workload(n, nrhs), "n": n, "nrhs": nrhs, "nb": 64,
+                       "l2": "fresh 2 GiB copy of A per step (inputs > L2)" if fresh
+                             else "A restored from a copy each step (2 GiB > L2)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "berr": berr, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches, "gpu_launches_by_class": prof.launches,
+            "clocks": clk.summary(), "fp64_peak_tflops": fp64_peak, "extras": extras,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -86,6 +86,28 @@ MO_API int mo_num_workers(mo_ctx *ctx, int n);
  * 28-56 vs 96-121).  Returns the old value. */
 MO_API int mo_set_syrk_blas_beta(mo_ctx *ctx, int on);
 
+/* ---- tracing: per-kernel-class device time (CUDA events on the context's stream) ---- */
+#define MO_PROF_GEMM 0     /* DMMA GEMM / SYRK engine (trailing updates, TRSM sweeps)  */
+#define MO_PROF_DIAG 1     /* diagonal-block Cholesky factor + inverse                  */
+#define MO_PROF_TRTRI 2    /* diagonal-block triangular inverses for TRSM               */
+#define MO_PROF_PANEL 3    /* LU panel (pivot search, interchanges, rank-1 updates)      */
+#define MO_PROF_LASWP 4    /* row interchanges outside the panel                        */
+#define MO_PROF_OTHER 5
+#define MO_PROF_CLASSES 6
+typedef struct mo_profile {
+  int64_t launches[MO_PROF_CLASSES]; /* kernel launches since the last reset            */
+  double ms[MO_PROF_CLASSES];        /* summed device time (only while enabled)         */
+  double flops[MO_PROF_CLASSES];     /* algorithmic flops of those launches             */
+  double bytes[MO_PROF_CLASSES];     /* algorithmic DRAM bytes of those launches        */
+} mo_profile;
+/* on != 0: bracket every launch with CUDA events (adds ~2 events per launch) */
+MO_API int mo_profile_enable(mo_ctx *ctx, int on);
+/* synchronizes, fills *out with the totals since the last reset, then resets them */
+MO_API int mo_profile_read(mo_ctx *ctx, mo_profile *out);
+/* FP64 tensor-pipe throughput of this device: a register-resident mma.sync.f64 loop on
+ * every SM for about `ms` milliseconds; *tflops receives the measured rate. */
+MO_API int mo_measure_fp64_peak(mo_ctx *ctx, double ms, double *tflops);
+
 /* ---- device memory helpers for shims that hold host-side matrices ---- */
 MO_API int mo_malloc(mo_ctx *ctx, void **ptr, size_t bytes);
 MO_API int mo_free(mo_ctx *ctx, void *ptr);

@@ -8,5 +8,6 @@ from .api import (  # noqa: F401
     LEFT, LOWER, NONE, NOTRANS, RIGHT, TRANS, TRANSA, TRANSB, UNIT, UPPER,
     BlockingParams, DecomposeBlockSize, DecomposeCHOL, DecomposeLU, MatopsError, MatopsPanic,
     Mult, NumWorkers, RankUpdateSym, SetPanicOnError, SolveCHOL, SolveLU, SolveTrm, Sync,
-    matrix, to_device, view,
+    matrix, to_device, view, Upload, Download, host_matrix, Profile, ProfileEnable, ProfileRead,
+    MeasureFP64Peak,
 )

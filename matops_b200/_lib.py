@@ -17,6 +17,12 @@ class MoMatrix(ctypes.Structure):
                 ("cols", ctypes.c_int64), ("ld", ctypes.c_int64)]
 
 
+class MoProfile(ctypes.Structure):
+    """mo_profile: per-class launches, device ms, algorithmic flops and bytes."""
+    _fields_ = [("launches", ctypes.c_int64 * 6), ("ms", ctypes.c_double * 6),
+                ("flops", ctypes.c_double * 6), ("bytes", ctypes.c_double * 6)]
+
+
 _lib = None
 
 
@@ -52,6 +58,9 @@ def lib() -> ctypes.CDLL:
         "mo_solve_chol": [p, M, M, i],
         "mo_decompose_lu": [p, M, p, i64, i],
         "mo_solve_lu": [p, M, M, p, i64, i],
+        "mo_profile_enable": [p, i],
+        "mo_profile_read": [p, ctypes.POINTER(MoProfile)],
+        "mo_measure_fp64_peak": [p, d, ctypes.POINTER(d)],
     }
     for name, args in sigs.items():
         fn = getattr(L, name)

@@ -171,3 +171,68 @@ def SolveLU(B, A, pivots: torch.Tensor, flags: int):
 def Sync() -> int:
     """Wait for the context's stream; returns the first device-side status recorded."""
     return _lib.lib().mo_sync(context())
+
+
+# ---- host <-> device transfers through the C ABI (what a shim holding host matrices uses) ----
+
+def _host_view(h: torch.Tensor):
+    if h.dim() != 2 or h.dtype != torch.float64 or h.is_cuda:
+        raise TypeError("expected a 2-D float64 host tensor")
+    r, c = h.shape
+    if r > 1 and h.stride(0) != 1:
+        raise TypeError("host matrix must be column-major (stride(0) == 1)")
+    ld = h.stride(1) if c > 1 else max(h.stride(1), r, 1)
+    return h.data_ptr(), max(ld, r, 1)
+
+
+def Upload(dst: torch.Tensor, src: torch.Tensor) -> None:
+    """Asynchronous host -> device copy of a column-major matrix (mo_upload)."""
+    ptr, ld = _host_view(src)
+    rc = _lib.lib().mo_upload(context(), view(dst), ctypes.c_void_p(ptr), ld)
+    if rc:
+        raise RuntimeError(_lib.lib().mo_strerror(rc).decode())
+
+
+def Download(dst: torch.Tensor, src: torch.Tensor) -> None:
+    """Asynchronous device -> host copy of a column-major matrix (mo_download)."""
+    ptr, ld = _host_view(dst)
+    rc = _lib.lib().mo_download(context(), ctypes.c_void_p(ptr), ld, view(src))
+    if rc:
+        raise RuntimeError(_lib.lib().mo_strerror(rc).decode())
+
+
+def host_matrix(rows: int, cols: int, pinned: bool = True) -> torch.Tensor:
+    """Column-major float64 host matrix (page-locked by default)."""
+    return torch.empty((cols, rows), dtype=torch.float64, pin_memory=pinned).t()
+
+
+class Profile:
+    """Per-kernel-class launches / device time / algorithmic work (mo_profile)."""
+    CLASSES = ("gemm", "diag", "trtri", "panel", "laswp", "other")
+
+    def __init__(self, raw):
+        self.launches = {k: int(raw.launches[i]) for i, k in enumerate(self.CLASSES)}
+        self.ms = {k: float(raw.ms[i]) for i, k in enumerate(self.CLASSES)}
+        self.flops = {k: float(raw.flops[i]) for i, k in enumerate(self.CLASSES)}
+        self.bytes = {k: float(raw.bytes[i]) for i, k in enumerate(self.CLASSES)}
+
+
+def ProfileEnable(on: bool) -> None:
+    _lib.lib().mo_profile_enable(context(), 1 if on else 0)
+
+
+def ProfileRead() -> Profile:
+    raw = _lib.MoProfile()
+    rc = _lib.lib().mo_profile_read(context(), ctypes.byref(raw))
+    if rc:
+        raise RuntimeError(_lib.lib().mo_strerror(rc).decode())
+    return Profile(raw)
+
+
+def MeasureFP64Peak(ms: float = 200.0) -> float:
+    """FP64 tensor-pipe TFLOP/s of this device (register-resident DMMA loop)."""
+    out = ctypes.c_double(0.0)
+    rc = _lib.lib().mo_measure_fp64_peak(context(), ms, ctypes.byref(out))
+    if rc:
+        raise RuntimeError(_lib.lib().mo_strerror(rc).decode())
+    return out.value

@@ -72,7 +72,13 @@ int gemm(mo_ctx *ctx, View C, View A, bool ta, View B, bool tb, double alpha, do
   g.ldc = C.ld;
   g.mode = kGemm;
   g.status = &control(ctx)->status;
-  return launch_gemm(g, ctx->stream);
+  if (g.M <= 0 || g.N <= 0) return MO_OK;
+  ProfScope ps;
+  prof_begin(ctx, ps, MO_PROF_GEMM);
+  const int rc = launch_gemm(g, ctx->stream);
+  const double M = g.M, N = g.N, K = g.K;
+  prof_end(ctx, ps, 2.0 * M * N * K, 8.0 * (M * K + K * N + M * N * (beta != 0.0 ? 2 : 1)));
+  return rc;
 }
 
 int syrk(mo_ctx *ctx, View C, View A, bool ta, bool upper, double alpha, double beta,
@@ -94,7 +100,13 @@ int syrk(mo_ctx *ctx, View C, View A, bool ta, bool upper, double alpha, double 
   g.mode = upper ? kSyrkUpper : kSyrkLower;
   g.beta_block = beta_block;
   g.status = &control(ctx)->status;
-  return launch_gemm(g, ctx->stream);
+  if (g.N <= 0) return MO_OK;
+  ProfScope ps;
+  prof_begin(ctx, ps, MO_PROF_GEMM);
+  const int rc = launch_gemm(g, ctx->stream);
+  const double N = g.N, K = g.K, tri = N * (N + 1) / 2;
+  prof_end(ctx, ps, 2.0 * tri * K, 8.0 * (N * K + tri * (beta != 0.0 ? 2 : 1)));
+  return rc;
 }
 
 }  // namespace mo

@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "common.cuh"
 #include "gemm.cuh"
 
@@ -16,9 +18,28 @@ struct mo_ctx {
   void *ws = nullptr;
   size_t ws_bytes = 0;
   int sms = 148;
+  // tracing (mo_profile_*)
+  bool prof_on = false;
+  mo_profile prof = {};
+  struct Pending {
+    int cls;
+    cudaEvent_t ev0, ev1;
+  };
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  std::vector<Pending> pending;
 };
 
 namespace mo {
+
+// brackets one kernel launch for tracing: counts it and, when tracing is on, records
+// CUDA events around it on the context's stream
+struct ProfScope {
+  int cls;
+  cudaEvent_t ev0, ev1;
+};
+void prof_begin(mo_ctx *ctx, ProfScope &s, int cls);
+void prof_end(mo_ctx *ctx, ProfScope &s, double flops, double bytes);
 
 struct View {
   double *d;

@@ -239,9 +239,12 @@ struct CtrlView {
 int laswp(mo_ctx *ctx, View A, int c0, int c1, const int64_t *piv, int ns, int64_t r0) {
   if (c1 <= c0 || ns <= 0) return MO_OK;
   const int nc = c1 - c0;
+  ProfScope ps;
+  prof_begin(ctx, ps, MO_PROF_LASWP);
   laswp_kernel<<<(nc + 127) / 128, 128, 0, ctx->stream>>>(
       A.at(0, c0), A.ld, A.rows, nc, piv, ns, r0,
       &reinterpret_cast<CtrlView *>(ctx->d_status)->status);
+  prof_end(ctx, ps, 0.0, 4.0 * 8.0 * ns * (double)nc);
   MO_CUDA_TRY(cudaGetLastError());
   return MO_OK;
 }
@@ -319,8 +322,11 @@ int getrf(mo_ctx *ctx, View A, int64_t *piv, int64_t npiv, int ref_nb) {
     int64_t pld = Pv.ld;
     int pw = b;
     void *args[] = {&pd, &pld, (void *)&pm, &pw, &pR, &pv, &row0, &sc, &status, &abort_flag};
+    ProfScope ps;
+    prof_begin(ctx, ps, MO_PROF_PANEL);
     MO_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)lu_panel_kernel, dim3(pblk),
                                             dim3(PANEL_THREADS), args, smem, ctx->stream));
+    prof_end(ctx, ps, (double)pm * b * b - (double)b * b * b / 3.0, 16.0 * pm * b);
     // interchanges on the columns left and right of the panel
     if ((rc = laswp(ctx, A, 0, k, piv + k, b, k))) return rc;
     if ((rc = laswp(ctx, A, k + b, n, piv + k, b, k))) return rc;
@@ -347,9 +353,13 @@ int getrf(mo_ctx *ctx, View A, int64_t *piv, int64_t npiv, int ref_nb) {
       k += (k + ref_nb > n) ? n - k : ref_nb;
     }
     const int64_t hi = std::min<int64_t>(npiv, k_last + ref_nb);
-    if (hi > mn)
+    if (hi > mn) {
+      ProfScope ps;
+      prof_begin(ctx, ps, MO_PROF_OTHER);
       fill_pivots_kernel<<<(unsigned)((hi - mn + 255) / 256), 256, 0, ctx->stream>>>(piv, mn, hi,
                                                                                      k_last);
+      prof_end(ctx, ps, 0.0, 8.0 * (hi - mn));
+    }
     MO_CUDA_TRY(cudaGetLastError());
   }
   return MO_OK;

@@ -57,8 +57,12 @@ int potrf(mo_ctx *ctx, View A, bool upper, int *d_info, double *d_bad, double *i
   const int n = A.rows;
   for (int k = 0; k < n; k += NB) {
     const int b = min(NB, n - k);
+    ProfScope ps;
+    prof_begin(ctx, ps, MO_PROF_DIAG);
     potrf_diag_kernel<<<1, TRI_THREADS, TRI_SMEM_BYTES, ctx->stream>>>(A.at(k, k), A.ld, b, upper,
                                                                        inv, d_info, d_bad, k);
+    // factor b^3/3 + inverse b^3/3; reads the triangle, writes it and the inverse
+    prof_end(ctx, ps, 2.0 * b * b * b / 3.0, 8.0 * 2.0 * b * b);
     MO_CUDA_TRY(cudaGetLastError());
     const int rest = n - k - b;
     if (rest <= 0) break;

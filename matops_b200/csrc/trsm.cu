@@ -56,8 +56,11 @@ int trtri_blocks(mo_ctx *ctx, View A, int N, bool trans, bool lower_eff, bool un
   const bool load_t = (trans == lower_eff);
   int rc = set_tri_smem((const void *)trtri_blocks_kernel);
   if (rc) return rc;
+  ProfScope ps;
+  prof_begin(ctx, ps, MO_PROF_TRTRI);
   trtri_blocks_kernel<<<nblk, TRI_THREADS, TRI_SMEM_BYTES, ctx->stream>>>(
       A.d, A.ld, N, load_t, !lower_eff, unit, inv);
+  prof_end(ctx, ps, nblk * (double)NBT * NBT * NBT / 3.0, 8.0 * nblk * 1.5 * NBT * NBT);
   MO_CUDA_TRY(cudaGetLastError());
   return MO_OK;
 }
