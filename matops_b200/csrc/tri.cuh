@@ -61,124 +61,190 @@ __device__ inline void tri_store_lower(const double *S, double *G, int64_t ld, i
   }
 }
 
+// S(i, j) -= sum_{k<32} S(i, kb + k) * S(j, kb + k) for the lower triangle (i >= j) of
+// rows/cols [r0, NP); register-blocked 4 x 4 micro-tiles, all threads.
+__device__ __forceinline__ void tri_syrk_update(double *S, int NP, int r0, int kb) {
+  const int nr = NP - r0;
+  const int nt = nr / 4;  // micro-tiles per side (nr is a multiple of 32)
+  const int ntiles = nt * (nt + 1) / 2;
+  for (int e = threadIdx.x; e < ntiles; e += blockDim.x) {
+    // e -> (ti >= tj): row-by-row enumeration of the lower triangle of micro-tiles
+    int ti = 0;
+    while ((ti + 1) * (ti + 2) / 2 <= e) ++ti;
+    const int tj = e - ti * (ti + 1) / 2;
+    const int i0 = r0 + 4 * ti, j0 = r0 + 4 * tj;
+    double acc[4][4];
+#pragma unroll
+    for (int x = 0; x < 4; ++x)
+#pragma unroll
+      for (int y = 0; y < 4; ++y) acc[x][y] = 0.0;
+#pragma unroll 4
+    for (int k = 0; k < SUB; ++k) {
+      double a[4], b[4];
+#pragma unroll
+      for (int x = 0; x < 4; ++x) {
+        a[x] = S[(i0 + x) * LDS + kb + k];
+        b[x] = S[(j0 + x) * LDS + kb + k];
+      }
+#pragma unroll
+      for (int x = 0; x < 4; ++x)
+#pragma unroll
+        for (int y = 0; y < 4; ++y) acc[x][y] = fma(a[x], b[y], acc[x][y]);
+    }
+#pragma unroll
+    for (int x = 0; x < 4; ++x)
+#pragma unroll
+      for (int y = 0; y < 4; ++y)
+        if (i0 + x >= j0 + y) S[(i0 + x) * LDS + j0 + y] -= acc[x][y];
+  }
+}
+
 // In-place Cholesky of the lower triangle of S (order NP, multiple of 32), right-looking
 // over 32-column sub-panels.  The pivot is sqrt(s_kk); when it is NaN (s_kk < 0 or NaN)
 // the column index is returned through *bad_col (first failure) and the routine stops.
 // Division (not reciprocal multiplication) scales the column, as the reference does
 // (calgo/dvec_util.c:230-246).  Must be called by all threads of the block.
+//   (1) 32 x 32 diagonal sub-block: one warp, lane i holds row i in registers
+//   (2) rows below: one thread per row, the 32-wide row segment in registers
+//   (3) trailing lower triangle: register-blocked rank-32 update
 __device__ inline void tri_potrf_lower(double *S, int NP, int *bad_col, double *bad_val) {
   __shared__ int s_bad;
   if (threadIdx.x == 0) s_bad = -1;
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int jb = 0; jb < NP; jb += SUB) {
-    // (1) factor the 32 x 32 diagonal sub-block with warp 0
     if (warp == 0) {
+      double r[SUB];
+#pragma unroll
+      for (int j = 0; j < SUB; ++j) r[j] = (j <= lane) ? S[(jb + lane) * LDS + jb + j] : 0.0;
+      int bad = -1;
+      double badv = 0.0;
+#pragma unroll
       for (int k = 0; k < SUB; ++k) {
-        const int kk = jb + k;
-        if (lane == 0) {
-          double a = S[kk * LDS + kk];
-          double d = sqrt(a);
-          if (isnan(d) && s_bad < 0) {
-            s_bad = kk;
-            *bad_val = a;
+        const double akk = __shfl_sync(0xffffffffu, r[k], k);
+        const double d = sqrt(akk);
+        if (bad < 0 && isnan(d)) {  // uniform: every lane sees the same akk
+          bad = k;
+          badv = akk;
+        }
+        if (bad < 0) {
+          if (lane == k) r[k] = d;
+          if (lane > k) r[k] = r[k] / d;
+#pragma unroll
+          for (int j = k + 1; j < SUB; ++j) {
+            const double ljk = __shfl_sync(0xffffffffu, r[k], j);
+            if (lane >= j) r[j] = fma(-r[k], ljk, r[j]);
           }
-          S[kk * LDS + kk] = d;
         }
-        __syncwarp();
-        if (s_bad >= 0) break;
-        const double d = S[kk * LDS + kk];
-        if (lane > k) S[(jb + lane) * LDS + kk] /= d;
-        __syncwarp();
-        if (lane > k) {
-          const double lik = S[(jb + lane) * LDS + kk];
-          for (int j = k + 1; j <= lane; ++j)
-            S[(jb + lane) * LDS + jb + j] -= lik * S[(jb + j) * LDS + kk];
-        }
-        __syncwarp();
+      }
+#pragma unroll
+      for (int j = 0; j < SUB; ++j)
+        if (j <= lane) S[(jb + lane) * LDS + jb + j] = r[j];
+      if (lane == 0 && bad >= 0) {
+        s_bad = jb + bad;
+        *bad_val = badv;
       }
     }
     __syncthreads();
     if (s_bad >= 0) break;
-    // (2) rows below: L(i, jb:jb+32) = A(i, jb:jb+32) * L_dd^-T by row substitution
+    // (2) L(i, jb:jb+32) = A(i, jb:jb+32) * L_dd^-T for rows i below the sub-block
     for (int i = jb + SUB + threadIdx.x; i < NP; i += blockDim.x) {
+      double v[SUB];
       double *row = S + i * LDS + jb;
+#pragma unroll
+      for (int k = 0; k < SUB; ++k) v[k] = row[k];
+#pragma unroll
       for (int k = 0; k < SUB; ++k) {
-        const double *lrow = S + (jb + k) * LDS + jb;
-        double s = row[k];
-        for (int m = 0; m < k; ++m) s -= row[m] * lrow[m];
-        row[k] = s / lrow[k];
+        v[k] = v[k] / S[(jb + k) * LDS + jb + k];
+#pragma unroll
+        for (int m = k + 1; m < SUB; ++m) v[m] = fma(-v[k], S[(jb + m) * LDS + jb + k], v[m]);
       }
+#pragma unroll
+      for (int k = 0; k < SUB; ++k) row[k] = v[k];
     }
     __syncthreads();
-    // (3) trailing update of the lower triangle: S(i,j) -= sum_k L(i,k) L(j,k)
-    const int r0 = jb + SUB, nr = NP - r0;
-    const int npairs = nr * (nr + 1) / 2;
-    for (int e = threadIdx.x; e < npairs; e += blockDim.x) {
-      // e -> (ii >= jj) in the trailing triangle
-      int ii = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
-      while ((ii + 1) * (ii + 2) / 2 <= e) ++ii;
-      while (ii * (ii + 1) / 2 > e) --ii;
-      const int jj = e - ii * (ii + 1) / 2;
-      const double *li = S + (r0 + ii) * LDS + jb;
-      const double *lj = S + (r0 + jj) * LDS + jb;
-      double s = 0.0;
-#pragma unroll 8
-      for (int k = 0; k < SUB; ++k) s = fma(li[k], lj[k], s);
-      S[(r0 + ii) * LDS + r0 + jj] -= s;
-    }
+    // (3) trailing update of the lower triangle
+    if (jb + SUB < NP) tri_syrk_update(S, NP, jb + SUB, jb);
     __syncthreads();
   }
   if (threadIdx.x == 0) *bad_col = s_bad;
   __syncthreads();
 }
 
+// C(32x32, in W at ldc) = sum over `nk` 32-blocks of P_q(32x32) * Q_q(32x32), where P_q is
+// S[prow + r, pcol + 32q + k] and Q_q is S or W data given by pointers; all threads,
+// 4 x 4 register micro-tiles (64 per 32 x 32 product).
+__device__ __forceinline__ void tri_small_gemm(double *C, int ldc, const double *P, int ldp,
+                                               const double *Q, int ldq, int nk, double sign,
+                                               int tile, int ntile_total) {
+  (void)ntile_total;
+  const int ti = tile / 8, tj = tile % 8;
+  double acc[4][4];
+#pragma unroll
+  for (int x = 0; x < 4; ++x)
+#pragma unroll
+    for (int y = 0; y < 4; ++y) acc[x][y] = 0.0;
+  for (int k = 0; k < nk; ++k) {
+    double a[4], b[4];
+#pragma unroll
+    for (int x = 0; x < 4; ++x) {
+      a[x] = P[(4 * ti + x) * ldp + k];
+      b[x] = Q[k * ldq + 4 * tj + x];
+    }
+#pragma unroll
+    for (int x = 0; x < 4; ++x)
+#pragma unroll
+      for (int y = 0; y < 4; ++y) acc[x][y] = fma(a[x], b[y], acc[x][y]);
+  }
+#pragma unroll
+  for (int x = 0; x < 4; ++x)
+#pragma unroll
+    for (int y = 0; y < 4; ++y) C[(4 * ti + x) * ldc + 4 * tj + y] = sign * acc[x][y];
+}
+
 // In-place inverse of the lower-triangular S (order NP, multiple of 32, non-singular
 // diagonal).  W: scratch of 4 * 32 * 33 doubles.  Must be called by all threads.
-//   X_ii = L_ii^-1 (one warp per diagonal sub-block, one lane per column)
+//   X_ii = L_ii^-1 (one warp per diagonal sub-block, one lane per column, registers)
 //   X_ij = -X_ii * sum_{k=j}^{i-1} L_ik X_kj   for i > j, block row by block row
 __device__ inline void tri_inverse_lower(double *S, int NP, double *W) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nsub = NP / SUB;
   constexpr int LW = SUB + 1;
-  // (1) diagonal sub-blocks, warps 0..nsub-1
+  // (1) diagonal sub-blocks, warps 0..nsub-1: lane c solves L_bb x = e_c
   if (warp < nsub) {
     const int b = warp * SUB;
-    double *w = W + warp * SUB * LW;
-    for (int i = 0; i < SUB; ++i) w[i * LW + lane] = 0.0;
-    __syncwarp();
-    const int c = lane;
-    const double xcc = 1.0 / S[(b + c) * LDS + b + c];
-    w[c * LW + c] = xcc;
-    for (int i = c + 1; i < SUB; ++i) {
+    double x[SUB];
+#pragma unroll
+    for (int i = 0; i < SUB; ++i) {
       const double *lrow = S + (b + i) * LDS + b;
-      double s = 0.0;
-      for (int m = c; m < i; ++m) s = fma(lrow[m], w[m * LW + c], s);
-      w[i * LW + c] = -s / lrow[i];
+      double s0 = (i == lane) ? 1.0 : 0.0, s1 = 0.0;
+#pragma unroll
+      for (int m = 0; m + 1 < i; m += 2) {
+        s0 = fma(-lrow[m], x[m], s0);
+        s1 = fma(-lrow[m + 1], x[m + 1], s1);
+      }
+      if (i & 1) s0 = fma(-lrow[i - 1], x[i - 1], s0);
+      x[i] = (i < lane) ? 0.0 : (s0 + s1) / lrow[i];
     }
     __syncwarp();
-    for (int i = 0; i < SUB; ++i) S[(b + i) * LDS + b + lane] = (lane <= i) ? w[i * LW + lane] : 0.0;
+#pragma unroll
+    for (int i = 0; i < SUB; ++i) S[(b + i) * LDS + b + lane] = x[i];  // column lane
   }
   __syncthreads();
   // (2) off-diagonal blocks, block row by block row
   for (int bi = 1; bi < nsub; ++bi) {
-    // T_bj = sum_{k=bj}^{bi-1} L(bi,k) X(k,bj) for bj < bi, into W (bi blocks of 32x33)
-    const int nel = bi * SUB * SUB;
-    for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-      const int bj = e / (SUB * SUB), r = (e / SUB) % SUB, c = e % SUB;
-      const double *lrow = S + (bi * SUB + r) * LDS;  // row of L in block row bi
-      double s = 0.0;
-      for (int k = bj * SUB + c; k < bi * SUB; ++k) s = fma(lrow[k], S[k * LDS + bj * SUB + c], s);
-      W[bj * SUB * LW + r * LW + c] = s;
+    // T_bj = sum_{k=bj}^{bi-1} L(bi,k) X(k,bj) for bj < bi  -> W block bj
+    for (int e = threadIdx.x; e < bi * 64; e += blockDim.x) {
+      const int bj = e / 64, tile = e % 64;
+      tri_small_gemm(W + bj * SUB * LW, LW, S + (bi * SUB) * LDS + bj * SUB, LDS,
+                     S + (bj * SUB) * LDS + bj * SUB, LDS, (bi - bj) * SUB, 1.0, tile, 64);
     }
     __syncthreads();
     // X(bi,bj) = -X(bi,bi) * T_bj
-    for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-      const int bj = e / (SUB * SUB), r = (e / SUB) % SUB, c = e % SUB;
-      const double *xrow = S + (bi * SUB + r) * LDS + bi * SUB;
-      double s = 0.0;
-      for (int q = 0; q <= r; ++q) s = fma(xrow[q], W[bj * SUB * LW + q * LW + c], s);
-      S[(bi * SUB + r) * LDS + bj * SUB + c] = -s;
+    for (int e = threadIdx.x; e < bi * 64; e += blockDim.x) {
+      const int bj = e / 64, tile = e % 64;
+      tri_small_gemm(S + (bi * SUB) * LDS + bj * SUB, LDS, S + (bi * SUB) * LDS + bi * SUB, LDS,
+                     W + bj * SUB * LW, LW, SUB, -1.0, tile, 64);
     }
     __syncthreads();
   }
