@@ -47,7 +47,67 @@ def parse():
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--case", default=None,
+                    help="profiling aid: run one operation instead of the benchmark, e.g. "
+                         "dgemm:M:N:K:flags, dsyrk:N:K, dpotrf:N, dgetrf:N (W+K calls)")
     return ap.parse_args()
+
+
+def run_case(args):
+    """Run a single operation W+K times (for ncu captures); prints its mean device time."""
+    import torch
+
+    import matops_b200 as mo
+    kind, *dims = args.case.split(":")
+    dims = [int(x) for x in dims]
+    g = torch.Generator(device="cuda").manual_seed(1)
+    if kind == "dgemm":
+        m, n, k, fl = dims
+        A = mo.matrix(k, m) if fl & 1 else mo.matrix(m, k)
+        B = mo.matrix(n, k) if fl & 2 else mo.matrix(k, n)
+        C = mo.matrix(m, n)
+        for t in (A, B, C):
+            t.uniform_(-1.0, 1.0, generator=g)
+        fn, flops = (lambda: mo.Mult(C, A, B, 1.5, -0.5, fl)), 2.0 * m * n * k
+    elif kind == "dsyrk":
+        n, k = dims
+        A, C = mo.matrix(n, k), mo.matrix(n, n)
+        A.uniform_(-1.0, 1.0, generator=g)
+        C.uniform_(-1.0, 1.0, generator=g)
+        fn, flops = (lambda: mo.RankUpdateSym(C, A, -1.0, 1.0, LOWER)), float(n) * n * k
+    elif kind in ("dpotrf", "dgetrf"):
+        n = dims[0]
+        A0 = mo.matrix(n, n)
+        A0.normal_(generator=g)
+        if kind == "dpotrf":
+            G = A0.clone()
+            mo.Mult(A0, G, G, 1.0 / n, 0.0, mo.TRANSB)
+            A0.diagonal().add_(0.5)
+            del G
+        A = mo.matrix(n, n)
+        piv = torch.zeros(n, dtype=torch.int64, device="cuda")
+
+        def fn():
+            A.copy_(A0)
+            if kind == "dpotrf":
+                mo.DecomposeCHOL(A, LOWER, 64)
+            else:
+                mo.DecomposeLU(A, piv, 64)
+        flops = n ** 3 / 3.0 if kind == "dpotrf" else 2.0 * n ** 3 / 3.0
+    else:
+        raise SystemExit(f"unknown case {kind}")
+    for _ in range(args.warmup):
+        fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(args.steps):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / args.steps
+    print(json.dumps({"case": args.case, "ms": ms, "tflops": flops / (ms * 1e-3) / 1e12}), flush=True)
+    return 0
 
 
 def workload(n, nrhs):
@@ -193,6 +253,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank)
+    if args.case:
+        return run_case(args)
 
     import torch
     import torch.distributed as dist

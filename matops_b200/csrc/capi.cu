@@ -72,6 +72,10 @@ int gemm(mo_ctx *ctx, View C, View A, bool ta, View B, bool tb, double alpha, do
   g.ldc = C.ld;
   g.mode = kGemm;
   g.status = &control(ctx)->status;
+  g.sms = ctx->sms;
+  g.sk_partial = ctx->sk_partial;
+  g.sk_flags = ctx->sk_flags;
+  g.sk_epoch = ++ctx->sk_epoch;
   if (g.M <= 0 || g.N <= 0) return MO_OK;
   ProfScope ps;
   prof_begin(ctx, ps, MO_PROF_GEMM);
@@ -100,6 +104,7 @@ int syrk(mo_ctx *ctx, View C, View A, bool ta, bool upper, double alpha, double 
   g.mode = upper ? kSyrkUpper : kSyrkLower;
   g.beta_block = beta_block;
   g.status = &control(ctx)->status;
+  g.sms = ctx->sms;
   if (g.N <= 0) return MO_OK;
   ProfScope ps;
   prof_begin(ctx, ps, MO_PROF_GEMM);
@@ -130,7 +135,13 @@ int mo_ctx_create(int device, mo_ctx **out) {
   ctx->sms = prop.multiProcessorCount;
   cudaError_t e = cudaMalloc(&ctx->d_status, sizeof(mo::Control));
   if (e == cudaSuccess) e = cudaMemset(ctx->d_status, 0, sizeof(mo::Control));
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->sk_partial, mo::gemm_partial_bytes(ctx->sms));
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->sk_flags, sizeof(int) * ctx->sms);
+  if (e == cudaSuccess) e = cudaMemset(ctx->sk_flags, 0, sizeof(int) * ctx->sms);
   if (e != cudaSuccess) {
+    if (ctx->sk_partial) cudaFree(ctx->sk_partial);
+    if (ctx->sk_flags) cudaFree(ctx->sk_flags);
+    if (ctx->d_status) cudaFree(ctx->d_status);
     delete ctx;
     return mo_from_cuda_error(e);
   }
@@ -144,6 +155,9 @@ int mo_ctx_destroy(mo_ctx *ctx) {
   cudaStreamSynchronize(ctx->stream);
   if (ctx->ws) cudaFree(ctx->ws);
   if (ctx->d_status) cudaFree(ctx->d_status);
+  if (ctx->sk_partial) cudaFree(ctx->sk_partial);
+  if (ctx->sk_flags) cudaFree(ctx->sk_flags);
+  for (auto e : ctx->ev_pool) cudaEventDestroy(e);
   delete ctx;
   return MO_OK;
 }

@@ -18,6 +18,10 @@ struct mo_ctx {
   void *ws = nullptr;
   size_t ws_bytes = 0;
   int sms = 148;
+  // stream-K scratch of the GEMM engine (allocated with the context)
+  double *sk_partial = nullptr;
+  int *sk_flags = nullptr;
+  int sk_epoch = 0;
   // tracing (mo_profile_*)
   bool prof_on = false;
   mo_profile prof = {};

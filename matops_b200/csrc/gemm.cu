@@ -13,8 +13,10 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstring>
 #include <mutex>
 
 #include "common.cuh"
@@ -55,7 +57,15 @@ struct KParams {
   int64_t ldc;
   int mode, beta_block;
   int *status;
-  int tiles_m;
+  int tiles_m, tiles_n;
+  int total_tiles;  // tiles of C (the triangle's tiles in SYRK modes)
+  int kt;           // k-slabs per tile
+  int dp_tiles;     // tiles [0, dp_tiles) are processed whole, round-robin over CTAs
+  int sk_iters;     // stream-K iterations over the remaining tiles
+  int sk_chunk;     // stream-K iterations per CTA
+  double *partial;  // [gridDim.x][64 * 256] stream-K partial accumulators
+  int *flags;       // [gridDim.x] epoch stamps of published partials
+  int epoch;
 };
 
 // cp.async producer for one 128 x 16 slab of an operand whose element (mn, k) lives at
@@ -86,17 +96,24 @@ __device__ __forceinline__ void load_slab_cpasync(double *dst, const double *src
   }
 }
 
-__device__ __forceinline__ void tile_of_block(const KParams &p, int bid, int &tm, int &tn) {
+__device__ __forceinline__ void tile_coords(const KParams &p, int t, int &tm, int &tn) {
   if (p.mode == kGemm) {
-    tm = bid % p.tiles_m;
-    tn = bid / p.tiles_m;
+    // groups of GROUP_M tile rows, column-major inside a group: a wave of persistent CTAs
+    // touches GROUP_M row panels of A and a narrow band of B, which stay in L2
+    constexpr int GROUP_M = 8;
+    const int per_group = GROUP_M * p.tiles_n;
+    const int grp = t / per_group, r = t % per_group;
+    const int m_first = grp * GROUP_M;
+    const int gm = min(GROUP_M, p.tiles_m - m_first);
+    tm = m_first + r % gm;
+    tn = r / gm;
     return;
   }
-  // bid enumerates the triangle row by row: (r, c) with c <= r
-  int r = (int)((sqrt(8.0 * (double)bid + 1.0) - 1.0) * 0.5);
-  while ((r + 1) * (r + 2) / 2 <= bid) ++r;
-  while (r * (r + 1) / 2 > bid) --r;
-  int c = bid - r * (r + 1) / 2;
+  // t enumerates the triangle row by row: (r, c) with c <= r
+  int r = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+  while ((r + 1) * (r + 2) / 2 <= t) ++r;
+  while (r * (r + 1) / 2 > t) --r;
+  const int c = t - r * (r + 1) / 2;
   if (p.mode == kSyrkLower) {
     tm = r;
     tn = c;
@@ -104,6 +121,50 @@ __device__ __forceinline__ void tile_of_block(const KParams &p, int bid, int &tm
     tm = c;
     tn = r;
   }
+}
+
+// One unit of work: k-slabs [k0, k1) of tile `tile`.  owner: this CTA finishes the tile
+// (adds the partials of CTAs [first_contrib, blockIdx.x) and writes C); otherwise it
+// publishes its partial sum.
+struct Unit {
+  int tile, k0, k1;
+  bool owner;
+  int first_contrib;
+};
+
+// Enumerates this CTA's units in processing order: whole tiles first, then its stream-K
+// range from the highest tile down (so that a partial is published before this CTA waits
+// for the partials of lower-numbered CTAs).  Returns the number of units; fills u[i] for
+// i == idx.
+__device__ __forceinline__ bool unit_at(const KParams &p, int idx, Unit &u) {
+  const int P = gridDim.x, b = blockIdx.x;
+  const int ndp = (p.dp_tiles > b) ? (p.dp_tiles - b + P - 1) / P : 0;
+  if (idx < ndp) {
+    u.tile = b + idx * P;
+    u.k0 = 0;
+    u.k1 = p.kt;
+    u.owner = true;
+    u.first_contrib = b;
+    return true;
+  }
+  idx -= ndp;
+  if (p.sk_iters <= 0) return false;
+  const int s = b * p.sk_chunk, e = min(s + p.sk_chunk, p.sk_iters);
+  if (s >= e) return false;
+  const int first = s / p.kt, last = (e - 1) / p.kt;
+  const int t = last - idx;
+  if (t < first) return false;
+  const int ts = t * p.kt, te = ts + p.kt;
+  u.tile = p.dp_tiles + t;
+  u.k0 = max(s, ts) - ts;
+  u.k1 = min(e, te) - ts;
+  u.owner = (e >= te);
+  u.first_contrib = ts / p.sk_chunk;
+  return true;
+}
+
+__device__ __forceinline__ void consumer_bar() {
+  asm volatile("bar.sync 1, 256;" ::: "memory");
 }
 
 template <bool A_KMAJ, bool B_KMAJ, bool USE_TMA>
@@ -115,18 +176,15 @@ __global__ void __launch_bounds__(THREADS, 1)
   double *tiles = reinterpret_cast<double *>(base);
   uint64_t *full = reinterpret_cast<uint64_t *>(base + STAGES * STAGE_BYTES);
   uint64_t *empty = full + STAGES;
+  __shared__ int s_abort;
 
-  int tm, tn;
-  tile_of_block(p, blockIdx.x, tm, tn);
-  const int m0 = tm * BM, n0 = tn * BN;
-  const int num_kt = (p.K + BK - 1) / BK;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&full[s], USE_TMA ? 1u : 32u);
       mbar_init(&empty[s], CONSUMER_WARPS);
     }
+    s_abort = 0;
     fence_barrier_init();
   }
   __syncthreads();
@@ -135,34 +193,46 @@ __global__ void __launch_bounds__(THREADS, 1)
     // ------------------------------ producer warpgroup ------------------------------
     asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(PRODUCER_REGS));
     if (warp != 0) return;
-    for (int kt = 0; kt < num_kt; ++kt) {
-      const int s = kt % STAGES;
-      const uint32_t ph = (kt / STAGES) & 1;
-      if (!mbar_wait(&empty[s], ph ^ 1u, p.status)) break;
-      double *As = tiles + s * 2 * TILE_DOUBLES;
-      double *Bs = As + TILE_DOUBLES;
-      const int k0 = kt * BK;
-      if constexpr (USE_TMA) {
-        if (lane == 0) {
-          mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
-          if (A_KMAJ) {
-            tma_load_2d(As, &tmA, &full[s], k0, m0);
-          } else {
-#pragma unroll
-            for (int b = 0; b < 8; ++b) tma_load_2d(As + b * 256, &tmA, &full[s], m0 + 16 * b, k0);
-          }
-          if (B_KMAJ) {
-            tma_load_2d(Bs, &tmB, &full[s], k0, n0);
-          } else {
-#pragma unroll
-            for (int b = 0; b < 8; ++b) tma_load_2d(Bs + b * 256, &tmB, &full[s], n0 + 16 * b, k0);
-          }
+    int it = 0;  // ring position, continues across units
+    Unit u;
+    for (int ui = 0; unit_at(p, ui, u); ++ui) {
+      int tm, tn;
+      tile_coords(p, u.tile, tm, tn);
+      const int m0 = tm * BM, n0 = tn * BN;
+      for (int kt = u.k0; kt < u.k1; ++kt, ++it) {
+        const int s = it % STAGES;
+        const uint32_t ph = (it / STAGES) & 1;
+        if (!mbar_wait(&empty[s], ph ^ 1u, p.status)) {
+          if constexpr (!USE_TMA) asm volatile("cp.async.wait_all;" ::: "memory");
+          return;
         }
-        __syncwarp();
-      } else {
-        load_slab_cpasync<A_KMAJ>(As, p.A, p.lda, m0, k0, p.M, p.K, lane);
-        load_slab_cpasync<B_KMAJ>(Bs, p.B, p.ldb, n0, k0, p.N, p.K, lane);
-        cp_async_arrive_noinc(&full[s]);
+        double *As = tiles + s * 2 * TILE_DOUBLES;
+        double *Bs = As + TILE_DOUBLES;
+        const int k0 = kt * BK;
+        if constexpr (USE_TMA) {
+          if (lane == 0) {
+            mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
+            if (A_KMAJ) {
+              tma_load_2d(As, &tmA, &full[s], k0, m0);
+            } else {
+#pragma unroll
+              for (int bb = 0; bb < 8; ++bb)
+                tma_load_2d(As + bb * 256, &tmA, &full[s], m0 + 16 * bb, k0);
+            }
+            if (B_KMAJ) {
+              tma_load_2d(Bs, &tmB, &full[s], k0, n0);
+            } else {
+#pragma unroll
+              for (int bb = 0; bb < 8; ++bb)
+                tma_load_2d(Bs + bb * 256, &tmB, &full[s], n0 + 16 * bb, k0);
+            }
+          }
+          __syncwarp();
+        } else {
+          load_slab_cpasync<A_KMAJ>(As, p.A, p.lda, m0, k0, p.M, p.K, lane);
+          load_slab_cpasync<B_KMAJ>(Bs, p.B, p.ldb, n0, k0, p.N, p.K, lane);
+          cp_async_arrive_noinc(&full[s]);
+        }
       }
     }
     if constexpr (!USE_TMA) asm volatile("cp.async.wait_all;" ::: "memory");
@@ -171,71 +241,166 @@ __global__ void __launch_bounds__(THREADS, 1)
 
   // ------------------------------ consumer warpgroups ------------------------------
   asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(CONSUMER_REGS));
+  const int ct = threadIdx.x - 128;  // consumer thread 0..255
   const int cw = warp - 4;
   const int wm = cw >> 2, wn = cw & 3;  // 2 x 4 grid of 64 x 32 warp tiles
   const int g = lane >> 2, t = lane & 3;
-  double acc[4][4][4];
+  // Fragment offsets into the swizzled slabs, split into a per-thread part computed once
+  // and compile-time constants (mt, nt, kk).  K-major: element (mn, k) at
+  // mn*16 + 2*((k>>1) ^ (mn&7)) + (k&1), with mn&7 == g and k = kk + t.
+  // MN-major: (mn>>4)*256 + k*16 + 2*(((mn&15)>>1) ^ (k&7)) + (mn&1).
+  int kv[4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int q = 0; q < 4; ++q) kv[q] = 2 * ((2 * q) ^ (g & 6)) + 2 * ((t >> 1) ^ (g & 1)) + (t & 1);
+  int xa[2][2], xb[2][2];
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+  for (int h = 0; h < 2; ++h)
 #pragma unroll
-      for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0;
-
-  bool ok = true;
-  for (int kt = 0; kt < num_kt; ++kt) {
-    const int s = kt % STAGES;
-    const uint32_t ph = (kt / STAGES) & 1;
-    if (!mbar_wait(&full[s], ph, p.status)) {
-      ok = false;
-      break;
+    for (int q2 = 0; q2 < 2; ++q2) {
+      xa[h][q2] = 2 * (((g >> 1) + 4 * h) ^ (4 * q2 + t));
+      xb[h][q2] = 2 * (((g >> 1) + 4 * h) ^ (4 * q2 + t));
     }
-    const double *As = tiles + s * 2 * TILE_DOUBLES;
-    const double *Bs = As + TILE_DOUBLES;
+  const int a_base = A_KMAJ ? (wm * 64 + g) * 16 : (wm * 4) * 256 + t * 16 + (g & 1);
+  const int b_base = B_KMAJ ? (wn * 32 + g) * 16 : (wn * 2) * 256 + t * 16 + (g & 1);
+  int it = 0;
+  Unit u;
+  for (int ui = 0; unit_at(p, ui, u); ++ui) {
+    int tm, tn;
+    tile_coords(p, u.tile, tm, tn);
+    const int m0 = tm * BM, n0 = tn * BN;
+    // warm L2 with this warp's C sub-tile (64 rows x 32 cols: 4 lines of 128 B per column)
+    if (u.owner && (p.beta != 0.0 || p.beta_block > 0)) {
 #pragma unroll
-    for (int kk = 0; kk < BK; kk += 4) {
-      const int k = kk + t;
-      double a[4][2], b[4];
-#pragma unroll
-      for (int mt = 0; mt < 4; ++mt) {
-        const int m = wm * 64 + mt * 16 + g;
-        a[mt][0] = As[A_KMAJ ? kmaj_off(m, k) : mnmaj_off(m, k)];
-        a[mt][1] = As[A_KMAJ ? kmaj_off(m + 8, k) : mnmaj_off(m + 8, k)];
+      for (int q = 0; q < 4; ++q) {
+        const int col = n0 + wn * 32 + lane;
+        const int row = m0 + wm * 64 + 16 * q;
+        if (col < p.N && row < p.M)
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(p.C + row + (int64_t)col * p.ldc));
       }
+    }
+    double acc[4][4][4];
 #pragma unroll
-      for (int nt = 0; nt < 4; ++nt) {
-        const int n = wn * 32 + nt * 8 + g;
-        b[nt] = Bs[B_KMAJ ? kmaj_off(n, k) : mnmaj_off(n, k)];
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0;
+
+    for (int kt = u.k0; kt < u.k1; ++kt, ++it) {
+      const int s = it % STAGES;
+      const uint32_t ph = (it / STAGES) & 1;
+      if (!mbar_wait(&full[s], ph, p.status)) return;
+      const double *As = tiles + s * 2 * TILE_DOUBLES;
+      const double *Bs = As + TILE_DOUBLES;
+#pragma unroll
+      for (int kk = 0; kk < BK; kk += 4) {
+        const int q = kk >> 2, q2 = q & 1;
+        double a[4][2], b[4];
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt) {
+          if constexpr (A_KMAJ) {
+            a[mt][0] = As[a_base + kv[q] + mt * 256];
+            a[mt][1] = As[a_base + kv[q] + mt * 256 + 128];
+          } else {
+            a[mt][0] = As[a_base + xa[0][q2] + mt * 256 + kk * 16];
+            a[mt][1] = As[a_base + xa[1][q2] + mt * 256 + kk * 16];
+          }
+        }
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+          if constexpr (B_KMAJ)
+            b[nt] = Bs[b_base + kv[q] + nt * 128];
+          else
+            b[nt] = Bs[b_base + xb[nt & 1][q2] + (nt >> 1) * 256 + kk * 16];
+        }
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+          for (int nt = 0; nt < 4; ++nt) dmma_16x8x4(acc[mt][nt], a[mt][0], a[mt][1], b[nt]);
       }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+    }
+
+    if (!u.owner) {
+      // publish the partial sum (fragment order: register r of consumer thread ct at
+      // [r * 256 + ct], coalesced per warp), then stamp this CTA's flag
+      double *slot = p.partial + (size_t)blockIdx.x * (64 * 256);
 #pragma unroll
       for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt) dmma_16x8x4(acc[mt][nt], a[mt][0], a[mt][1], b[nt]);
+        for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+          for (int r = 0; r < 4; ++r) slot[((mt * 4 + nt) * 4 + r) * 256 + ct] = acc[mt][nt][r];
+      __threadfence();
+      consumer_bar();
+      if (ct == 0) atomicExch(&p.flags[blockIdx.x], p.epoch);
+      continue;
     }
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[s]);
-  }
-  if (!ok) return;
-
-  // ------------------------------ epilogue ------------------------------
+    if (u.first_contrib < (int)blockIdx.x) {
+      // add the partials of the lower-numbered CTAs that computed the tile's first slabs
+      for (int c = u.first_contrib; c < (int)blockIdx.x; ++c) {
+        if (ct == 0) {
+          uint32_t i = 0;
+          while (atomicAdd(&p.flags[c], 0) != p.epoch) {
+            if (++i > MO_SPIN_LIMIT) {
+              set_status(p.status, MO_EDEVTIMEOUT);
+              s_abort = 1;
+              break;
+            }
+          }
+          __threadfence();
+        }
+        consumer_bar();
+        if (s_abort) return;
+        const double *slot = p.partial + (size_t)c * (64 * 256);
 #pragma unroll
-  for (int mt = 0; mt < 4; ++mt)
+        for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
-    for (int nt = 0; nt < 4; ++nt)
+          for (int nt = 0; nt < 4; ++nt)
 #pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int row = m0 + wm * 64 + mt * 16 + g + ((r >> 1) << 3);
-        const int col = n0 + wn * 32 + nt * 8 + 2 * t + (r & 1);
-        if (row >= p.M || col >= p.N) continue;
-        if (p.mode == kSyrkLower && row < col) continue;
-        if (p.mode == kSyrkUpper && row > col) continue;
-        double bet = p.beta;
-        if (p.beta_block > 0 && (row / p.beta_block) != (col / p.beta_block)) bet = 1.0;
-        double *cp = p.C + row + (int64_t)col * p.ldc;
-        double v = p.alpha * acc[mt][nt][r];
-        if (bet != 0.0) v = fma(bet, *cp, v);
-        *cp = v;
+            for (int r = 0; r < 4; ++r)
+              acc[mt][nt][r] += __ldcg(slot + ((mt * 4 + nt) * 4 + r) * 256 + ct);
       }
+    }
+
+    // ------------------------------ epilogue ------------------------------
+    // 16 elements at a time: all loads of C are issued before any store, so the L2 round
+    // trips overlap (stores may alias later loads, which would otherwise serialize them)
+    // C is read unless beta == 0 everywhere (with diagonal-block beta, off-block
+    // elements use beta = 1)
+    const bool need_c = p.beta != 0.0 || p.beta_block > 0;
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt) {
+      double cv[4][4];
+      bool keep[4][4];
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int row = m0 + wm * 64 + mt * 16 + g + ((r >> 1) << 3);
+          const int col = n0 + wn * 32 + nt * 8 + 2 * t + (r & 1);
+          bool k = row < p.M && col < p.N;
+          if (p.mode == kSyrkLower && row < col) k = false;
+          if (p.mode == kSyrkUpper && row > col) k = false;
+          keep[nt][r] = k;
+          cv[nt][r] = (k && need_c) ? __ldcg(p.C + row + (int64_t)col * p.ldc) : 0.0;
+        }
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          if (!keep[nt][r]) continue;
+          const int row = m0 + wm * 64 + mt * 16 + g + ((r >> 1) << 3);
+          const int col = n0 + wn * 32 + nt * 8 + 2 * t + (r & 1);
+          double bet = p.beta;
+          if (p.beta_block > 0 && (row / p.beta_block) != (col / p.beta_block)) bet = 1.0;
+          double v = p.alpha * acc[mt][nt][r];
+          if (bet != 0.0) v = fma(bet, cv[nt][r], v);
+          p.C[row + (int64_t)col * p.ldc] = v;
+        }
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -309,6 +474,9 @@ bool gemm_tma_ok(const GemmArgs &a) {
   return al(a.A) && al(a.B) && (a.lda % 2 == 0) && (a.ldb % 2 == 0) && encode_fn() != nullptr;
 }
 
+int gemm_partial_slots(int sms) { return sms; }
+size_t gemm_partial_bytes(int sms) { return (size_t)sms * 64 * 256 * sizeof(double); }
+
 int launch_gemm(const GemmArgs &a, cudaStream_t stream) {
   if (a.M <= 0 || a.N <= 0) return MO_OK;
   KParams kp;
@@ -328,14 +496,42 @@ int launch_gemm(const GemmArgs &a, cudaStream_t stream) {
   kp.status = a.status;
   const int tiles_m = (a.M + BM - 1) / BM, tiles_n = (a.N + BN - 1) / BN;
   kp.tiles_m = tiles_m;
-  long long grid;
+  kp.tiles_n = tiles_n;
+  long long T;
   if (a.mode == kGemm) {
-    grid = (long long)tiles_m * tiles_n;
+    T = (long long)tiles_m * tiles_n;
   } else {
     if (a.M != a.N) return MO_EINVAL;
-    grid = (long long)tiles_m * (tiles_m + 1) / 2;
+    T = (long long)tiles_m * (tiles_m + 1) / 2;
   }
-  if (grid <= 0 || grid > 0x7fffffffLL) return MO_EINVAL;
+  if (T <= 0 || T > 0x7fffffffLL) return MO_EINVAL;
+  kp.total_tiles = (int)T;
+  kp.kt = (kp.K + BK - 1) / BK;
+  const int sms = a.sms > 0 ? a.sms : 148;
+  // Schedule: whole tiles round-robin over persistent CTAs; when a GEMM has only a few,
+  // unequal waves (e.g. 256 tiles on 148 SMs), the last one or two waves are split along
+  // K evenly over all CTAs (stream-K) and finished by the CTA holding each tile's last slab.
+  int grid = (int)std::min<long long>(T, sms);
+  kp.dp_tiles = (int)T;
+  kp.sk_iters = 0;
+  kp.sk_chunk = 1;
+  kp.partial = a.sk_partial;
+  kp.flags = a.sk_flags;
+  kp.epoch = a.sk_epoch;
+  const long long waves = T / sms, rem = T % sms;
+  if (a.mode == kGemm && a.sk_partial && a.sk_flags && rem != 0 && waves < 4 && kp.kt >= 8) {
+    const long long dp = (waves >= 1 ? waves - 1 : 0) * sms;
+    kp.dp_tiles = (int)dp;
+    kp.sk_iters = (int)((T - dp) * kp.kt);
+    grid = sms;
+    kp.sk_chunk = (kp.sk_iters + grid - 1) / grid;
+    if (kp.sk_chunk < 4) {  // too little work per CTA: stay data-parallel
+      kp.dp_tiles = (int)T;
+      kp.sk_iters = 0;
+      kp.sk_chunk = 1;
+      grid = (int)std::min<long long>(T, sms);
+    }
+  }
 
   const bool ak = a.transA;   // op(A) stored K-major when A is transposed
   const bool bk = !a.transB;  // op(B) stored K-major when B is not transposed
@@ -346,11 +542,11 @@ int launch_gemm(const GemmArgs &a, cudaStream_t stream) {
                   : make_tmap(&ta, a.A, a.M, kp.K, a.lda, 16, 16);
     bool okB = bk ? make_tmap(&tb, a.B, kp.K, a.N, a.ldb, 16, 128)
                   : make_tmap(&tb, a.B, a.N, kp.K, a.ldb, 16, 16);
-    if (okA && okB) return dispatch<true>(ak, bk, kp, ta, tb, (int)grid, stream);
+    if (okA && okB) return dispatch<true>(ak, bk, kp, ta, tb, grid, stream);
   }
   memset(&ta, 0, sizeof(ta));
   memset(&tb, 0, sizeof(tb));
-  return dispatch<false>(ak, bk, kp, ta, tb, (int)grid, stream);
+  return dispatch<false>(ak, bk, kp, ta, tb, grid, stream);
 }
 
 }  // namespace mo

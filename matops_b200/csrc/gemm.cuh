@@ -27,6 +27,12 @@ struct GemmArgs {
   int beta_block = 0;
   int *status = nullptr;  // device status word (first error wins)
   bool force_fallback = false;  // use the cp.async producer even when TMA is legal
+  int sms = 148;                // persistent grid size
+  // stream-K scratch (nullptr: data-parallel schedule only): one 128 KB partial-sum slot
+  // and one flag per CTA, and a value unique to this launch for the flags
+  double *sk_partial = nullptr;
+  int *sk_flags = nullptr;
+  int sk_epoch = 0;
 };
 
 // Enqueue one launch on `stream`.  Returns MO_OK or a negative MO_E* code.
@@ -35,5 +41,8 @@ int launch_gemm(const GemmArgs &args, cudaStream_t stream);
 // True when the TMA producer can be used for these operands (16-byte aligned bases,
 // leading dimensions that are multiples of 2 doubles).
 bool gemm_tma_ok(const GemmArgs &args);
+
+// bytes of stream-K partial-sum scratch for a device with `sms` SMs
+size_t gemm_partial_bytes(int sms);
 
 }  // namespace mo

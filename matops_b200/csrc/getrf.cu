@@ -25,7 +25,7 @@ int trtri_blocks(mo_ctx *ctx, View A, int N, bool trans, bool lower_eff, bool un
 namespace {
 
 constexpr int PANEL_THREADS = 256;
-constexpr int MAX_PANEL_W = 64;
+constexpr int MAX_PANEL_W = 128;
 
 struct PanelScratch {
   // double-buffered per-CTA candidates: value, index, NaN-on-diagonal flag, row values

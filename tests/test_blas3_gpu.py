@@ -24,10 +24,10 @@ def host(t):
 
 @pytest.mark.parametrize("flags", [0, TA, TB, TA | TB])
 @pytest.mark.parametrize("m,n,k", [(2048, 2048, 2048), (137, 91, 213), (1, 1, 1), (128, 128, 16),
-                                   (129, 257, 65), (300, 5, 1000), (7, 300, 3)])
+                                   (129, 257, 65), (300, 5, 1000), (7, 300, 3),
+                                   # few-wave shapes: K split over CTAs (stream-K partial sums)
+                                   (1536, 1536, 256), (1280, 1408, 400), (1000, 700, 1333)])
 def test_mult(gpu, oracle, rng, flags, m, n, k):
-    if m * n * k > 2e8 and flags != 0:
-        pytest.skip("large case only for NoTrans")
     A = colmajor(rng.uniform(-1, 1, (k, m) if flags & TA else (m, k)))
     B = colmajor(rng.uniform(-1, 1, (n, k) if flags & TB else (k, n)))
     C0 = colmajor(rng.uniform(-1, 1, (m, n)))
