@@ -55,6 +55,7 @@ extern "C" {
 #define MO_EDEVTIMEOUT (-21) /* a bounded device-side wait gave up                    */
 #define MO_ENOMEM (-22)      /* device allocation failed                              */
 #define MO_ENOKERNEL (-23)   /* no sm_100a kernel image for this device               */
+#define MO_ESTATICLIMIT (-11) /* larger than the fixed scratch of mo_solve_trm_static   */
 
 typedef struct mo_ctx mo_ctx;
 
@@ -168,6 +169,27 @@ MO_API int mo_decompose_lu(mo_ctx *ctx, mo_matrix A, int64_t *pivots, int64_t np
  * L^-T then U^-T, exactly the reference's sequence. */
 MO_API int mo_solve_lu(mo_ctx *ctx, mo_matrix B, mo_matrix A, const int64_t *pivots, int64_t npiv,
                 int flags);
+
+/* ---- allocation-free variant (no counterpart in the reference) ---- */
+
+/* Largest order of A accepted by mo_solve_trm_static. */
+#define MO_SOLVE_TRM_STATIC_MAX_N 1024
+
+/* mo_solve_trm_static: the triangular solve of mo_solve_trm (same arguments, flags, size
+ * checks and results) for callers that must not have a library allocate device memory --
+ * e.g. an application whose GPU memory is all handed out by its own pool allocator, a
+ * service held to a fixed footprint on a shared GPU, or a latency-critical loop that cannot
+ * pay for cudaMalloc's implicit synchronization.  It needs no context and calls no
+ * allocation routine: its only scratch is a 1 MiB block compiled into this library, which
+ * every GPU that loads the library keeps until the process exits.
+ *   - order of A (A's column count) > MO_SOLVE_TRM_STATIC_MAX_N -> MO_ESTATICLIMIT.
+ *   - runs on `stream` (a cudaStream_t, NULL = legacy default stream) of the current device
+ *     and waits for it; returns 0, a size error, or a device-side failure code.
+ *   - every call on a device uses the same block, which keeps the previous call's data:
+ *     calls that overlap on the GPU race; serialize them.
+ *   - the first call on each device looks the block up with that device current; make it
+ *     before any stream capture begins. */
+MO_API int mo_solve_trm_static(mo_matrix B, mo_matrix A, double alpha, int flags, void *stream);
 
 #ifdef __cplusplus
 }

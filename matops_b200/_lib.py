@@ -61,6 +61,7 @@ def lib() -> ctypes.CDLL:
         "mo_profile_enable": [p, i],
         "mo_profile_read": [p, ctypes.POINTER(MoProfile)],
         "mo_measure_fp64_peak": [p, d, ctypes.POINTER(d)],
+        "mo_solve_trm_static": [M, M, d, i, p],
     }
     for name, args in sigs.items():
         fn = getattr(L, name)

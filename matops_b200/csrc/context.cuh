@@ -72,5 +72,7 @@ int syrk(mo_ctx *ctx, View C, View A, bool ta, bool upper, double alpha, double 
 
 // B = alpha*op(A)^-1*B (left) or alpha*B*op(A)^-1 (right); A n x n triangle
 int trsm(mo_ctx *ctx, View B, View A, int flags, double alpha);
+// the same with caller-provided scratch for the ceil(n/128) inverted 128 x 128 blocks
+int trsm_with_scratch(mo_ctx *ctx, View B, View A, int flags, double alpha, double *inv);
 
 }  // namespace mo

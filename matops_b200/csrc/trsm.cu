@@ -67,6 +67,19 @@ int trtri_blocks(mo_ctx *ctx, View A, int N, bool trans, bool lower_eff, bool un
 
 int trsm(mo_ctx *ctx, View B, View A, int flags, double alpha) {
   const int N = A.cols;
+  const int nrhs = (flags & MO_RIGHT) ? B.rows : B.cols;
+  if (N == 0 || nrhs == 0) return MO_OK;
+  const int nblk = (N + NBT - 1) / NBT;
+  double *inv = nullptr;
+  int rc = workspace(ctx, (size_t)nblk * NBT * NBT * sizeof(double), (void **)&inv);
+  if (rc) return rc;
+  return trsm_with_scratch(ctx, B, A, flags, alpha, inv);
+}
+
+// The sweep of trsm() with the caller's scratch for the inverted diagonal blocks
+// (ceil(N/128) blocks of 128 x 128 doubles).
+int trsm_with_scratch(mo_ctx *ctx, View B, View A, int flags, double alpha, double *inv) {
+  const int N = A.cols;
   const bool right = (flags & MO_RIGHT) != 0;
   const bool upper = (flags & MO_UPPER) != 0;
   const bool tr = (flags & MO_TRANSA) != 0;
@@ -75,10 +88,7 @@ int trsm(mo_ctx *ctx, View B, View A, int flags, double alpha) {
   const int nrhs = right ? B.rows : B.cols;
   if (N == 0 || nrhs == 0) return MO_OK;
   const int nblk = (N + NBT - 1) / NBT;
-  double *inv = nullptr;
-  int rc = workspace(ctx, (size_t)nblk * NBT * NBT * sizeof(double), (void **)&inv);
-  if (rc) return rc;
-  rc = trtri_blocks(ctx, A, N, tr, lower_eff, unit, inv);
+  int rc = trtri_blocks(ctx, A, N, tr, lower_eff, unit, inv);
   if (rc) return rc;
   // op(A)[r:r+nr, c:c+nc] as a stored view, transposed iff tr
   auto opA = [&](int r, int c, int nr, int nc) -> View {
