@@ -55,7 +55,8 @@ int workspace(mo_ctx *ctx, size_t bytes, void **out) {
 
 static Control *control(mo_ctx *ctx) { return reinterpret_cast<Control *>(ctx->d_status); }
 
-int gemm(mo_ctx *ctx, View C, View A, bool ta, View B, bool tb, double alpha, double beta) {
+int gemm_ex(mo_ctx *ctx, View C, View A, bool ta, View B, bool tb, double alpha, double beta,
+            const GemmOpts &o) {
   GemmArgs g;
   g.M = C.rows;
   g.N = C.cols;
@@ -70,48 +71,57 @@ int gemm(mo_ctx *ctx, View C, View A, bool ta, View B, bool tb, double alpha, do
   g.transB = tb;
   g.C = C.d;
   g.ldc = C.ld;
-  g.mode = kGemm;
+  g.mode = o.mode;
+  g.beta_block = o.beta_block;
   g.status = &control(ctx)->status;
   g.sms = ctx->sms;
-  g.sk_partial = ctx->sk_partial;
-  g.sk_flags = ctx->sk_flags;
-  g.sk_epoch = ++ctx->sk_epoch;
+  g.max_ctas = o.max_ctas;
+  if (o.stream_k && o.mode == kGemm) {
+    g.sk_partial = ctx->sk_partial;
+    g.sk_flags = ctx->sk_flags;
+    g.sk_epoch = ++ctx->sk_epoch;
+  }
   if (g.M <= 0 || g.N <= 0) return MO_OK;
   ProfScope ps;
   prof_begin(ctx, ps, MO_PROF_GEMM);
   const int rc = launch_gemm(g, ctx->stream);
   const double M = g.M, N = g.N, K = g.K;
-  prof_end(ctx, ps, 2.0 * M * N * K, 8.0 * (M * K + K * N + M * N * (beta != 0.0 ? 2 : 1)));
+  const bool tri = (o.mode == kSyrkLower || o.mode == kSyrkUpper);
+  const double elems = tri ? N * (N + 1) / 2 : M * N;
+  prof_end(ctx, ps, 2.0 * elems * K,
+           8.0 * (M * K + (tri ? 0.0 : K * N) + elems * (beta != 0.0 ? 2 : 1)));
   return rc;
+}
+
+int gemm(mo_ctx *ctx, View C, View A, bool ta, View B, bool tb, double alpha, double beta) {
+  return gemm_ex(ctx, C, A, ta, B, tb, alpha, beta, GemmOpts());
 }
 
 int syrk(mo_ctx *ctx, View C, View A, bool ta, bool upper, double alpha, double beta,
          int beta_block) {
-  GemmArgs g;
-  g.M = C.rows;
-  g.N = C.cols;
-  g.K = ta ? A.rows : A.cols;
-  g.alpha = alpha;
-  g.beta = beta;
-  g.A = A.d;
-  g.lda = A.ld;
-  g.transA = ta;
-  g.B = A.d;
-  g.ldb = A.ld;
-  g.transB = !ta;
-  g.C = C.d;
-  g.ldc = C.ld;
-  g.mode = upper ? kSyrkUpper : kSyrkLower;
-  g.beta_block = beta_block;
-  g.status = &control(ctx)->status;
-  g.sms = ctx->sms;
-  if (g.N <= 0) return MO_OK;
-  ProfScope ps;
-  prof_begin(ctx, ps, MO_PROF_GEMM);
-  const int rc = launch_gemm(g, ctx->stream);
-  const double N = g.N, K = g.K, tri = N * (N + 1) / 2;
-  prof_end(ctx, ps, 2.0 * tri * K, 8.0 * (N * K + tri * (beta != 0.0 ? 2 : 1)));
-  return rc;
+  GemmOpts o;
+  o.mode = upper ? kSyrkUpper : kSyrkLower;
+  o.beta_block = beta_block;
+  return gemm_ex(ctx, C, A, ta, A, !ta, alpha, beta, o);
+}
+
+int aux_stream(mo_ctx *ctx, cudaStream_t *out) {
+  if (!ctx->aux) {
+    int lo = 0, hi = 0;
+    MO_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    MO_CUDA_TRY(cudaStreamCreateWithPriority(&ctx->aux, cudaStreamNonBlocking, hi));
+    MO_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+    MO_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
+  }
+  *out = ctx->aux;
+  return MO_OK;
+}
+
+int stream_wait(mo_ctx *ctx, cudaStream_t waiter, cudaStream_t producer, cudaEvent_t ev) {
+  (void)ctx;
+  MO_CUDA_TRY(cudaEventRecord(ev, producer));
+  MO_CUDA_TRY(cudaStreamWaitEvent(waiter, ev, 0));
+  return MO_OK;
 }
 
 }  // namespace mo
@@ -158,6 +168,12 @@ int mo_ctx_destroy(mo_ctx *ctx) {
   if (ctx->sk_partial) cudaFree(ctx->sk_partial);
   if (ctx->sk_flags) cudaFree(ctx->sk_flags);
   for (auto e : ctx->ev_pool) cudaEventDestroy(e);
+  if (ctx->aux) {
+    cudaStreamSynchronize(ctx->aux);
+    cudaStreamDestroy(ctx->aux);
+  }
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
   delete ctx;
   return MO_OK;
 }

@@ -18,6 +18,9 @@ struct mo_ctx {
   void *ws = nullptr;
   size_t ws_bytes = 0;
   int sms = 148;
+  // second, high-priority stream for look-ahead panels, and fork/join events
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // stream-K scratch of the GEMM engine (allocated with the context)
   double *sk_partial = nullptr;
   int *sk_flags = nullptr;
@@ -65,6 +68,30 @@ int workspace(mo_ctx *ctx, size_t bytes, void **out);
 
 // C = alpha*op(A)*op(B) + beta*C on device views (sizes already checked)
 int gemm(mo_ctx *ctx, View C, View A, bool ta, View B, bool tb, double alpha, double beta);
+
+// the same with engine options: masked modes, a cap on the persistent grid (to leave SMs
+// to another stream), and whether the stream-K schedule may be used
+struct GemmOpts {
+  int mode = kGemm;
+  int max_ctas = 0;
+  bool stream_k = true;
+  int beta_block = 0;
+};
+int gemm_ex(mo_ctx *ctx, View C, View A, bool ta, View B, bool tb, double alpha, double beta,
+            const GemmOpts &o);
+
+// temporarily launch the context's work on another stream
+struct StreamSwap {
+  mo_ctx *c;
+  cudaStream_t old;
+  StreamSwap(mo_ctx *ctx, cudaStream_t s) : c(ctx), old(ctx->stream) { ctx->stream = s; }
+  ~StreamSwap() { c->stream = old; }
+};
+
+// the context's auxiliary stream (created on first use, highest priority)
+int aux_stream(mo_ctx *ctx, cudaStream_t *out);
+// make `waiter` wait for all work enqueued so far on `producer`
+int stream_wait(mo_ctx *ctx, cudaStream_t waiter, cudaStream_t producer, cudaEvent_t ev);
 
 // triangle(C) = alpha*op(A)*op(A)^T + beta*C; beta_block as in GemmArgs
 int syrk(mo_ctx *ctx, View C, View A, bool ta, bool upper, double alpha, double beta,

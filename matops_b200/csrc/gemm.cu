@@ -97,7 +97,7 @@ __device__ __forceinline__ void load_slab_cpasync(double *dst, const double *src
 }
 
 __device__ __forceinline__ void tile_coords(const KParams &p, int t, int &tm, int &tn) {
-  if (p.mode == kGemm) {
+  if (p.mode == kGemm || p.mode == kGemmLower || p.mode == kGemmUpper) {
     // groups of GROUP_M tile rows, column-major inside a group: a wave of persistent CTAs
     // touches GROUP_M row panels of A and a narrow band of B, which stay in L2
     constexpr int GROUP_M = 8;
@@ -381,8 +381,8 @@ __global__ void __launch_bounds__(THREADS, 1)
           const int row = m0 + wm * 64 + mt * 16 + g + ((r >> 1) << 3);
           const int col = n0 + wn * 32 + nt * 8 + 2 * t + (r & 1);
           bool k = row < p.M && col < p.N;
-          if (p.mode == kSyrkLower && row < col) k = false;
-          if (p.mode == kSyrkUpper && row > col) k = false;
+          if ((p.mode == kSyrkLower || p.mode == kGemmLower) && row < col) k = false;
+          if ((p.mode == kSyrkUpper || p.mode == kGemmUpper) && row > col) k = false;
           keep[nt][r] = k;
           cv[nt][r] = (k && need_c) ? __ldcg(p.C + row + (int64_t)col * p.ldc) : 0.0;
         }
@@ -498,7 +498,7 @@ int launch_gemm(const GemmArgs &a, cudaStream_t stream) {
   kp.tiles_m = tiles_m;
   kp.tiles_n = tiles_n;
   long long T;
-  if (a.mode == kGemm) {
+  if (a.mode == kGemm || a.mode == kGemmLower || a.mode == kGemmUpper) {
     T = (long long)tiles_m * tiles_n;
   } else {
     if (a.M != a.N) return MO_EINVAL;
@@ -507,7 +507,8 @@ int launch_gemm(const GemmArgs &a, cudaStream_t stream) {
   if (T <= 0 || T > 0x7fffffffLL) return MO_EINVAL;
   kp.total_tiles = (int)T;
   kp.kt = (kp.K + BK - 1) / BK;
-  const int sms = a.sms > 0 ? a.sms : 148;
+  int sms = a.sms > 0 ? a.sms : 148;
+  if (a.max_ctas > 0 && a.max_ctas < sms) sms = a.max_ctas;
   // Schedule: whole tiles round-robin over persistent CTAs; when a GEMM has only a few,
   // unequal waves (e.g. 256 tiles on 148 SMs), the last one or two waves are split along
   // K evenly over all CTAs (stream-K) and finished by the CTA holding each tile's last slab.

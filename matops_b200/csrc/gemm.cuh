@@ -9,6 +9,8 @@ enum GemmMode : int {
   kGemm = 0,       // C[M,N] = alpha*op(A)*op(B) + beta*C
   kSyrkLower = 1,  // only tiles / elements with row >= col are computed and written
   kSyrkUpper = 2,  // only row <= col
+  kGemmLower = 3,  // rectangular tiles of C, elements with row < col left untouched
+  kGemmUpper = 4,  // rectangular tiles of C, elements with row > col left untouched
 };
 
 struct GemmArgs {
@@ -28,6 +30,7 @@ struct GemmArgs {
   int *status = nullptr;  // device status word (first error wins)
   bool force_fallback = false;  // use the cp.async producer even when TMA is legal
   int sms = 148;                // persistent grid size
+  int max_ctas = 0;             // > 0: cap the persistent grid (leave SMs to other streams)
   // stream-K scratch (nullptr: data-parallel schedule only): one 128 KB partial-sum slot
   // and one flag per CTA, and a value unique to this launch for the flags
   double *sk_partial = nullptr;
