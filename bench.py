@@ -75,6 +75,23 @@ def run_case(args):
         A.uniform_(-1.0, 1.0, generator=g)
         C.uniform_(-1.0, 1.0, generator=g)
         fn, flops = (lambda: mo.RankUpdateSym(C, A, -1.0, 1.0, LOWER)), float(n) * n * k
+    elif kind == "dpotrs":
+        n, nrhs = dims
+        G = mo.matrix(n, n)
+        G.normal_(generator=g)
+        A = mo.matrix(n, n)
+        mo.Mult(A, G, G, 1.0 / n, 0.0, mo.TRANSB)
+        A.diagonal().add_(0.5)
+        del G
+        mo.DecomposeCHOL(A, LOWER, 64)
+        B0 = mo.matrix(n, nrhs)
+        B0.uniform_(-1.0, 1.0, generator=g)
+        B = mo.matrix(n, nrhs)
+
+        def fn():
+            B.copy_(B0)
+            mo.SolveCHOL(B, A, LOWER)
+        flops = 2.0 * 2.0 * n * n * nrhs
     elif kind in ("dpotrf", "dgetrf"):
         n = dims[0]
         A0 = mo.matrix(n, n)

@@ -65,14 +65,21 @@ int trtri_blocks(mo_ctx *ctx, View A, int N, bool trans, bool lower_eff, bool un
   return MO_OK;
 }
 
+int trsm_few(mo_ctx *ctx, View B, View A, int flags, double alpha, double *inv, int *flag_buf);
+
 int trsm(mo_ctx *ctx, View B, View A, int flags, double alpha) {
   const int N = A.cols;
   const int nrhs = (flags & MO_RIGHT) ? B.rows : B.cols;
   if (N == 0 || nrhs == 0) return MO_OK;
   const int nblk = (N + NBT - 1) / NBT;
+  const size_t inv_bytes = (size_t)nblk * NBT * NBT * sizeof(double);
   double *inv = nullptr;
-  int rc = workspace(ctx, (size_t)nblk * NBT * NBT * sizeof(double), (void **)&inv);
+  int rc = workspace(ctx, inv_bytes + sizeof(int) * (2 * nblk + 64), (void **)&inv);
   if (rc) return rc;
+  // few right-hand sides: one cooperative launch instead of a sweep of 2*nblk GEMMs
+  if (nblk > 1 && nrhs <= 64)
+    return trsm_few(ctx, B, A, flags, alpha, inv,
+                    reinterpret_cast<int *>(reinterpret_cast<char *>(inv) + inv_bytes));
   return trsm_with_scratch(ctx, B, A, flags, alpha, inv);
 }
 
