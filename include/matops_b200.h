@@ -94,7 +94,9 @@ MO_API int mo_set_syrk_blas_beta(mo_ctx *ctx, int on);
 #define MO_PROF_PANEL 3    /* LU panel (pivot search, interchanges, rank-1 updates)      */
 #define MO_PROF_LASWP 4    /* row interchanges outside the panel                        */
 #define MO_PROF_OTHER 5
-#define MO_PROF_CLASSES 6
+#define MO_PROF_LPGEMM 6   /* split-product (BF16x3 / TF32x3) GEMMs and operand splits  */
+#define MO_PROF_IR 7       /* refinement: FP64 residuals, norms, GMRES vector kernels   */
+#define MO_PROF_CLASSES 8
 typedef struct mo_profile {
   int64_t launches[MO_PROF_CLASSES]; /* kernel launches since the last reset            */
   double ms[MO_PROF_CLASSES];        /* summed device time (only while enabled)         */
@@ -169,6 +171,50 @@ MO_API int mo_decompose_lu(mo_ctx *ctx, mo_matrix A, int64_t *pivots, int64_t np
  * L^-T then U^-T, exactly the reference's sequence. */
 MO_API int mo_solve_lu(mo_ctx *ctx, mo_matrix B, mo_matrix A, const int64_t *pivots, int64_t npiv,
                 int flags);
+
+/* ---- mixed-precision Cholesky solve with FP64 refinement (no counterpart in the
+ * reference; LAPACK's dsposv is the model) ---- */
+
+/* low-precision factor arithmetic: every O(n^3) product is formed from three tensor-core
+ * products of split operands with FP32 accumulation, on an FP32 copy of A */
+#define MO_PREC_BF16X3 1 /* x = bf16 hi + bf16 lo (about 16 significant bits)     */
+#define MO_PREC_TF32X3 2 /* x = tf32 hi + tf32 lo (FP32 accuracy: "FP32" factor)   */
+/* refinement method (low byte) and option bits */
+#define MO_IR_AUTO 0          /* classic refinement, GMRES-IR once it converges slowly  */
+#define MO_IR_CLASSIC 1       /* x += (L L^T)^-1 (b - A x)                              */
+#define MO_IR_GMRES 2         /* x += GMRES(A, b - A x) preconditioned by (L L^T)^-1    */
+#define MO_IR_NO_FALLBACK 0x100 /* do not re-solve in FP64 when refinement fails      */
+#define MO_IR_HISTORY 32
+typedef struct mo_ir_info {
+  int iters;        /* refinement steps taken (corrections applied)                    */
+  int gmres_iters;  /* inner GMRES iterations, summed over the steps                   */
+  int converged;    /* 1 if berr <= tol                                                */
+  int fallback;     /* 1 if X came from the FP64 factorization (DecomposeCHOL path)    */
+  int shifts;       /* low-precision factorizations retried with a diagonal shift      */
+  int method;       /* MO_IR_CLASSIC or MO_IR_GMRES: the method of the last step       */
+  double berr;      /* max over columns of |b - A x|_inf / (|A|_inf |x|_inf + |b|_inf) */
+  double shift;     /* relative diagonal shift of the factored matrix (0 = none)       */
+  double history[MO_IR_HISTORY]; /* berr before each step (history[0]: x = 0)          */
+} mo_ir_info;
+/* X = A^-1 B for symmetric positive definite A (n x n, float64; only the triangle that
+ * flags selects, MO_LOWER (default) or MO_UPPER, is read; A is not modified).  A is
+ * factored as L L^T in the low precision `prec` and X is refined in FP64 until the
+ * normwise backward error is <= tol, for at most maxit steps (method as above).  If the
+ * low-precision factorization breaks down, it is retried on A + s*diag(A) with a growing
+ * relative shift s.  Unless MO_IR_NO_FALLBACK is set, a solve that does not converge is
+ * redone with the FP64 factorization.  B and X are n x nrhs (X may be B).  Returns 0, a
+ * size/argument error, or i > 0 if the FP64 fallback found A not positive definite at
+ * column i - 1.  `info` may be NULL.  Synchronous. */
+MO_API int mo_dsposv_ir(mo_ctx *ctx, mo_matrix X, mo_matrix A, mo_matrix B, int flags, int prec,
+                        int method, double tol, int maxit, mo_ir_info *info);
+
+/* The split-product GEMM of the factorization as a plain operation on FP32 data:
+ * C = alpha*op(A)*op(B) + beta*C, C M x N, op(A) M x K, op(B) K x N, column-major float
+ * device arrays; flags: MO_TRANSA, MO_TRANSB, and MO_LOWER to update only C(i, j) with
+ * i >= j (N <= M).  Asynchronous on the context's stream. */
+MO_API int mo_lp_gemm(mo_ctx *ctx, int prec, int64_t M, int64_t N, int64_t K, float alpha,
+                      const float *A, int64_t lda, const float *B, int64_t ldb, float beta,
+                      float *C, int64_t ldc, int flags);
 
 /* ---- allocation-free variant (no counterpart in the reference) ---- */
 

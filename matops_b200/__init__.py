@@ -9,5 +9,6 @@ from .api import (  # noqa: F401
     BlockingParams, DecomposeBlockSize, DecomposeCHOL, DecomposeLU, MatopsError, MatopsPanic,
     Mult, NumWorkers, RankUpdateSym, SetPanicOnError, SolveCHOL, SolveLU, SolveTrm, Sync,
     matrix, to_device, view, Upload, Download, host_matrix, Profile, ProfileEnable, ProfileRead,
-    MeasureFP64Peak,
+    MeasureFP64Peak, PREC_BF16X3, PREC_TF32X3, IR_AUTO, IR_CLASSIC, IR_GMRES, IR_NO_FALLBACK,
+    IRInfo, SolveCHOLMixed, LPGemm,
 )

@@ -19,8 +19,17 @@ class MoMatrix(ctypes.Structure):
 
 class MoProfile(ctypes.Structure):
     """mo_profile: per-class launches, device ms, algorithmic flops and bytes."""
-    _fields_ = [("launches", ctypes.c_int64 * 6), ("ms", ctypes.c_double * 6),
-                ("flops", ctypes.c_double * 6), ("bytes", ctypes.c_double * 6)]
+    _fields_ = [("launches", ctypes.c_int64 * 8), ("ms", ctypes.c_double * 8),
+                ("flops", ctypes.c_double * 8), ("bytes", ctypes.c_double * 8)]
+
+
+class MoIRInfo(ctypes.Structure):
+    """mo_ir_info: outcome of mo_dsposv_ir."""
+    _fields_ = [("iters", ctypes.c_int), ("gmres_iters", ctypes.c_int),
+                ("converged", ctypes.c_int), ("fallback", ctypes.c_int),
+                ("shifts", ctypes.c_int), ("method", ctypes.c_int),
+                ("berr", ctypes.c_double), ("shift", ctypes.c_double),
+                ("history", ctypes.c_double * 32)]
 
 
 _lib = None
@@ -62,6 +71,9 @@ def lib() -> ctypes.CDLL:
         "mo_profile_read": [p, ctypes.POINTER(MoProfile)],
         "mo_measure_fp64_peak": [p, d, ctypes.POINTER(d)],
         "mo_solve_trm_static": [M, M, d, i, p],
+        "mo_dsposv_ir": [p, M, M, M, i, i, i, d, i, ctypes.POINTER(MoIRInfo)],
+        "mo_lp_gemm": [p, i, i64, i64, i64, ctypes.c_float, p, i64, p, i64, ctypes.c_float, p,
+                       i64, i],
     }
     for name, args in sigs.items():
         fn = getattr(L, name)

@@ -168,6 +168,67 @@ def SolveLU(B, A, pivots: torch.Tensor, flags: int):
     return _err(rc)
 
 
+# ---- mixed precision (no counterpart in the reference; LAPACK dsposv is the model) ----
+
+PREC_BF16X3, PREC_TF32X3 = 1, 2
+IR_AUTO, IR_CLASSIC, IR_GMRES, IR_NO_FALLBACK = 0, 1, 2, 0x100
+
+
+class IRInfo:
+    """Outcome of SolveCHOLMixed (mo_ir_info)."""
+
+    def __init__(self, raw):
+        self.iters = raw.iters
+        self.gmres_iters = raw.gmres_iters
+        self.converged = bool(raw.converged)
+        self.fallback = bool(raw.fallback)
+        self.shifts = raw.shifts
+        self.method = raw.method
+        self.berr = raw.berr
+        self.shift = raw.shift
+        self.history = [raw.history[i] for i in range(min(32, raw.iters + 1))]
+
+    def __repr__(self):
+        return (f"IRInfo(iters={self.iters}, gmres_iters={self.gmres_iters}, "
+                f"converged={self.converged}, fallback={self.fallback}, shifts={self.shifts}, "
+                f"method={self.method}, berr={self.berr:.3e}, shift={self.shift:.3e})")
+
+
+def SolveCHOLMixed(X, A, B, flags: int = LOWER, prec: int = PREC_TF32X3, method: int = IR_AUTO,
+                   tol: float = 1e-14, maxit: int = 30):
+    """X = A^-1 B for SPD A: low-precision Cholesky (BF16x3 or TF32x3 split products on the
+    tensor cores) refined in FP64 (classic IR / GMRES-IR).  Only the triangle selected by
+    flags (LOWER or UPPER) is read; A is not modified.  Returns (IRInfo, err); a matrix
+    that is not positive definite in FP64 raises MatopsPanic like DecomposeCHOL."""
+    info = _lib.MoIRInfo()
+    rc = _lib.lib().mo_dsposv_ir(context(), view(X), view(A), view(B), flags, prec, method, tol,
+                                 maxit, ctypes.byref(info))
+    if rc > 0:
+        raise MatopsPanic(f"illegal value at {rc - 1}")
+    return IRInfo(info), _err(rc)
+
+
+def _fview(t: torch.Tensor):
+    if t.dim() != 2 or t.dtype != torch.float32 or not t.is_cuda:
+        raise TypeError("expected a 2-D float32 CUDA tensor")
+    r, c = t.shape
+    if r > 1 and t.stride(0) != 1:
+        raise TypeError("matrix view must be column-major (stride(0) == 1)")
+    ld = t.stride(1) if c > 1 else max(t.stride(1), r, 1)
+    return ctypes.c_void_p(t.data_ptr()), max(ld, r, 1)
+
+
+def LPGemm(C, A, B, alpha: float, beta: float, flags: int = NOTRANS, prec: int = PREC_TF32X3):
+    """C = beta*C + alpha*op(A)*op(B) on column-major float32 CUDA tensors with the
+    split-product tensor-core arithmetic of the mixed-precision factorization; LOWER in
+    flags updates only C(i, j) with i >= j."""
+    m, n = C.shape
+    k = A.shape[0] if flags & TRANSA else A.shape[1]
+    (pa, lda), (pb, ldb), (pc, ldc) = _fview(A), _fview(B), _fview(C)
+    return _err(_lib.lib().mo_lp_gemm(context(), prec, m, n, k, alpha, pa, lda, pb, ldb, beta, pc,
+                                      ldc, flags))
+
+
 def Sync() -> int:
     """Wait for the context's stream; returns the first device-side status recorded."""
     return _lib.lib().mo_sync(context())
@@ -208,7 +269,7 @@ def host_matrix(rows: int, cols: int, pinned: bool = True) -> torch.Tensor:
 
 class Profile:
     """Per-kernel-class launches / device time / algorithmic work (mo_profile)."""
-    CLASSES = ("gemm", "diag", "trtri", "panel", "laswp", "other")
+    CLASSES = ("gemm", "diag", "trtri", "panel", "laswp", "other", "lpgemm", "ir")
 
     def __init__(self, raw):
         self.launches = {k: int(raw.launches[i]) for i, k in enumerate(self.CLASSES)}

@@ -11,14 +11,6 @@ int potrf(mo_ctx *ctx, View A, bool upper, int *d_info, double *d_bad, double *i
 int getrf(mo_ctx *ctx, View A, int64_t *piv, int64_t npiv, int ref_nb);
 int laswp_forward(mo_ctx *ctx, View B, const int64_t *piv, int64_t npiv);
 
-namespace {
-// control block in device memory: [0] status word, [1] info, [2..3] bad pivot value
-struct Control {
-  int status;
-  int info;
-  double bad;
-};
-}  // namespace
 
 int to_view(const mo_matrix &m, View &v) {
   if (m.rows < 0 || m.cols < 0 || m.rows > INT_MAX || m.cols > INT_MAX) return MO_EINVAL;
@@ -53,7 +45,6 @@ int workspace(mo_ctx *ctx, size_t bytes, void **out) {
   return MO_OK;
 }
 
-static Control *control(mo_ctx *ctx) { return reinterpret_cast<Control *>(ctx->d_status); }
 
 int gemm_ex(mo_ctx *ctx, View C, View A, bool ta, View B, bool tb, double alpha, double beta,
             const GemmOpts &o) {
@@ -164,6 +155,7 @@ int mo_ctx_destroy(mo_ctx *ctx) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   if (ctx->ws) cudaFree(ctx->ws);
+  if (ctx->ws_ir) cudaFree(ctx->ws_ir);
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->sk_partial) cudaFree(ctx->sk_partial);
   if (ctx->sk_flags) cudaFree(ctx->sk_flags);

@@ -35,9 +35,22 @@ struct mo_ctx {
   std::vector<cudaEvent_t> ev_pool;
   size_t ev_used = 0;
   std::vector<Pending> pending;
+  // workspace of the mixed-precision solver (separate from `ws`, which the FP64 routines
+  // it may call for a fallback grow and reallocate)
+  void *ws_ir = nullptr;
+  size_t ws_ir_bytes = 0;
 };
 
 namespace mo {
+
+// control block in device memory (ctx->d_status): status word, factorization info, value
+// of the failing pivot
+struct Control {
+  int status;
+  int info;
+  double bad;
+};
+inline Control *control(mo_ctx *ctx) { return reinterpret_cast<Control *>(ctx->d_status); }
 
 // brackets one kernel launch for tracing: counts it and, when tracing is on, records
 // CUDA events around it on the context's stream

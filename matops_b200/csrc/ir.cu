@@ -1,0 +1,661 @@
+// Mixed-precision Cholesky solve with FP64 iterative refinement (mo_dsposv_ir).
+//
+// The factor L comes from lpchol.cu (split-product GEMMs on an FP32 copy of A, FP64
+// diagonal blocks).  Everything that decides the accuracy runs in FP64 on the device:
+//   residual   r = b - A x      sym_apply_kernel reads only the stored triangle of A
+//   correction d = M^-1 r       M = L L^T: two triangular solves that read the FP32 L and
+//                               compute in FP64 (trsm_few.cu)
+//              or d = GMRES(A, r) left-preconditioned by M^-1, restarted after
+//                               kGmresMax iterations, classical Gram-Schmidt applied twice
+//   update     x += d
+//   stop       berr = |r|_inf / (|A|_inf |x|_inf + |b|_inf) <= tol (max over columns)
+// Classic refinement converges while kappa(A) * u_factor << 1; GMRES-IR (Carson and
+// Higham, SIAM J. Sci. Comput. 40 (2018) A817-A847) extends this to kappa(A) near
+// u_factor^-2.  If the low-precision factorization meets a non-positive pivot, it is
+// redone on A + s*diag(A) (the shift of Higham and Pranesh, SIAM J. Sci. Comput. 43 (2021)
+// A258-A277) with s growing 8x per retry.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "lpchol.cuh"
+
+namespace mo {
+int potrf(mo_ctx *ctx, View A, bool upper, int *d_info, double *d_bad, double *inv);
+int trsm_few_f32(mo_ctx *ctx, View B, const float *L, int64_t ldl, int N, bool trans,
+                 const double *inv_L, int *flag_buf);
+
+namespace {
+
+constexpr int RR = 64;    // rows of A per CTA in sym_apply
+constexpr int RT = 32;    // tile depth
+constexpr int RNR = 16;   // right-hand sides per launch
+constexpr int kGmresMax = 60;
+constexpr int DOT_ROWS = 1024;
+
+// Y = Bv + sa * op|A| X for symmetric A stored as its lower (UP == false) or upper
+// triangle; ABS uses |A|.  CTA b owns rows r0 = 64 b .. r0 + 63.  It reads its row strip
+// L(r0.., 0..r0+63) (masked to j <= r) and its column strip L(r0.., r0..)^T (masked to
+// i > r), so every stored element is read twice over the grid and never mirrored in
+// memory.  Tiles are 32 deep, staged in shared memory from loads that are coalesced in
+// either storage; the next tile is fetched into registers while the current one is used.
+// Thread (r, q) = (tid % 64, tid / 64) accumulates 8 of each tile's 32 depth indices for
+// all right-hand sides; the four partial sums per row are added at the end in fixed order.
+struct SymArgs {
+  const double *A;
+  int64_t lda;
+  int n;
+  const double *X;
+  int64_t ldx;
+  const double *Bv;  // may be null (0)
+  int64_t ldb;
+  double *Y;
+  int64_t ldy;
+  int nr;
+  double sa;
+};
+
+template <bool UP, bool ABS>
+__global__ void __launch_bounds__(256) sym_apply_kernel(SymArgs p) {
+  // the tile buffers and, after the last tile, the cross-q reduction share one block
+  __shared__ double buf[4 * RR * (RNR + 1)];
+  double(*T)[RR + 1] = reinterpret_cast<double(*)[RR + 1]>(buf);
+  double(*Xs)[RNR] = reinterpret_cast<double(*)[RNR]>(buf + RT * (RR + 1));
+  double(*red)[RR][RNR + 1] = reinterpret_cast<double(*)[RR][RNR + 1]>(buf);
+  const int r = threadIdx.x & 63, q = threadIdx.x >> 6;
+  const int r0 = blockIdx.x * RR;
+  const int n = p.n;
+  const int t1 = (min(r0 + RR, n) + RT - 1) / RT;
+  const int ntile = t1 + (n - r0 + RT - 1) / RT;
+  double acc[RNR];
+#pragma unroll
+  for (int c = 0; c < RNR; ++c) acc[c] = 0.0;
+  double av[8], xv[2];
+  auto fetch = [&](int t) {
+    const bool ph1 = t < t1;
+    const int base = ph1 ? t * RT : r0 + (t - t1) * RT;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int e = threadIdx.x + u * 256;
+      int a, b;
+      bool use;
+      int row, col;
+      if (ph1) {  // L(r0 + b, base + a), j <= r
+        if (!UP) { b = e % RR; a = e / RR; } else { a = e % RT; b = e / RT; }
+        row = r0 + b;
+        col = base + a;
+        use = row < n && col <= row;
+      } else {    // L(base + a, r0 + b), i > r
+        if (!UP) { a = e % RT; b = e / RT; } else { b = e % RR; a = e / RR; }
+        row = base + a;
+        col = r0 + b;
+        use = row < n && col < n && row > col;
+      }
+      const double v = use ? (UP ? p.A[col + (int64_t)row * p.lda] : p.A[row + (int64_t)col * p.lda])
+                           : 0.0;
+      av[u] = ABS ? fabs(v) : v;
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int e = threadIdx.x + u * 256;
+      const int a = e % RT, c = e / RT;
+      const int row = base + a;
+      xv[u] = (row < n && c < p.nr) ? p.X[row + (int64_t)c * p.ldx] : 0.0;
+    }
+  };
+  auto stash = [&](int t) {
+    const bool ph1 = t < t1;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int e = threadIdx.x + u * 256;
+      int a, b;
+      if (ph1) {
+        if (!UP) { b = e % RR; a = e / RR; } else { a = e % RT; b = e / RT; }
+      } else {
+        if (!UP) { a = e % RT; b = e / RT; } else { b = e % RR; a = e / RR; }
+      }
+      T[a][b] = av[u];
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int e = threadIdx.x + u * 256;
+      Xs[e % RT][e / RT] = xv[u];
+    }
+  };
+  if (ntile > 0) fetch(0);
+  for (int t = 0; t < ntile; ++t) {
+    __syncthreads();  // the previous tile is no longer read
+    stash(t);
+    __syncthreads();
+    if (t + 1 < ntile) fetch(t + 1);
+#pragma unroll
+    for (int jj = 0; jj < 8; ++jj) {
+      const double a = T[8 * q + jj][r];
+#pragma unroll
+      for (int c = 0; c < RNR; ++c) acc[c] = fma(a, Xs[8 * q + jj][c], acc[c]);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < RNR; ++c) red[q][r][c] = acc[c];
+  __syncthreads();
+  for (int e = threadIdx.x; e < RR * RNR; e += 256) {
+    const int rr = e % RR, c = e / RR;
+    const int row = r0 + rr;
+    if (row < n && c < p.nr) {
+      const double s = ((red[0][rr][c] + red[1][rr][c]) + red[2][rr][c]) + red[3][rr][c];
+      const double b = p.Bv ? p.Bv[row + (int64_t)c * p.ldb] : 0.0;
+      p.Y[row + (int64_t)c * p.ldy] = fma(p.sa, s, b);
+    }
+  }
+}
+
+// out[c] = max_r |V(r, c)| (out zeroed by the caller; non-negative doubles order like
+// their bit patterns, so the maximum is exact and independent of the order)
+__global__ void colmax_kernel(const double *V, int64_t ld, int n, int nr, double *out) {
+  const int c = blockIdx.y;
+  double m = 0.0;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+    m = fmax(m, fabs(V[r + (int64_t)c * ld]));
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m > 0.0)
+    atomicMax(reinterpret_cast<unsigned long long *>(out + c),
+              (unsigned long long)__double_as_longlong(m));
+}
+
+// partial[blk * pstride + i * nr + c] = sum over rows of chunk blk of V_i(r, c) * W(r, c)
+// (V_i = V + i * vstride, all n x nr with leading dimension n)
+__global__ void __launch_bounds__(256) dots_kernel(const double *V, int64_t vstride, int nv,
+                                                   const double *W, int n, int nr,
+                                                   double *partial, int pstride) {
+  __shared__ double s[8][kGmresMax + 2];
+  const int c = blockIdx.y, blk = blockIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double w[4];
+  int rows[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    rows[k] = blk * DOT_ROWS + threadIdx.x + 256 * k;
+    w[k] = rows[k] < n ? W[rows[k] + (int64_t)c * n] : 0.0;
+  }
+  for (int i = 0; i < nv; ++i) {
+    const double *vi = V + i * vstride + (int64_t)c * n;
+    double t = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (rows[k] < n) t = fma(vi[rows[k]], w[k], t);
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0) s[warp][i] = t;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nv; i += 256) {
+    double t = 0.0;
+    for (int w8 = 0; w8 < 8; ++w8) t += s[w8][i];
+    partial[(size_t)blk * pstride + i * nr + c] = t;
+  }
+}
+
+// h[i * nr + c] (+)= sum over chunks (fixed order); with `root`, h = sqrt of the sum
+__global__ void dots_reduce_kernel(const double *partial, int pstride, int nblk, int nv, int nr,
+                                   double *h, bool root) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nv * nr) return;
+  double t = 0.0;
+  for (int b = 0; b < nblk; ++b) t += partial[(size_t)b * pstride + e];
+  h[e] = root ? sqrt(t) : t;
+}
+
+// W(r, c) += sign * sum_{i < nv} V_i(r, c) * h[i * nr + c]
+__global__ void vupdate_kernel(double *W, const double *V, int64_t vstride, int nv,
+                               const double *h, int n, int nr, double sign) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+  if (r >= n) return;
+  double t = 0.0;
+  for (int i = 0; i < nv; ++i) t = fma(V[i * vstride + r + (int64_t)c * n], h[i * nr + c], t);
+  W[r + (int64_t)c * n] = fma(sign, t, W[r + (int64_t)c * n]);
+}
+
+// dst(r, c) = src(r, c) / s[c]  (0 where s[c] == 0)
+__global__ void vscale_kernel(double *dst, const double *src, const double *s, int n, int nr) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+  if (r >= n) return;
+  const double d = s[c];
+  dst[r + (int64_t)c * n] = d > 0.0 ? src[r + (int64_t)c * n] / d : 0.0;
+}
+
+// copy between an n x nr view (ld) and a packed n x nr block (ld n)
+__global__ void vcopy_kernel(double *dst, int64_t ldd, const double *src, int64_t lds, int n,
+                             int nr) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+  if (r < n && c < nr) dst[r + (int64_t)c * ldd] = src[r + (int64_t)c * lds];
+}
+
+__global__ void vfill_kernel(double *dst, double v, int64_t count) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < count) dst[e] = v;
+}
+
+// ---------------------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------------------
+
+struct Solver {
+  mo_ctx *ctx;
+  View A;
+  bool upper;
+  int n, nr;  // nr: right-hand sides (all columns)
+  LpChol f;
+  double *b, *x, *r, *d;  // n x nr packed
+  double *V;              // (kGmresMax + 1) blocks of n x nr
+  double *h, *h2;         // Gram-Schmidt coefficients, (kGmresMax + 1) x nr each
+  double *scal;           // per-column scalars (nr)
+  double *partial;        // dot partial sums
+  double *norms;          // [0, nr): |r|, [nr, 2nr): |x|, [2nr, 3nr): |b|, 3nr: |A|
+  int *flags;             // trsm_few block flags
+  int nblk_dot, pstride;
+};
+
+dim3 vgrid(int n, int nr) { return dim3((n + 255) / 256, nr); }
+
+int sym_apply(Solver &s, const double *X, int64_t ldx, const double *Bv, double *Y, double sa,
+              bool abs_a, int nr) {
+  mo_ctx *ctx = s.ctx;
+  ProfScope ps;
+  prof_begin(ctx, ps, MO_PROF_IR);
+  for (int c0 = 0; c0 < nr; c0 += RNR) {
+    SymArgs p;
+    p.A = s.A.d;
+    p.lda = s.A.ld;
+    p.n = s.n;
+    p.X = X + (int64_t)c0 * ldx;
+    p.ldx = ldx;
+    p.Bv = Bv ? Bv + (int64_t)c0 * s.n : nullptr;
+    p.ldb = s.n;
+    p.Y = Y + (int64_t)c0 * s.n;
+    p.ldy = s.n;
+    p.nr = std::min(RNR, nr - c0);
+    p.sa = sa;
+    const int grid = (s.n + RR - 1) / RR;
+    if (s.upper) {
+      if (abs_a) sym_apply_kernel<true, true><<<grid, 256, 0, ctx->stream>>>(p);
+      else sym_apply_kernel<true, false><<<grid, 256, 0, ctx->stream>>>(p);
+    } else {
+      if (abs_a) sym_apply_kernel<false, true><<<grid, 256, 0, ctx->stream>>>(p);
+      else sym_apply_kernel<false, false><<<grid, 256, 0, ctx->stream>>>(p);
+    }
+  }
+  prof_end(ctx, ps, 2.0 * s.n * (double)s.n * nr,
+           8.0 * s.n * (double)s.n * ((nr + RNR - 1) / RNR) + 24.0 * s.n * nr);
+  MO_CUDA_TRY(cudaGetLastError());
+  return MO_OK;
+}
+
+int colmax(Solver &s, const double *V, int64_t ld, int n, int nr, double *out) {
+  MO_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(double) * nr, s.ctx->stream));
+  colmax_kernel<<<dim3(std::min(64, (n + 255) / 256), nr), 256, 0, s.ctx->stream>>>(V, ld, n,
+                                                                                   nr, out);
+  MO_CUDA_TRY(cudaGetLastError());
+  return MO_OK;
+}
+
+// D = M^-1 D in place (D: packed n x nr); RHS in groups of 64
+int precond(Solver &s, double *D) {
+  for (int c0 = 0; c0 < s.nr; c0 += 64) {
+    const View B{D + (int64_t)c0 * s.n, s.n, std::min(64, s.nr - c0), s.n};
+    int rc = trsm_few_f32(s.ctx, B, s.f.W, s.f.ldw, s.n, false, s.f.inv, s.flags);
+    if (!rc) rc = trsm_few_f32(s.ctx, B, s.f.W, s.f.ldw, s.n, true, s.f.inv, s.flags);
+    if (rc) return rc;
+  }
+  return MO_OK;
+}
+
+// h(0..nv-1, :) = V_0..nv-1^T W per column; root: h = sqrt(W^T W) (nv = 1, V = W)
+int dots(Solver &s, const double *V, int nv, const double *W, double *h, bool root) {
+  cudaStream_t st = s.ctx->stream;
+  ProfScope ps;
+  prof_begin(s.ctx, ps, MO_PROF_IR);
+  dots_kernel<<<dim3(s.nblk_dot, s.nr), 256, 0, st>>>(V, (int64_t)s.n * s.nr, nv, W, s.n, s.nr,
+                                                      s.partial, s.pstride);
+  const int m = nv * s.nr;
+  dots_reduce_kernel<<<(m + 127) / 128, 128, 0, st>>>(s.partial, s.pstride, s.nblk_dot, nv, s.nr,
+                                                      h, root);
+  prof_end(s.ctx, ps, 2.0 * s.n * (double)s.nr * nv, 8.0 * s.n * (double)s.nr * (nv + 1));
+  MO_CUDA_TRY(cudaGetLastError());
+  return MO_OK;
+}
+
+int vupdate(Solver &s, double *W, const double *V, int nv, const double *h, double sign) {
+  ProfScope ps;
+  prof_begin(s.ctx, ps, MO_PROF_IR);
+  vupdate_kernel<<<vgrid(s.n, s.nr), 256, 0, s.ctx->stream>>>(W, V, (int64_t)s.n * s.nr, nv, h,
+                                                              s.n, s.nr, sign);
+  prof_end(s.ctx, ps, 2.0 * s.n * (double)s.nr * nv, 8.0 * s.n * (double)s.nr * (nv + 2));
+  MO_CUDA_TRY(cudaGetLastError());
+  return MO_OK;
+}
+
+// d = GMRES(A, r) preconditioned on the left by M^-1, at most kGmresMax iterations, until
+// every column's preconditioned residual has dropped by tau; *its receives the iterations
+int gmres(Solver &s, double tau, int *its) {
+  const int n = s.n, nr = s.nr;
+  const int64_t vs = (int64_t)n * nr;
+  cudaStream_t st = s.ctx->stream;
+  int rc;
+  MO_CUDA_TRY(cudaMemcpyAsync(s.d, s.r, sizeof(double) * vs, cudaMemcpyDeviceToDevice, st));
+  if ((rc = precond(s, s.d))) return rc;
+  if ((rc = dots(s, s.d, 1, s.d, s.scal, true))) return rc;  // beta = |M^-1 r|_2
+  vscale_kernel<<<vgrid(n, nr), 256, 0, st>>>(s.V, s.d, s.scal, n, nr);
+  std::vector<double> beta(nr);
+  MO_CUDA_TRY(cudaMemcpyAsync(beta.data(), s.scal, sizeof(double) * nr, cudaMemcpyDeviceToHost, st));
+  MO_CUDA_TRY(cudaStreamSynchronize(st));
+  // per column c: R (rotated Hessenberg, column-major (kGmresMax+1) x kGmresMax), the
+  // rotations (cs, sn) and the rotated right-hand side g
+  const int LDR = kGmresMax + 1;
+  std::vector<double> R((size_t)LDR * kGmresMax * nr, 0.0), cs((size_t)kGmresMax * nr, 1.0),
+      sn((size_t)kGmresMax * nr, 0.0), g((size_t)LDR * nr, 0.0);
+  auto Rat = [&](int i, int j, int c) -> double & { return R[((size_t)c * kGmresMax + j) * LDR + i]; };
+  for (int c = 0; c < nr; ++c) g[(size_t)c * LDR] = beta[c];
+  std::vector<double> h1((size_t)(kGmresMax + 1) * nr), h2((size_t)(kGmresMax + 1) * nr), hn(nr);
+  int m = 0;
+  for (int j = 0; j < kGmresMax; ++j) {
+    double *vj = s.V + j * vs, *w = s.V + (j + 1) * vs;
+    if ((rc = sym_apply(s, vj, n, nullptr, w, 1.0, false, nr))) return rc;  // w = A v_j
+    if ((rc = precond(s, w))) return rc;                                     // w = M^-1 w
+    // classical Gram-Schmidt, applied twice (h = h1 + h2)
+    if ((rc = dots(s, s.V, j + 1, w, s.h, false))) return rc;
+    if ((rc = vupdate(s, w, s.V, j + 1, s.h, -1.0))) return rc;
+    if ((rc = dots(s, s.V, j + 1, w, s.h2, false))) return rc;
+    if ((rc = vupdate(s, w, s.V, j + 1, s.h2, -1.0))) return rc;
+    if ((rc = dots(s, w, 1, w, s.scal, true))) return rc;  // |w|_2
+    vscale_kernel<<<vgrid(n, nr), 256, 0, st>>>(w, w, s.scal, n, nr);
+    MO_CUDA_TRY(cudaGetLastError());
+    MO_CUDA_TRY(cudaMemcpyAsync(h1.data(), s.h, sizeof(double) * (j + 1) * nr,
+                                cudaMemcpyDeviceToHost, st));
+    MO_CUDA_TRY(cudaMemcpyAsync(h2.data(), s.h2, sizeof(double) * (j + 1) * nr,
+                                cudaMemcpyDeviceToHost, st));
+    MO_CUDA_TRY(cudaMemcpyAsync(hn.data(), s.scal, sizeof(double) * nr, cudaMemcpyDeviceToHost, st));
+    MO_CUDA_TRY(cudaStreamSynchronize(st));
+    m = j + 1;
+    double worst = 0.0;
+    for (int c = 0; c < nr; ++c) {
+      for (int i = 0; i <= j; ++i) Rat(i, j, c) = h1[(size_t)i * nr + c] + h2[(size_t)i * nr + c];
+      Rat(j + 1, j, c) = hn[c];
+      for (int i = 0; i < j; ++i) {  // earlier rotations
+        const double a = Rat(i, j, c), b = Rat(i + 1, j, c);
+        const double cc = cs[(size_t)c * kGmresMax + i], ss = sn[(size_t)c * kGmresMax + i];
+        Rat(i, j, c) = cc * a + ss * b;
+        Rat(i + 1, j, c) = -ss * a + cc * b;
+      }
+      const double a = Rat(j, j, c), b = Rat(j + 1, j, c);
+      const double rr = std::hypot(a, b);
+      const double cc = rr > 0.0 ? a / rr : 1.0, ss = rr > 0.0 ? b / rr : 0.0;
+      cs[(size_t)c * kGmresMax + j] = cc;
+      sn[(size_t)c * kGmresMax + j] = ss;
+      Rat(j, j, c) = rr;
+      Rat(j + 1, j, c) = 0.0;
+      double &gj = g[(size_t)c * LDR + j];
+      g[(size_t)c * LDR + j + 1] = -ss * gj;
+      gj = cc * gj;
+      if (beta[c] > 0.0) worst = std::max(worst, std::fabs(g[(size_t)c * LDR + j + 1]) / beta[c]);
+    }
+    if (worst <= tau) break;
+  }
+  // y = R^-1 g (m x m upper triangular, per column), d = V y
+  std::vector<double> y((size_t)m * nr, 0.0);
+  for (int c = 0; c < nr; ++c)
+    for (int i = m - 1; i >= 0; --i) {
+      double t = g[(size_t)c * LDR + i];
+      for (int k = i + 1; k < m; ++k) t -= Rat(i, k, c) * y[(size_t)k * nr + c];
+      const double dii = Rat(i, i, c);
+      y[(size_t)i * nr + c] = dii != 0.0 ? t / dii : 0.0;
+    }
+  MO_CUDA_TRY(cudaMemcpyAsync(s.h, y.data(), sizeof(double) * m * nr, cudaMemcpyHostToDevice, st));
+  MO_CUDA_TRY(cudaMemsetAsync(s.d, 0, sizeof(double) * vs, st));
+  if ((rc = vupdate(s, s.d, s.V, m, s.h, 1.0))) return rc;
+  // y lives in host memory only until the copy above has run
+  MO_CUDA_TRY(cudaStreamSynchronize(st));
+  *its = m;
+  return MO_OK;
+}
+
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// workspace bytes for order n, nr right-hand sides
+size_t ir_bytes(int n, int nr, int prec, bool gmres_possible) {
+  const size_t vec = align256((size_t)n * nr * 8);
+  const int nblk_dot = (n + DOT_ROWS - 1) / DOT_ROWS;
+  size_t b = lp_chol_bytes(n, prec) + 4 * vec;
+  if (gmres_possible) b += (kGmresMax + 1) * vec;
+  b += 2 * align256((size_t)(kGmresMax + 1) * nr * 8) + align256((size_t)nr * 8);
+  b += align256((size_t)nblk_dot * (kGmresMax + 2) * nr * 8);
+  b += align256((size_t)(3 * nr + 1) * 8) + align256((size_t)((n + 63) / 64 + 64) * 4) + 4096;
+  return b;
+}
+
+// The FP64 path (potrf + two triangular solves) for a copy of A; returns info like
+// mo_decompose_chol
+int fp64_solve(mo_ctx *ctx, const View &A, bool upper, const View &X, const double *b) {
+  const int n = A.rows;
+  double *tmp = nullptr;
+  MO_CUDA_TRY(cudaMalloc(&tmp, (size_t)n * n * sizeof(double)));
+  int rc = MO_OK;
+  do {
+    if (cudaMemcpy2DAsync(tmp, (size_t)n * 8, A.d, (size_t)A.ld * 8, (size_t)n * 8, n,
+                          cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess) {
+      rc = MO_ECUDA;
+      break;
+    }
+    const View T{tmp, n, n, n};
+    double *inv = nullptr;
+    if ((rc = workspace(ctx, 128 * 128 * sizeof(double), (void **)&inv))) break;
+    Control *cb = control(ctx);
+    if (cudaMemsetAsync(&cb->info, 0, sizeof(Control) - offsetof(Control, info), ctx->stream) !=
+        cudaSuccess) {
+      rc = MO_ECUDA;
+      break;
+    }
+    if ((rc = potrf(ctx, T, upper, &cb->info, &cb->bad, inv))) break;
+    Control h;
+    if (cudaMemcpy(&h, cb, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) {
+      rc = MO_ECUDA;
+      break;
+    }
+    if (h.info > 0) {
+      rc = h.info;
+      break;
+    }
+    vcopy_kernel<<<vgrid(n, X.cols), 256, 0, ctx->stream>>>(X.d, X.ld, b, n, n, X.cols);
+    if (upper) {
+      rc = trsm(ctx, X, T, MO_UPPER | MO_TRANSA, 1.0);
+      if (!rc) rc = trsm(ctx, X, T, MO_UPPER, 1.0);
+    } else {
+      rc = trsm(ctx, X, T, MO_LOWER, 1.0);
+      if (!rc) rc = trsm(ctx, X, T, MO_LOWER | MO_TRANSA, 1.0);
+    }
+    if (!rc && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = MO_ECUDA;
+  } while (false);
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(tmp);
+  return rc;
+}
+
+// berr per column from the device norms; returns the max (0 for all-zero columns)
+double backward_error(Solver &s, std::vector<double> &nh) {
+  double worst = 0.0;
+  const double an = nh[3 * s.nr];
+  for (int c = 0; c < s.nr; ++c) {
+    const double den = an * nh[s.nr + c] + nh[2 * s.nr + c];
+    const double e = den > 0.0 ? nh[c] / den : (nh[c] > 0.0 ? INFINITY : 0.0);
+    worst = std::max(worst, e);
+  }
+  return worst;
+}
+
+int dsposv(mo_ctx *ctx, const View &X, const View &A, const View &B, bool upper, int prec,
+           int method_flags, double tol, int maxit, mo_ir_info &info) {
+  const int n = A.rows, nr = B.cols;
+  const int method = method_flags & 0xff;
+  const bool fallback_ok = (method_flags & MO_IR_NO_FALLBACK) == 0;
+  cudaStream_t st = ctx->stream;
+  Solver s;
+  s.ctx = ctx;
+  s.A = A;
+  s.upper = upper;
+  s.n = n;
+  s.nr = nr;
+  const bool gm = method != MO_IR_CLASSIC;
+  const size_t need = ir_bytes(n, nr, prec, gm);
+  if (need > ctx->ws_ir_bytes) {
+    MO_CUDA_TRY(cudaStreamSynchronize(st));
+    if (ctx->ws_ir) cudaFree(ctx->ws_ir);
+    ctx->ws_ir = nullptr;
+    ctx->ws_ir_bytes = 0;
+    MO_CUDA_TRY(cudaMalloc(&ctx->ws_ir, need));
+    ctx->ws_ir_bytes = need;
+  }
+  char *p = (char *)ctx->ws_ir;
+  auto take = [&](size_t bytes) {
+    char *r = p;
+    p += align256(bytes);
+    return r;
+  };
+  lp_chol_setup(n, prec, take(lp_chol_bytes(n, prec)), s.f);
+  const size_t vec = (size_t)n * nr * 8;
+  s.b = (double *)take(vec);
+  s.x = (double *)take(vec);
+  s.r = (double *)take(vec);
+  s.d = (double *)take(vec);
+  // GMRES basis: kGmresMax + 1 blocks of n x nr, packed with stride n * nr
+  s.V = gm ? (double *)take((kGmresMax + 1) * align256(vec)) : nullptr;
+  s.h = (double *)take((size_t)(kGmresMax + 1) * nr * 8);
+  s.h2 = (double *)take((size_t)(kGmresMax + 1) * nr * 8);
+  s.scal = (double *)take((size_t)nr * 8);
+  s.nblk_dot = (n + DOT_ROWS - 1) / DOT_ROWS;
+  s.pstride = (kGmresMax + 2) * nr;
+  s.partial = (double *)take((size_t)s.nblk_dot * s.pstride * 8);
+  s.norms = (double *)take((size_t)(3 * nr + 1) * 8);
+  s.flags = (int *)take((size_t)((n + 63) / 64 + 64) * 4);
+  int rc;
+  // b, |b|, |A|_inf (row sums of |A| through the same symmetric kernel, with x = 1)
+  vcopy_kernel<<<vgrid(n, nr), 256, 0, st>>>(s.b, n, B.d, B.ld, n, nr);
+  vfill_kernel<<<(n + 255) / 256, 256, 0, st>>>(s.d, 1.0, n);
+  if ((rc = sym_apply(s, s.d, n, nullptr, s.r, 1.0, true, 1))) return rc;
+  if ((rc = colmax(s, s.r, n, n, 1, s.norms + 3 * nr))) return rc;
+  if ((rc = colmax(s, s.b, n, n, nr, s.norms + 2 * nr))) return rc;
+  // low-precision factorization, shifted on breakdown
+  Control *cb = control(ctx);
+  const double s0 = prec == kLpBf16x3 ? 0x1p-15 : 0x1p-22;
+  double shift = 0.0;
+  bool factored = false;
+  for (int attempt = 0; attempt < 5; ++attempt) {
+    MO_CUDA_TRY(cudaMemsetAsync(&cb->info, 0, sizeof(Control) - offsetof(Control, info), st));
+    if ((rc = lp_chol_convert(ctx, s.f, A, upper, shift))) return rc;
+    if ((rc = lp_chol_factor(ctx, s.f, &cb->info, &cb->bad))) return rc;
+    Control h;
+    MO_CUDA_TRY(cudaStreamSynchronize(st));
+    MO_CUDA_TRY(cudaMemcpy(&h, cb, sizeof(h), cudaMemcpyDeviceToHost));
+    if (h.status) {
+      cudaMemset(&cb->status, 0, sizeof(int));
+      return h.status;
+    }
+    if (h.info == 0) {
+      factored = true;
+      break;
+    }
+    shift = shift == 0.0 ? s0 : shift * 8.0;
+    info.shifts += 1;
+  }
+  info.shift = factored ? shift : 0.0;
+  std::vector<double> nh(3 * nr + 1);
+  double prev = INFINITY;
+  bool use_gmres = method == MO_IR_GMRES;
+  int stall = 0;
+  if (factored) {
+    MO_CUDA_TRY(cudaMemsetAsync(s.x, 0, vec, st));
+    for (int it = 0;; ++it) {
+      if (it == 0) MO_CUDA_TRY(cudaMemcpyAsync(s.r, s.b, vec, cudaMemcpyDeviceToDevice, st));
+      else if ((rc = sym_apply(s, s.x, n, s.b, s.r, -1.0, false, nr))) return rc;
+      if ((rc = colmax(s, s.r, n, n, nr, s.norms))) return rc;
+      if ((rc = colmax(s, s.x, n, n, nr, s.norms + nr))) return rc;
+      MO_CUDA_TRY(cudaMemcpyAsync(nh.data(), s.norms, nh.size() * 8, cudaMemcpyDeviceToHost, st));
+      MO_CUDA_TRY(cudaStreamSynchronize(st));
+      const double berr = backward_error(s, nh);
+      if (it < MO_IR_HISTORY) info.history[it] = berr;
+      info.berr = berr;
+      if (berr <= tol) {
+        info.converged = 1;
+        break;
+      }
+      if (it >= maxit || !std::isfinite(berr)) break;
+      // a step that did not reduce berr 20x: switch to GMRES-IR (auto), else count stalls
+      if (it > 0 && berr > 0.05 * prev) {
+        if (method == MO_IR_AUTO && !use_gmres) use_gmres = true;
+        else if (berr > 0.5 * prev && ++stall >= 2) break;
+      }
+      prev = berr;
+      if (use_gmres) {
+        int its = 0;
+        if ((rc = gmres(s, 1e-10, &its))) return rc;
+        info.gmres_iters += its;
+        info.method = MO_IR_GMRES;
+      } else {
+        MO_CUDA_TRY(cudaMemcpyAsync(s.d, s.r, vec, cudaMemcpyDeviceToDevice, st));
+        if ((rc = precond(s, s.d))) return rc;
+        info.method = MO_IR_CLASSIC;
+      }
+      vfill_kernel<<<(nr + 255) / 256, 256, 0, st>>>(s.scal, 1.0, nr);
+      // x += d  (as x += V_0 h with V_0 = d, h = 1 per column)
+      if ((rc = vupdate(s, s.x, s.d, 1, s.scal, 1.0))) return rc;
+      info.iters += 1;
+    }
+    MO_CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  if (info.converged || (!fallback_ok && factored)) {
+    vcopy_kernel<<<vgrid(n, nr), 256, 0, st>>>(X.d, X.ld, s.x, n, n, nr);
+    MO_CUDA_TRY(cudaGetLastError());
+    MO_CUDA_TRY(cudaStreamSynchronize(st));
+    return MO_OK;
+  }
+  if (!fallback_ok) return MO_EINVAL;
+  // FP64 factorization and solve
+  info.fallback = 1;
+  if ((rc = fp64_solve(ctx, A, upper, X, s.b)) != MO_OK) return rc;
+  // report the backward error of the FP64 solution
+  vcopy_kernel<<<vgrid(n, nr), 256, 0, st>>>(s.x, n, X.d, X.ld, n, nr);
+  if ((rc = sym_apply(s, s.x, n, s.b, s.r, -1.0, false, nr))) return rc;
+  if ((rc = colmax(s, s.r, n, n, nr, s.norms))) return rc;
+  if ((rc = colmax(s, s.x, n, n, nr, s.norms + nr))) return rc;
+  MO_CUDA_TRY(cudaMemcpyAsync(nh.data(), s.norms, nh.size() * 8, cudaMemcpyDeviceToHost, st));
+  MO_CUDA_TRY(cudaStreamSynchronize(st));
+  info.berr = backward_error(s, nh);
+  info.converged = info.berr <= tol;
+  return MO_OK;
+}
+
+}  // namespace
+}  // namespace mo
+
+extern "C" int mo_dsposv_ir(mo_ctx *ctx, mo_matrix Xm, mo_matrix Am, mo_matrix Bm, int flags,
+                            int prec, int method, double tol, int maxit, mo_ir_info *info) {
+  using namespace mo;
+  int rc = enter(ctx);
+  if (rc) return rc;
+  View X, A, B;
+  if ((rc = to_view(Xm, X)) || (rc = to_view(Am, A)) || (rc = to_view(Bm, B))) return rc;
+  if (A.rows != A.cols) return MO_ENOTSQUARE;
+  if (B.rows != A.rows || X.rows != B.rows || X.cols != B.cols) return MO_ESIZE;
+  if (prec != MO_PREC_BF16X3 && prec != MO_PREC_TF32X3) return MO_EINVAL;
+  const int m = method & 0xff;
+  if (m != MO_IR_AUTO && m != MO_IR_CLASSIC && m != MO_IR_GMRES) return MO_EINVAL;
+  if (maxit < 0 || !(tol >= 0.0)) return MO_EINVAL;
+  mo_ir_info local;
+  mo_ir_info &inf = info ? *info : local;
+  std::memset(&inf, 0, sizeof(inf));
+  if (A.rows == 0 || B.cols == 0) {
+    inf.converged = 1;
+    return MO_OK;
+  }
+  const int lp = prec == MO_PREC_BF16X3 ? kLpBf16x3 : kLpTf32x3;
+  return dsposv(ctx, X, A, B, (flags & MO_UPPER) != 0, lp, method, tol, maxit, inf);
+}

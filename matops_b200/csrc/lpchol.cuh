@@ -1,0 +1,27 @@
+// Mixed-precision Cholesky factor (lpchol.cu): workspace layout and entry points.
+#pragma once
+#include "lp.cuh"
+
+namespace mo {
+
+struct LpChol {
+  int n = 0, NP = 0, prec = 0;
+  float *W = nullptr;  // NP x NP FP32 working matrix; its lower triangle becomes L
+  int64_t ldw = 0;
+  double *inv = nullptr;  // NP/128 FP64 inverses of L's 128 x 128 diagonal blocks
+  LpSplit Linv{};         // split inverse of the current diagonal block
+  LpSplit PA{};           // split A21 of the current panel
+  LpSplit P[2]{};         // split L21 panels, by step parity
+};
+
+// device bytes for the workspace of an order-n factorization
+size_t lp_chol_bytes(int n, int prec);
+// carve the workspace out of `mem` (lp_chol_bytes(n, prec) bytes)
+int lp_chol_setup(int n, int prec, void *mem, LpChol &f);
+// W = FP32(lower triangle of A) (upper: transpose of its upper triangle), diagonal scaled
+// by (1 + shift), identity padding
+int lp_chol_convert(mo_ctx *ctx, const LpChol &f, View A, bool upper, double shift);
+// factor W in place; a failing pivot sets *d_info = column + 1 (device word)
+int lp_chol_factor(mo_ctx *ctx, LpChol &f, int *d_info, double *d_bad);
+
+}  // namespace mo

@@ -30,7 +30,7 @@ constexpr int LDX = MAX_RHS + 4;
 constexpr int FEW_SMEM = (3 * TB * LDL + TB * LDX) * 8;  // inverse, 2 x op(A) block, X
 
 struct FewArgs {
-  const double *A;
+  const void *A;  // double, or float for the mixed-precision factor (FP64 arithmetic)
   int64_t lda;
   bool trans;      // op(A) = A^T
   bool lower_eff;  // op(A) lower -> steps top-down
@@ -40,6 +40,7 @@ struct FewArgs {
   int nrhs;
   double alpha;
   const double *inv;  // 128 x 128 inverses of op(A)'s diagonal blocks (ld 128)
+  bool inv_t;         // inv holds the inverses of A's blocks: read them transposed
   int *flags;         // [nblk]
   int epoch;
   int *status;
@@ -53,19 +54,28 @@ __device__ __forceinline__ void cp_async_join() {
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
+__device__ __forceinline__ void cp_async_el(double *dst, const double *src, uint32_t n) {
+  cp_async_8(dst, src, n ? 8u : 0u);
+}
+__device__ __forceinline__ void cp_async_el(float *dst, const float *src, uint32_t n) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(smem_u32(dst)), "l"(src),
+               "r"(n ? 4u : 0u)
+               : "memory");
+}
+
 // issue cp.async copies of op(A)[rb*64 .., cb*64 ..] into L (row-major, ld LDL); zero past N
-__device__ __forceinline__ void stage_block(const FewArgs &p, double *L, int rb, int cb) {
+template <typename TA>
+__device__ __forceinline__ void stage_block(const FewArgs &p, TA *L, int rb, int cb) {
   const int r0 = rb * TB, c0 = cb * TB;
+  const TA *A = static_cast<const TA *>(p.A);
   for (int e = threadIdx.x; e < TB * TB; e += blockDim.x) {
     const int i = e % TB, j = e / TB;  // consecutive threads -> consecutive A addresses
     if (!p.trans) {
       const bool ok = r0 + i < p.N && c0 + j < p.N;
-      cp_async_8(L + i * LDL + j, ok ? p.A + (r0 + i) + (int64_t)(c0 + j) * p.lda : p.A,
-                 ok ? 8u : 0u);
+      cp_async_el(L + i * LDL + j, ok ? A + (r0 + i) + (int64_t)(c0 + j) * p.lda : A, ok);
     } else {
       const bool ok = c0 + i < p.N && r0 + j < p.N;
-      cp_async_8(L + j * LDL + i, ok ? p.A + (c0 + i) + (int64_t)(r0 + j) * p.lda : p.A,
-                 ok ? 8u : 0u);
+      cp_async_el(L + j * LDL + i, ok ? A + (c0 + i) + (int64_t)(r0 + j) * p.lda : A, ok);
     }
   }
 }
@@ -78,33 +88,34 @@ __device__ __forceinline__ void stage_inverse(const FewArgs &p, double *I, int r
   for (int e = threadIdx.x; e < TB * TB; e += blockDim.x) {
     const int i = e % TB, j = e / TB;  // column-major source, ld 128
     const bool ok = i < nbh && j < nbh;
-    cp_async_8(I + i * LDL + j, ok ? iv + i + j * IB : iv, ok ? 8u : 0u);
+    const double *src = p.inv_t ? iv + j + i * IB : iv + i + j * IB;
+    cp_async_8(I + i * LDL + j, ok ? src : iv, ok ? 8u : 0u);
   }
 }
 
 // acc[nt] (+)= sign * M(16 rows of this warp, 64) * X(64, 8 nt ..)
-template <int NT>
-__device__ __forceinline__ void block_mma(double (&acc)[NT][4], const double *M, const double *X,
+template <int NT, typename TM>
+__device__ __forceinline__ void block_mma(double (&acc)[NT][4], const TM *M, const double *X,
                                           double sign) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
-  const double *m0 = M + (16 * warp + g) * LDL + t;
-  const double *m1 = m0 + 8 * LDL;
+  const TM *m0 = M + (16 * warp + g) * LDL + t;
+  const TM *m1 = m0 + 8 * LDL;
   const double *xb = X + t * LDX + g;
 #pragma unroll 4
   for (int k = 0; k < TB; k += 4) {
-    const double a0 = sign * m0[k], a1 = sign * m1[k];
+    const double a0 = sign * (double)m0[k], a1 = sign * (double)m1[k];
 #pragma unroll
     for (int nt = 0; nt < NT; ++nt) dmma_16x8x4(acc[nt], a0, a1, xb[k * LDX + 8 * nt]);
   }
 }
 
-template <int NT>
+template <typename TA, int NT>
 __global__ void __launch_bounds__(FEW_THREADS, 1) trsm_few_kernel(FewArgs p) {
   extern __shared__ double sm[];
-  double *I = sm;                    // inverse of the owned diagonal block
-  double *Lb0 = sm + TB * LDL;       // op(A) blocks, double-buffered
-  double *Lb1 = sm + 2 * TB * LDL;
+  double *I = sm;                                       // inverse of the owned diagonal block
+  TA *Lb0 = reinterpret_cast<TA *>(sm + TB * LDL);      // op(A) blocks, double-buffered
+  TA *Lb1 = reinterpret_cast<TA *>(sm + 2 * TB * LDL);
   double *Xs = sm + 3 * TB * LDL;    // X of a step (row-major, ld LDX)
   __shared__ int s_abort;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -195,12 +206,12 @@ __global__ void __launch_bounds__(FEW_THREADS, 1) trsm_few_kernel(FewArgs p) {
   }
 }
 
-template <int NT>
+template <typename TA, int NT>
 int launch_few(mo_ctx *ctx, FewArgs &p) {
   static int attr_mask = 0;
   int dev = 0;
   cudaGetDevice(&dev);
-  const void *kern = (const void *)trsm_few_kernel<NT>;
+  const void *kern = (const void *)trsm_few_kernel<TA, NT>;
   if (!(attr_mask & (1 << (dev & 31)))) {
     MO_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, FEW_SMEM));
     attr_mask |= 1 << (dev & 31);
@@ -217,15 +228,15 @@ int launch_few(mo_ctx *ctx, FewArgs &p) {
 
 }  // namespace
 
-// Left solve (right solves via the transposed view of B) with nrhs <= 64.  `inv` receives
-// the 128 x 128 diagonal-block inverses; `flag_buf` holds one int per 64-row block.
-int trsm_few(mo_ctx *ctx, View B, View A, int flags, double alpha, double *inv, int *flag_buf) {
+namespace {
+
+// flags -> (B strides, effective transposition and sweep direction) and the launch
+int few_run(mo_ctx *ctx, View B, const void *A, bool a32, int64_t lda, int N, int flags,
+            double alpha, const double *inv, bool inv_t, int *flag_buf) {
   const bool right = (flags & MO_RIGHT) != 0;
   const bool upper = (flags & MO_UPPER) != 0;
   bool tr = (flags & MO_TRANSA) != 0;
-  const bool unit = (flags & MO_UNIT) != 0;
   bool lower_eff = upper ? tr : !tr;
-  const int N = A.cols;
   const int nrhs = right ? B.rows : B.cols;
   if (nrhs > MAX_RHS || N <= 0 || nrhs <= 0) return MO_EINVAL;
   FewArgs p;
@@ -239,10 +250,8 @@ int trsm_few(mo_ctx *ctx, View B, View A, int flags, double alpha, double *inv, 
     tr = !tr;
     lower_eff = !lower_eff;
   }
-  int rc = trtri_blocks(ctx, A, N, tr, lower_eff, unit, inv);
-  if (rc) return rc;
-  p.A = A.d;
-  p.lda = A.ld;
+  p.A = A;
+  p.lda = lda;
   p.trans = tr;
   p.lower_eff = lower_eff;
   p.N = N;
@@ -251,18 +260,58 @@ int trsm_few(mo_ctx *ctx, View B, View A, int flags, double alpha, double *inv, 
   p.nrhs = nrhs;
   p.alpha = alpha;
   p.inv = inv;
+  p.inv_t = inv_t;
   p.flags = flag_buf;
   p.epoch = ++ctx->sk_epoch;
   p.status = reinterpret_cast<int *>(ctx->d_status);
   MO_CUDA_TRY(cudaMemsetAsync(flag_buf, 0, sizeof(int) * p.nblk, ctx->stream));
   ProfScope ps;
-  prof_begin(ctx, ps, MO_PROF_GEMM);
+  prof_begin(ctx, ps, a32 ? MO_PROF_IR : MO_PROF_GEMM);
   const int nt = (nrhs + 7) / 8;
-  if (nt <= 2) rc = launch_few<2>(ctx, p);
-  else if (nt <= 4) rc = launch_few<4>(ctx, p);
-  else rc = launch_few<8>(ctx, p);
-  prof_end(ctx, ps, (double)N * N * nrhs, 8.0 * ((double)N * N / 2 + 2.0 * N * nrhs));
+  int rc;
+  if (a32) {
+    if (nt <= 2) rc = launch_few<float, 2>(ctx, p);
+    else if (nt <= 4) rc = launch_few<float, 4>(ctx, p);
+    else rc = launch_few<float, 8>(ctx, p);
+  } else {
+    if (nt <= 2) rc = launch_few<double, 2>(ctx, p);
+    else if (nt <= 4) rc = launch_few<double, 4>(ctx, p);
+    else rc = launch_few<double, 8>(ctx, p);
+  }
+  prof_end(ctx, ps, (double)N * N * nrhs,
+           (a32 ? 4.0 : 8.0) * (double)N * N / 2 + 8.0 * 2.0 * N * nrhs);
   return rc;
+}
+
+}  // namespace
+
+// Left solve (right solves via the transposed view of B) with nrhs <= 64.  `inv` receives
+// the 128 x 128 diagonal-block inverses; `flag_buf` holds one int per 64-row block.
+int trsm_few(mo_ctx *ctx, View B, View A, int flags, double alpha, double *inv, int *flag_buf) {
+  const bool right = (flags & MO_RIGHT) != 0;
+  const bool upper = (flags & MO_UPPER) != 0;
+  bool tr = (flags & MO_TRANSA) != 0;
+  const bool unit = (flags & MO_UNIT) != 0;
+  bool lower_eff = upper ? tr : !tr;
+  if (right) {
+    tr = !tr;
+    lower_eff = !lower_eff;
+  }
+  const int N = A.cols;
+  const int nrhs = right ? B.rows : B.cols;
+  if (nrhs > MAX_RHS || N <= 0 || nrhs <= 0) return MO_EINVAL;
+  int rc = trtri_blocks(ctx, A, N, tr, lower_eff, unit, inv);
+  if (rc) return rc;
+  return few_run(ctx, B, A.d, false, A.ld, N, flags, alpha, inv, false, flag_buf);
+}
+
+// Left solve with an FP32 lower-triangular L (order N, ld) in FP64 arithmetic, using the
+// FP64 inverses of L's 128 x 128 diagonal blocks (ld 128): op(L) X = B in place, op = L
+// (trans == false) or L^T.
+int trsm_few_f32(mo_ctx *ctx, View B, const float *L, int64_t ldl, int N, bool trans,
+                 const double *inv_L, int *flag_buf) {
+  const int flags = MO_LOWER | (trans ? MO_TRANSA : 0);
+  return few_run(ctx, B, L, true, ldl, N, flags, 1.0, inv_L, trans, flag_buf);
 }
 
 }  // namespace mo
