@@ -92,6 +92,13 @@ def run_case(args):
             B.copy_(B0)
             mo.SolveCHOL(B, A, LOWER)
         flops = 2.0 * 2.0 * n * n * nrhs
+    elif kind == "dsposv":
+        # dsposv:N:NRHS:KAPPA_EXP -- mixed vs FP64 Cholesky solve, both precisions
+        n, nrhs, kexp = dims
+        res = mixed_leg(mo, n, nrhs, [10.0 ** kexp], [mo.PREC_TF32X3, mo.PREC_BF16X3],
+                        torch.device("cuda", torch.cuda.current_device()), reps=max(1, args.steps))
+        print(json.dumps({"case": args.case, **res}), flush=True)
+        return 0
     elif kind in ("dpotrf", "dgetrf"):
         n = dims[0]
         A0 = mo.matrix(n, n)
@@ -125,6 +132,90 @@ def run_case(args):
     ms = a.elapsed_time(b) / args.steps
     print(json.dumps({"case": args.case, "ms": ms, "tflops": flops / (ms * 1e-3) / 1e12}), flush=True)
     return 0
+
+
+def kappa_spd(mo, n, kappa, seed, dev):
+    """A = Q diag(s) Q^T, Q from the Householder QR of an iid N(0,1) matrix (seed), s
+    log-spaced from 1 to kappa; built on the device in FP64 (torch QR is harness only)."""
+    import torch
+    g = torch.Generator(device=dev).manual_seed(seed)
+    M = torch.randn(n, n, dtype=torch.float64, device=dev, generator=g)
+    Q, R = torch.linalg.qr(M)
+    del M
+    Q *= torch.sign(torch.diagonal(R)).unsqueeze(0)
+    del R
+    s = torch.logspace(0, float(torch.log10(torch.tensor(kappa))), n, dtype=torch.float64,
+                       device=dev)
+    Qc = mo.matrix(n, n)
+    Qc.copy_(Q)
+    del Q
+    QS = mo.matrix(n, n)
+    QS.copy_(Qc * s.unsqueeze(0))
+    A = mo.matrix(n, n)
+    assert mo.Mult(A, QS, Qc, 1.0, 0.0, mo.TRANSB) is None
+    del QS, Qc
+    A.copy_((A + A.t()) * 0.5)
+    return A
+
+
+def mixed_leg(mo, n, nrhs, kappas, precs, dev, reps=2):
+    """Mixed-precision + FP64-refined Cholesky solve against the FP64 path on the same
+    A = Q diag(s) Q^T (seed 6) and B ~ N(0,1) (seed 7): time, iterations, backward and
+    forward error per (kappa, prec)."""
+    import torch
+    B = mo.matrix(n, nrhs)
+    B.normal_(generator=torch.Generator(device=dev).manual_seed(7))
+    out = {}
+    for kappa in kappas:
+        A = kappa_spd(mo, n, kappa, 6, dev)
+        Af = mo.matrix(n, n)
+        Xf = mo.matrix(n, nrhs)
+        tf = []
+        for _ in range(reps):
+            Af.copy_(A)
+            Xf.copy_(B)
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            _, err = mo.DecomposeCHOL(Af, LOWER, 64)
+            assert err is None
+            mo.SolveCHOL(Xf, Af, LOWER)
+            b.record()
+            torch.cuda.synchronize()
+            tf.append(a.elapsed_time(b))
+        del Af
+        an = float(A.abs().sum(1).max())
+
+        def berr(X):
+            R = B.clone()
+            mo.Mult(R, A, X, -1.0, 1.0, 0)
+            return max(float(R[:, c].abs().max() / (an * X[:, c].abs().max() + B[:, c].abs().max()))
+                       for c in range(nrhs))
+        row = {"fp64_ms": min(tf), "fp64_berr": berr(Xf)}
+        for prec in precs:
+            X = mo.matrix(n, nrhs)
+            tm, info = [], None
+            for _ in range(reps):
+                torch.cuda.synchronize()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record()
+                info, err = mo.SolveCHOLMixed(X, A, B, LOWER, prec, mo.IR_AUTO, 1e-14, 40)
+                b.record()
+                torch.cuda.synchronize()
+                assert err is None, err
+                tm.append(a.elapsed_time(b))
+            name = "tf32x3" if prec == mo.PREC_TF32X3 else "bf16x3"
+            row[name] = {"ms": min(tm), "speedup_vs_fp64": min(tf) / min(tm),
+                         "iters": info.iters, "gmres_iters": info.gmres_iters,
+                         "method": "gmres" if info.method == mo.IR_GMRES else "classic",
+                         "fallback": info.fallback, "converged": info.converged,
+                         "shift": info.shift, "berr": info.berr, "berr_check": berr(X),
+                         "ferr_vs_fp64": float((X - Xf).norm() / Xf.norm())}
+            del X
+        out[f"kappa={kappa:.0e}"] = row
+        del A, Xf
+        torch.cuda.empty_cache()
+    return out
 
 
 def workload(n, nrhs):
@@ -463,6 +554,9 @@ def main():
         extras["lu_16384"] = {"s": lms * 1e-3, "factor_tflops": 2 * n ** 3 / 3 / (lms * 1e-3) / 1e12,
                               "berr": lberr}
         del L0, Lb0, LA, LB, R
+        torch.cuda.empty_cache()
+        extras["mixed_ir"] = mixed_leg(mo, n, 16, [1e2, 1e6, 1e10],
+                                       [mo.PREC_TF32X3, mo.PREC_BF16X3], dev)
 
     # ---- CPU baseline (rank 0, one GPU only) ----
     cpu = None
