@@ -99,6 +99,16 @@ def run_case(args):
                         torch.device("cuda", torch.cuda.current_device()), reps=max(1, args.steps))
         print(json.dumps({"case": args.case, **res}), flush=True)
         return 0
+    elif kind == "batched":
+        # batched:KIND:COUNT[:TUNE] -- config 4 (KIND 1 = Cholesky, 2 = LU; TUNE 0 skips
+        # the autotuner)
+        bk, cnt = dims[0], dims[1]
+        tune = dims[2] != 0 if len(dims) > 2 else True
+        res, _ = batched_leg(mo, bk, cnt, 8 if bk == 1 else 9,
+                             torch.device("cuda", torch.cuda.current_device()),
+                             reps=max(1, args.steps), tune=tune)
+        print(json.dumps({"case": args.case, **res}), flush=True)
+        return 0
     elif kind in ("dpotrf", "dgetrf"):
         n = dims[0]
         A0 = mo.matrix(n, n)
@@ -216,6 +226,71 @@ def mixed_leg(mo, n, nrhs, kappas, precs, dev, reps=2):
         del A, Xf
         torch.cuda.empty_cache()
     return out
+
+
+def batched_leg(mo, kind, count, seed, dev, reps=5, tune=True):
+    """Config 4: `count` systems with n_i ~ U{16..512} (seed), 1 RHS each; SPD
+    A_i = G_i G_i^T / n_i + I for Cholesky, iid N(0,1) for LU.  All matrices live in one
+    flat device buffer; each timed run factors and solves a fresh copy (one D2D copy
+    outside the timed region)."""
+    import numpy as np
+    import torch
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(16, 513, count).astype(np.int32)
+    offs = np.concatenate([[0], np.cumsum(sizes.astype(np.int64) ** 2)])
+    g = torch.Generator(device=dev).manual_seed(seed)
+    flat0 = torch.empty(int(offs[-1]), dtype=torch.float64, device=dev)
+    rhs0 = torch.empty(int(sizes.sum()), dtype=torch.float64, device=dev)
+    roffs = np.concatenate([[0], np.cumsum(sizes.astype(np.int64))])
+
+    def mats(flat):
+        return [flat[offs[i]:offs[i + 1]].view(int(n), int(n)).t() for i, n in enumerate(sizes)]
+
+    def vecs(flat):
+        return [flat[roffs[i]:roffs[i + 1]].view(1, int(n)).t() for i, n in enumerate(sizes)]
+    for a, n in zip(mats(flat0), sizes):
+        G = torch.randn(int(n), int(n), dtype=torch.float64, device=dev, generator=g)
+        if kind == mo.BATCH_CHOL:
+            a.copy_(G @ G.t() / float(n))
+            a.diagonal().add_(1.0)
+        else:
+            a.copy_(G)
+    rhs0.normal_(generator=g)
+    flat, rhs = flat0.clone(), rhs0.clone()
+    As, Bs = mats(flat), vecs(rhs)
+    pivs = [torch.zeros(int(n), dtype=torch.int64, device=dev) for n in sizes] \
+        if kind == mo.BATCH_LU else None
+    plan = mo.BatchPlan(kind, sizes, 1)
+    tune_ms = plan.tune(2) if tune else None
+    ts = []
+    for r in range(reps + 1):
+        flat.copy_(flat0)
+        rhs.copy_(rhs0)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        info = plan.run(As, Bs, pivs)
+        b.record()
+        torch.cuda.synchronize()
+        if r > 0:
+            ts.append(a.elapsed_time(b))
+    ok = int((info != 0).sum())
+    # backward error of every 64th system against the untouched copy
+    worst = 0.0
+    A0s, B0s = mats(flat0), vecs(rhs0)
+    for i in range(0, count, 64):
+        r_ = B0s[i] - A0s[i] @ Bs[i]
+        worst = max(worst, float(r_.norm() / (A0s[i].norm() * Bs[i].norm() + B0s[i].norm())))
+    ms = min(ts)
+    flops = float(np.sum(sizes.astype(np.float64) ** 3)) * (1 if kind == mo.BATCH_CHOL else 2) / 3 \
+        + float(np.sum(2.0 * sizes.astype(np.float64) ** 2))
+    byts = float(np.sum(16.0 * sizes.astype(np.float64) ** 2 + 16.0 * sizes))
+    out = {"ms": ms, "gflops": flops / (ms * 1e-3) / 1e9, "tflops": flops / (ms * 1e-3) / 1e12,
+           "gbs": byts / (ms * 1e-3) / 1e9, "failed": ok, "berr_sample_max": worst,
+           "schedule": plan.schedule(), "tune_ms": tune_ms, "count": count,
+           "sizes": "n_i ~ U{16..512}", "flops": flops, "bytes": byts}
+    plan.close()
+    return out, (sizes, mats(flat0), vecs(rhs0))
 
 
 def workload(n, nrhs):

@@ -56,6 +56,7 @@ extern "C" {
 #define MO_ENOMEM (-22)      /* device allocation failed                              */
 #define MO_ENOKERNEL (-23)   /* no sm_100a kernel image for this device               */
 #define MO_ESTATICLIMIT (-11) /* larger than the fixed scratch of mo_solve_trm_static   */
+#define MO_EBATCHN (-12)     /* a batched matrix order outside 1..MO_BATCH_MAX_N      */
 
 typedef struct mo_ctx mo_ctx;
 
@@ -96,7 +97,8 @@ MO_API int mo_set_syrk_blas_beta(mo_ctx *ctx, int on);
 #define MO_PROF_OTHER 5
 #define MO_PROF_LPGEMM 6   /* split-product (BF16x3 / TF32x3) GEMMs and operand splits  */
 #define MO_PROF_IR 7       /* refinement: FP64 residuals, norms, GMRES vector kernels   */
-#define MO_PROF_CLASSES 8
+#define MO_PROF_BATCH 8    /* batched factor + solve launches (whole graph)              */
+#define MO_PROF_CLASSES 9
 typedef struct mo_profile {
   int64_t launches[MO_PROF_CLASSES]; /* kernel launches since the last reset            */
   double ms[MO_PROF_CLASSES];        /* summed device time (only while enabled)         */
@@ -215,6 +217,42 @@ MO_API int mo_dsposv_ir(mo_ctx *ctx, mo_matrix X, mo_matrix A, mo_matrix B, int 
 MO_API int mo_lp_gemm(mo_ctx *ctx, int prec, int64_t M, int64_t N, int64_t K, float alpha,
                       const float *A, int64_t lda, const float *B, int64_t ldb, float beta,
                       float *C, int64_t ldc, int flags);
+
+/* ---- batched factor + solve of many small systems (no counterpart in the reference,
+ * which factors one matrix per call: DecomposeCHOL chol.go:116 / SolveCHOL chol.go:147,
+ * DecomposeLU lu.go:420 / SolveLU lu.go:483; each matrix gets the same results those
+ * calls give, to rounding, and the same pivots) ---- */
+#define MO_BATCH_CHOL 1     /* A_i = L_i L_i^T (lower; the strict upper part is not read) */
+#define MO_BATCH_LU 2       /* P_i A_i = L_i U_i with partial pivoting                    */
+#define MO_BATCH_MAX_N 512  /* largest order in a batch                                   */
+#define MO_BATCH_BUCKETS 4  /* schedule buckets: n <= 64, <= 128, <= 256, <= 512         */
+typedef struct mo_batch mo_batch;
+/* A plan for `count` square matrices of orders n[0..count) (host array, 1..MO_BATCH_MAX_N,
+ * else MO_EBATCHN), each with nrhs right-hand sides (0: factor only).  The plan orders the
+ * matrices longest first, groups them by the kernel configuration chosen for their size
+ * bucket and records one CUDA graph (queue reset + one persistent kernel per group, the
+ * group with the largest matrices first) on its first run. */
+MO_API int mo_batch_create(mo_ctx *ctx, int kind, int count, const int32_t *n, int nrhs,
+                           mo_batch **plan);
+MO_API int mo_batch_destroy(mo_batch *plan);
+/* Factor every A_i in place and, when B is non-NULL, solve A_i X_i = B_i in place (B_i is
+ * n_i x nrhs).  All arrays are DEVICE arrays of `count` entries: A / B / piv hold device
+ * pointers, lda / ldb leading dimensions (>= n_i).  piv (LU only) receives n_i 0-based
+ * row indices per matrix (piv[k] = row exchanged with row k).  info[i] = 0, or for
+ * Cholesky the column + 1 whose pivot is not positive (that matrix is left partially
+ * factored and not solved), for LU the first column + 1 with an exactly zero pivot.
+ * Asynchronous on the context's stream: one graph launch; a call with other pointer
+ * arrays updates the graph's kernel parameters instead of re-recording it. */
+MO_API int mo_batch_run(mo_batch *plan, double *const *A, const int64_t *lda, double *const *B,
+                        const int64_t *ldb, int64_t *const *piv, int *info);
+/* Autotuner: for each size bucket in the plan, times every kernel configuration (panel
+ * width 32 or 16, CTAs per SM) on synthetic matrices of the plan's own orders (`reps`
+ * timed runs each, best kept) and keeps the fastest.  ms (optional, MO_BATCH_BUCKETS x 2
+ * doubles) receives the times (-1 where a bucket is empty).  Synchronous. */
+MO_API int mo_batch_tune(mo_batch *plan, int reps, double *ms);
+/* Read (set = 0) or replace (set = 1) the per-bucket configuration table (MO_BATCH_BUCKETS
+ * ints, each 0 or 1), e.g. to persist a tuned schedule and restore it in a later run. */
+MO_API int mo_batch_schedule(mo_batch *plan, int *cfg, int set);
 
 /* ---- allocation-free variant (no counterpart in the reference) ---- */
 

@@ -19,8 +19,8 @@ class MoMatrix(ctypes.Structure):
 
 class MoProfile(ctypes.Structure):
     """mo_profile: per-class launches, device ms, algorithmic flops and bytes."""
-    _fields_ = [("launches", ctypes.c_int64 * 8), ("ms", ctypes.c_double * 8),
-                ("flops", ctypes.c_double * 8), ("bytes", ctypes.c_double * 8)]
+    _fields_ = [("launches", ctypes.c_int64 * 9), ("ms", ctypes.c_double * 9),
+                ("flops", ctypes.c_double * 9), ("bytes", ctypes.c_double * 9)]
 
 
 class MoIRInfo(ctypes.Structure):
@@ -72,6 +72,11 @@ def lib() -> ctypes.CDLL:
         "mo_measure_fp64_peak": [p, d, ctypes.POINTER(d)],
         "mo_solve_trm_static": [M, M, d, i, p],
         "mo_dsposv_ir": [p, M, M, M, i, i, i, d, i, ctypes.POINTER(MoIRInfo)],
+        "mo_batch_create": [p, i, i, p, i, ctypes.POINTER(p)],
+        "mo_batch_destroy": [p],
+        "mo_batch_run": [p, p, p, p, p, p, p],
+        "mo_batch_tune": [p, i, p],
+        "mo_batch_schedule": [p, p, i],
         "mo_lp_gemm": [p, i, i64, i64, i64, ctypes.c_float, p, i64, p, i64, ctypes.c_float, p,
                        i64, i],
     }

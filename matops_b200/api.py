@@ -269,7 +269,7 @@ def host_matrix(rows: int, cols: int, pinned: bool = True) -> torch.Tensor:
 
 class Profile:
     """Per-kernel-class launches / device time / algorithmic work (mo_profile)."""
-    CLASSES = ("gemm", "diag", "trtri", "panel", "laswp", "other", "lpgemm", "ir")
+    CLASSES = ("gemm", "diag", "trtri", "panel", "laswp", "other", "lpgemm", "ir", "batch")
 
     def __init__(self, raw):
         self.launches = {k: int(raw.launches[i]) for i, k in enumerate(self.CLASSES)}
@@ -297,3 +297,100 @@ def MeasureFP64Peak(ms: float = 200.0) -> float:
     if rc:
         raise RuntimeError(_lib.lib().mo_strerror(rc).decode())
     return out.value
+
+
+# ---- batched factor + solve (no counterpart in the reference; one DecomposeCHOL /
+# SolveCHOL or DecomposeLU / SolveLU per matrix there) ----
+
+BATCH_CHOL, BATCH_LU = 1, 2
+BATCH_MAX_N, BATCH_BUCKETS = 512, 4
+
+
+class BatchPlan:
+    """A reusable plan (mo_batch) for factoring, and optionally solving, many small
+    systems of the given orders in one CUDA-graph launch.  run() takes lists of column-major
+    CUDA float64 matrices (views allowed); their pointer arrays are cached on the device
+    while the same list objects are passed again."""
+
+    def __init__(self, kind: int, orders, nrhs: int = 0):
+        import numpy as np
+        self.kind, self.nrhs = kind, nrhs
+        self.orders = np.ascontiguousarray(orders, dtype=np.int32)
+        self._h = ctypes.c_void_p()
+        rc = _lib.lib().mo_batch_create(context(), kind, len(self.orders),
+                                        ctypes.c_void_p(self.orders.ctypes.data), nrhs,
+                                        ctypes.byref(self._h))
+        if rc:
+            raise MatopsError(rc, _lib.lib().mo_strerror(rc).decode())
+        self._arrays = None
+        self._key = None
+
+    def close(self):
+        if self._h:
+            _lib.lib().mo_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _pack(self, As, Bs, pivs):
+        key = (tuple(a.data_ptr() for a in As), tuple(b.data_ptr() for b in Bs) if Bs else None,
+               tuple(p.data_ptr() for p in pivs) if pivs else None)
+        if key == self._key:
+            return self._arrays
+        dev = As[0].device if As else torch.device("cuda", torch.cuda.current_device())
+
+        def ptrs(ts):
+            return torch.tensor([t.data_ptr() for t in ts], dtype=torch.int64, device=dev)
+
+        def lds(ts):
+            return torch.tensor([view(t).ld for t in ts], dtype=torch.int64, device=dev)
+        for a, n in zip(As, self.orders):
+            if tuple(a.shape) != (int(n), int(n)):
+                raise ValueError("matrix shape does not match the plan's order")
+        arr = {"A": ptrs(As), "lda": lds(As),
+               "B": ptrs(Bs) if Bs else None, "ldb": lds(Bs) if Bs else None,
+               "piv": ptrs(pivs) if pivs else None,
+               "info": torch.zeros(len(As), dtype=torch.int32, device=dev)}
+        self._arrays, self._key = arr, key
+        return arr
+
+    def run(self, As, Bs=None, pivs=None):
+        """Factor every A (and solve A X = B in place when Bs is given).  pivs: list of CUDA
+        int64 tensors (LU).  Returns the device int32 info tensor (0 = success)."""
+        if len(As) != len(self.orders):
+            raise ValueError("number of matrices does not match the plan")
+        for a in As:
+            view(a)
+        if Bs is not None:
+            for b, n in zip(Bs, self.orders):
+                if view(b).rows != n or b.shape[1] != self.nrhs:
+                    raise ValueError("right-hand side shape does not match the plan")
+        arr = self._pack(As, Bs, pivs)
+
+        def p(t):
+            return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+        rc = _lib.lib().mo_batch_run(self._h, p(arr["A"]), p(arr["lda"]), p(arr["B"]),
+                                     p(arr["ldb"]), p(arr["piv"]), p(arr["info"]))
+        if rc:
+            raise MatopsError(rc, _lib.lib().mo_strerror(rc).decode())
+        return arr["info"]
+
+    def tune(self, reps: int = 3):
+        """Autotune the per-bucket kernel configuration; returns {bucket: [ms cfg0, ms cfg1]}."""
+        ms = (ctypes.c_double * (BATCH_BUCKETS * 2))()
+        rc = _lib.lib().mo_batch_tune(self._h, reps, ms)
+        if rc:
+            raise MatopsError(rc, _lib.lib().mo_strerror(rc).decode())
+        return {b: [ms[2 * b], ms[2 * b + 1]] for b in range(BATCH_BUCKETS) if ms[2 * b] >= 0}
+
+    def schedule(self, cfg=None):
+        """Read (cfg None) or set the per-bucket configuration table."""
+        arr = (ctypes.c_int * BATCH_BUCKETS)(*(cfg or [0] * BATCH_BUCKETS))
+        rc = _lib.lib().mo_batch_schedule(self._h, arr, 1 if cfg is not None else 0)
+        if rc:
+            raise MatopsError(rc, _lib.lib().mo_strerror(rc).decode())
+        return list(arr)

@@ -200,6 +200,7 @@ const char *mo_strerror(int s) {
     case MO_ENOMEM: return "device out of memory";
     case MO_ENOKERNEL: return "no sm_100a kernel image for this device";
     case MO_ESTATICLIMIT: return "matrix order exceeds the fixed scratch of mo_solve_trm_static";
+    case MO_EBATCHN: return "batched matrix order outside 1..MO_BATCH_MAX_N";
     default: return s > 0 ? "illegal value (non-positive pivot)" : "unknown error";
   }
 }
