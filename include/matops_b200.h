@@ -218,6 +218,27 @@ MO_API int mo_lp_gemm(mo_ctx *ctx, int prec, int64_t M, int64_t N, int64_t K, fl
                       const float *A, int64_t lda, const float *B, int64_t ldb, float beta,
                       float *C, int64_t ldc, int flags);
 
+/* ---- reverse mode (no counterpart in the reference: the adjoints of DecomposeCHOL,
+ * chol.go:116, and SolveCHOL, chol.go:147, for LOWER factors) ---- */
+
+/* Given the factor L of A = L L^T (as mo_decompose_chol leaves it with MO_LOWER; only
+ * its lower triangle is read) and Lbar, the adjoint of L (lower triangle read), overwrite
+ * Lbar with the symmetric gradient Abar (both triangles): for every symmetric
+ * perturbation dA, d(loss) = sum_ij Abar_ij dA_ij.  Blocked right to left on the FP64
+ * GEMM engine, about 2 n^3 / 3 flops; it reads no stored forward panel and needs only a
+ * few 128 x 128 blocks of scratch.  flags: MO_LOWER (MO_UPPER -> MO_EINVAL).
+ * Asynchronous on the context's stream. */
+MO_API int mo_decompose_chol_adjoint(mo_ctx *ctx, mo_matrix L, mo_matrix Lbar, int flags);
+/* The same for `count` independent matrices (host arrays of views), spread over a pool of
+ * streams forked from and joined back into the context's stream. */
+MO_API int mo_decompose_chol_adjoint_batched(mo_ctx *ctx, int count, const mo_matrix *L,
+                                             const mo_matrix *Lbar, int flags);
+/* Adjoint of X = A^-1 B solved with the factor L (SolveCHOL LOWER): Xbar (n x nrhs) is
+ * overwritten with Bbar = A^-1 Xbar, and Abar (n x n) receives Abar -= (Bbar X^T +
+ * X Bbar^T) / 2, the symmetric gradient of the solve with respect to A.  Asynchronous. */
+MO_API int mo_solve_chol_adjoint(mo_ctx *ctx, mo_matrix L, mo_matrix X, mo_matrix Xbar,
+                                 mo_matrix Abar, int flags);
+
 /* ---- batched factor + solve of many small systems (no counterpart in the reference,
  * which factors one matrix per call: DecomposeCHOL chol.go:116 / SolveCHOL chol.go:147,
  * DecomposeLU lu.go:420 / SolveLU lu.go:483; each matrix gets the same results those

@@ -72,6 +72,9 @@ def lib() -> ctypes.CDLL:
         "mo_measure_fp64_peak": [p, d, ctypes.POINTER(d)],
         "mo_solve_trm_static": [M, M, d, i, p],
         "mo_dsposv_ir": [p, M, M, M, i, i, i, d, i, ctypes.POINTER(MoIRInfo)],
+        "mo_decompose_chol_adjoint": [p, M, M, i],
+        "mo_decompose_chol_adjoint_batched": [p, i, p, p, i],
+        "mo_solve_chol_adjoint": [p, M, M, M, M, i],
         "mo_batch_create": [p, i, i, p, i, ctypes.POINTER(p)],
         "mo_batch_destroy": [p],
         "mo_batch_run": [p, p, p, p, p, p, p],

@@ -394,3 +394,26 @@ class BatchPlan:
         if rc:
             raise MatopsError(rc, _lib.lib().mo_strerror(rc).decode())
         return list(arr)
+
+
+# ---- reverse mode (no counterpart in the reference) ----
+
+def DecomposeCHOLAdjoint(L, Lbar, flags: int = LOWER):
+    """Lbar (adjoint of the lower factor L of A = L L^T) is overwritten with the symmetric
+    gradient of A.  Returns None or a MatopsError."""
+    return _err(_lib.lib().mo_decompose_chol_adjoint(context(), view(L), view(Lbar), flags))
+
+
+def DecomposeCHOLAdjointBatched(Ls, Lbars, flags: int = LOWER):
+    """DecomposeCHOLAdjoint for lists of independent matrices (one call, a pool of streams)."""
+    n = len(Ls)
+    arrL = (_lib.MoMatrix * max(n, 1))(*[view(t) for t in Ls])
+    arrG = (_lib.MoMatrix * max(n, 1))(*[view(t) for t in Lbars])
+    return _err(_lib.lib().mo_decompose_chol_adjoint_batched(context(), n, arrL, arrG, flags))
+
+
+def SolveCHOLAdjoint(L, X, Xbar, Abar, flags: int = LOWER):
+    """Adjoint of X = A^-1 B (A = L L^T): Xbar becomes Bbar = A^-1 Xbar and
+    Abar -= (Bbar X^T + X Bbar^T) / 2."""
+    return _err(_lib.lib().mo_solve_chol_adjoint(context(), view(L), view(X), view(Xbar),
+                                                 view(Abar), flags))

@@ -156,6 +156,12 @@ int mo_ctx_destroy(mo_ctx *ctx) {
   cudaStreamSynchronize(ctx->stream);
   if (ctx->ws) cudaFree(ctx->ws);
   if (ctx->ws_ir) cudaFree(ctx->ws_ir);
+  if (ctx->ws_adj) cudaFree(ctx->ws_adj);
+  for (auto s : ctx->pool) {
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+  }
+  for (auto e : ctx->pool_ev) cudaEventDestroy(e);
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->sk_partial) cudaFree(ctx->sk_partial);
   if (ctx->sk_flags) cudaFree(ctx->sk_flags);

@@ -39,6 +39,12 @@ struct mo_ctx {
   // it may call for a fallback grow and reallocate)
   void *ws_ir = nullptr;
   size_t ws_ir_bytes = 0;
+  // scratch of the Cholesky adjoint (a few 128 x 128 blocks per stream) and the stream
+  // pool of its batched form
+  void *ws_adj = nullptr;
+  size_t ws_adj_bytes = 0;
+  std::vector<cudaStream_t> pool;
+  std::vector<cudaEvent_t> pool_ev;
 };
 
 namespace mo {
