@@ -99,6 +99,11 @@ def run_case(args):
                         torch.device("cuda", torch.cuda.current_device()), reps=max(1, args.steps))
         print(json.dumps({"case": args.case, **res}), flush=True)
         return 0
+    elif kind == "adjoint":
+        res = adjoint_leg(mo, torch.device("cuda", torch.cuda.current_device()),
+                          reps=max(1, args.steps))
+        print(json.dumps({"case": args.case, **res}), flush=True)
+        return 0
     elif kind == "batched":
         # batched:KIND:COUNT[:TUNE] -- config 4 (KIND 1 = Cholesky, 2 = LU; TUNE 0 skips
         # the autotuner)
@@ -214,13 +219,22 @@ def mixed_leg(mo, n, nrhs, kappas, precs, dev, reps=2):
                 torch.cuda.synchronize()
                 assert err is None, err
                 tm.append(a.elapsed_time(b))
+            # one more solve with per-kernel-class tracing (not part of the timing above)
+            mo.ProfileRead()
+            mo.ProfileEnable(True)
+            mo.SolveCHOLMixed(X, A, B, LOWER, prec, mo.IR_AUTO, 1e-14, 40)
+            prof = mo.ProfileRead()
+            mo.ProfileEnable(False)
+            by_class = {k: {"ms": round(v, 3), "launches": prof.launches[k]}
+                        for k, v in prof.ms.items() if prof.launches[k]}
             name = "tf32x3" if prec == mo.PREC_TF32X3 else "bf16x3"
             row[name] = {"ms": min(tm), "speedup_vs_fp64": min(tf) / min(tm),
                          "iters": info.iters, "gmres_iters": info.gmres_iters,
                          "method": "gmres" if info.method == mo.IR_GMRES else "classic",
                          "fallback": info.fallback, "converged": info.converged,
                          "shift": info.shift, "berr": info.berr, "berr_check": berr(X),
-                         "ferr_vs_fp64": float((X - Xf).norm() / Xf.norm())}
+                         "ferr_vs_fp64": float((X - Xf).norm() / Xf.norm()),
+                         "traced_ms_by_class": by_class}
             del X
         out[f"kappa={kappa:.0e}"] = row
         del A, Xf
@@ -291,6 +305,98 @@ def batched_leg(mo, kind, count, seed, dev, reps=5, tune=True):
            "sizes": "n_i ~ U{16..512}", "flops": flops, "bytes": byts}
     plan.close()
     return out, (sizes, mats(flat0), vecs(rhs0))
+
+
+def adjoint_leg(mo, dev, n_single=8192, batch=512, n_batch=256, reps=3):
+    """Config 5: forward (DecomposeCHOL + SolveCHOL) and reverse (Cholesky adjoint + solve
+    adjoint) of loss = sum(W*L) + 2 sum(log diag L) + w^T x in FP64, A = G G^T / n + I;
+    single n = 8192 and a batch of 512 x n = 256.  Device time of forward and backward."""
+    import torch
+    res = {}
+    g = torch.Generator(device=dev).manual_seed(10)
+
+    def problem(n):
+        G = mo.matrix(n, n)
+        G.normal_(generator=g)
+        A = mo.matrix(n, n)
+        assert mo.Mult(A, G, G, 1.0 / n, 0.0, mo.TRANSB) is None
+        A.diagonal().add_(1.0)
+        W = torch.randn(n, n, dtype=torch.float64, device=dev, generator=g)
+        b = mo.matrix(n, 1)
+        b.normal_(generator=g)
+        w = mo.matrix(n, 1)
+        w.normal_(generator=g)
+        return A, W, b, w
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+    # single
+    n = n_single
+    A, W, b, w = problem(n)
+    L, x, G, xb, Ab = mo.matrix(n, n), mo.matrix(n, 1), mo.matrix(n, n), mo.matrix(n, 1), mo.matrix(n, n)
+    tf, tb = [], []
+    for r in range(reps + 1):
+        L.copy_(A)
+        x.copy_(b)
+        torch.cuda.synchronize()
+        e0, e1, e2 = ev(), ev(), ev()
+        e0.record()
+        _, err = mo.DecomposeCHOL(L, LOWER, 64)
+        assert err is None
+        mo.SolveCHOL(x, L, LOWER)
+        e1.record()
+        # Lbar = tril(W) + 2 diag(1/L_ii), xbar = w
+        G.copy_(torch.tril(W))
+        G.diagonal().add_(2.0 / L.diagonal())
+        xb.copy_(w)
+        Ab.zero_()
+        assert mo.SolveCHOLAdjoint(L, x, xb, Ab, LOWER) is None
+        assert mo.DecomposeCHOLAdjoint(L, G, LOWER) is None
+        G.add_(Ab)
+        e2.record()
+        torch.cuda.synchronize()
+        if r > 0:
+            tf.append(e0.elapsed_time(e1))
+            tb.append(e1.elapsed_time(e2))
+    fl_f = n ** 3 / 3 + 2.0 * n * n
+    fl_b = 2 * n ** 3 / 3 + 6.0 * n * n
+    res["single_8192"] = {"forward_ms": min(tf), "backward_ms": min(tb),
+                          "forward_tflops": fl_f / (min(tf) * 1e-3) / 1e12,
+                          "backward_tflops": fl_b / (min(tb) * 1e-3) / 1e12,
+                          "grad_symmetric": bool(torch.equal(G, G.t()))}
+    del A, W, b, w, L, x, G, xb, Ab
+    torch.cuda.empty_cache()
+    # batch: forward by the batched factor + solve plan, reverse by the batched adjoint
+    nb_ = n_batch
+    probs = [problem(nb_) for _ in range(batch)]
+    Ls = [mo.matrix(nb_, nb_) for _ in range(batch)]
+    xs = [mo.matrix(nb_, 1) for _ in range(batch)]
+    Gs = [mo.matrix(nb_, nb_) for _ in range(batch)]
+    plan = mo.BatchPlan(mo.BATCH_CHOL, [nb_] * batch, 1)
+    tf, tb = [], []
+    for r in range(reps + 1):
+        for (A, W, b, w), L, x in zip(probs, Ls, xs):
+            L.copy_(A)
+            x.copy_(b)
+        torch.cuda.synchronize()
+        e0, e1, e2 = ev(), ev(), ev()
+        e0.record()
+        info = plan.run(Ls, xs)
+        e1.record()
+        for (A, W, b, w), L, G in zip(probs, Ls, Gs):
+            G.copy_(torch.tril(W))
+        assert mo.DecomposeCHOLAdjointBatched(Ls, Gs, LOWER) is None
+        e2.record()
+        torch.cuda.synchronize()
+        assert int(info.abs().sum()) == 0
+        if r > 0:
+            tf.append(e0.elapsed_time(e1))
+            tb.append(e1.elapsed_time(e2))
+    plan.close()
+    res["batch_512x256"] = {"forward_ms": min(tf), "backward_ms_incl_Lbar_setup": min(tb),
+                            "forward_tflops": batch * (nb_ ** 3 / 3) / (min(tf) * 1e-3) / 1e12,
+                            "backward_tflops": batch * (2 * nb_ ** 3 / 3) / (min(tb) * 1e-3) / 1e12}
+    return res
 
 
 def workload(n, nrhs):
@@ -632,6 +738,11 @@ def main():
         torch.cuda.empty_cache()
         extras["mixed_ir"] = mixed_leg(mo, n, 16, [1e2, 1e6, 1e10],
                                        [mo.PREC_TF32X3, mo.PREC_BF16X3], dev)
+        torch.cuda.empty_cache()
+        extras["batched_chol_4096"], _ = batched_leg(mo, mo.BATCH_CHOL, 4096, 8, dev, reps=3)
+        extras["batched_lu_4096"], _ = batched_leg(mo, mo.BATCH_LU, 4096, 9, dev, reps=3)
+        torch.cuda.empty_cache()
+        extras["adjoint"] = adjoint_leg(mo, dev)
 
     # ---- CPU baseline (rank 0, one GPU only) ----
     cpu = None
