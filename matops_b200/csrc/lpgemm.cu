@@ -1,85 +1,63 @@
-// Split-product GEMM on the tensor cores (BF16x3 / TF32x3, FP32 accumulation) for the
-// mixed-precision Cholesky; see lp.cuh for the number format.
-//
-// Tile 128 x 128, 256 threads (8 warps as 2 x 4, warp tile 64 x 32).  A stage holds 64
-// bytes of K per row (32 bf16 or 16 tf32 elements) for the four parts A.hi, A.lo, B.hi,
-// B.lo, loaded with 16-byte cp.async into a 4-deep ring; fragments come from ldmatrix
-// (a 16-byte chunk of row r is stored at chunk c ^ ((r >> 1) & 3), so the 8 rows of an
-// ldmatrix phase fall in distinct banks).  One k-step is 32 bytes of K: m16n8k16 for bf16,
-// m16n8k8 for tf32 -- both read A as (rows 0-7 | 8-15) x (bytes 0-15 | 16-31) and B as
-// rows 0-7 x (bytes 0-15 | 16-31), so one ldmatrix addressing serves both.  Each
-// product issues lo*hi, hi*lo, hi*hi into one FP32 accumulator.  CTAs are persistent;
-// the slab stream runs across tile boundaries, so the next tile's loads are in flight
-// during a tile's epilogue.
+// Split-product GEMM on the 5th-generation tensor cores (tcgen05.mma with TMEM
+// accumulators) for the mixed-precision Cholesky: C = beta*C + alpha * A * B^T with A, B
+// stored pre-split (hi, lo) and K-major, each product formed as hi*hi + hi*lo + lo*hi
+// with FP32 accumulation (BF16x3: kind::f16 with BF16 inputs; TF32x3: kind::tf32); see
+// lp.cuh for the number format.
 #include <cuda_bf16.h>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <algorithm>
+#include <atomic>
+#include <mutex>
 
 #include "lp.cuh"
 
 namespace mo {
 namespace {
 
-constexpr int LBM = 128, LBN = 128;
-constexpr int LTHREADS = 256;
-constexpr int LSTAGES = 4;
-constexpr int LROWB = 64;                  // bytes of K per row per stage
-constexpr int LPART = LBM * LROWB;         // 8 KB
-constexpr int LSTAGE = 4 * LPART;          // A.hi, A.lo, B.hi, B.lo
-constexpr int LSMEM = LSTAGES * LSTAGE;    // 128 KB
+// Tile 128 x 128 of C per step of a persistent CTA; K consumed in stages of 128 bytes per
+// operand row (64 bf16 or 32 tf32 elements), four 16 KB parts per stage (A.hi, A.lo,
+// B.hi, B.lo) loaded by TMA with the 128-byte swizzle into a 3-deep ring.  Warp roles:
+//   warp 0    TMA producer (one thread)
+//   warp 1    TMEM owner (allocates 256 columns = two 128 x 128 FP32 accumulators) and
+//             MMA issuer (one thread): per 32-byte K step three tcgen05.mma -- hi*hi,
+//             hi*lo, lo*hi -- into the same accumulator; tcgen05.commit frees the smem
+//             stage, and after the tile's last stage signals the epilogue
+//   warps 2-5 epilogue: tcgen05.ld of their 32-lane quarter of the accumulator (TMEM lane
+//             = tile row), C = alpha * acc + beta * C, coalesced along the column
+// The accumulator is double-buffered, so the MMAs of tile t + 1 overlap the epilogue of
+// tile t.  C (FP32, column-major) moves through a 64 KB shared tile: the producer loads
+// it by TMA after the tile's operand stages, the epilogue combines it with the
+// accumulator in place and one thread stores it back by TMA (when C's base and leading
+// dimension allow TMA; otherwise the epilogue reads and writes C directly).  Every wait
+// is bounded (MO_SPIN_LIMIT) and reports MO_EDEVTIMEOUT.
+constexpr int TB = 128;                  // tile rows = tile columns
+constexpr int TSTAGES = 2;
+constexpr int TPART = TB * 128;          // one operand part of a stage: 128 rows x 128 B
+constexpr int TSTAGE = 4 * TPART;        // 64 KB
+constexpr int TCTILE = TB * TB * 4;      // the C tile in shared memory (column-major FP32)
+constexpr int TTHREADS = 192;
+constexpr int TSMEM = TSTAGES * TSTAGE + TCTILE + 1024 + 256;  // + alignment slack + barriers
+constexpr int TMEM_COLS = 256;
 
-struct LpParams {
+struct TcParams {
   int M, N, K;
   float alpha, beta;
-  const char *a_hi, *a_lo, *b_hi, *b_lo;
-  int64_t a_ldb, b_ldb;  // bytes between rows
   float *C;
   int64_t ldc;
   int mode;
-  int mt, nt;     // tiles per dimension
-  int ntiles;     // tiles in the schedule
-  int kslabs;     // K / (elements per 64 bytes)
+  int mt, nt;
+  int ntiles;   // tiles in the schedule (lower mode: only those with tm >= tn)
+  int kstages;  // ceil(K * esize / 128)
+  int c_tma;    // C moves through shared memory by TMA (else plain loads and stores)
+  int c_load;   // the C tile is read (beta != 0, or lower mode)
+  int *status;
 };
 
-__device__ __forceinline__ uint32_t swz(int r, int c) {
-  return (uint32_t)(r * LROWB + ((c ^ ((r >> 1) & 3)) << 4));
-}
-
-__device__ __forceinline__ void cp_async_16(uint32_t dst, const void *src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-__device__ __forceinline__ void ldsm_x4(uint32_t addr, uint32_t &r0, uint32_t &r1, uint32_t &r2,
-                                        uint32_t &r3) {
-  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
-               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
-               : "r"(addr));
-}
-
-template <int PREC>
-__device__ __forceinline__ void mma(float (&d)[4], const uint32_t (&a)[4], uint32_t b0,
-                                    uint32_t b1) {
-  if (PREC == kLpBf16x3)
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
-        "{%8,%9}, {%0,%1,%2,%3};"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-  else
-    asm volatile(
-        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
-        "{%8,%9}, {%0,%1,%2,%3};"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-
 // tile index -> (tm, tn); lower mode enumerates tiles with tm >= tn column by column
-__device__ __forceinline__ void tile_coords(const LpParams &p, int t, int &tm, int &tn) {
+__device__ __forceinline__ void tile_coords(const TcParams &p, int t, int &tm, int &tn) {
   if (p.mode == kGemmLower) {
     int c = 0;
     while (t >= p.mt - c) {
@@ -94,135 +72,254 @@ __device__ __forceinline__ void tile_coords(const LpParams &p, int t, int &tm, i
   }
 }
 
-// issue the cp.async copies of slab `s` of tile (tm, tn) into stage buffer `st`
-__device__ __forceinline__ void load_slab(const LpParams &p, uint32_t st, int tm, int tn, int s) {
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int idx = threadIdx.x + i * LTHREADS;
-    const int part = idx >> 9, rem = idx & 511;
-    const int r = rem >> 2, c = rem & 3;
-    const char *base;
-    int64_t ldb;
-    int row;
-    if (part < 2) {
-      base = part == 0 ? p.a_hi : p.a_lo;
-      ldb = p.a_ldb;
-      row = tm * LBM + r;
-    } else {
-      base = part == 2 ? p.b_hi : p.b_lo;
-      ldb = p.b_ldb;
-      row = tn * LBN + r;
-    }
-    cp_async_16(st + part * LPART + swz(r, c), base + row * ldb + s * LROWB + c * 16);
-  }
+// UMMA shared-memory descriptor of a K-major operand with the 128-byte swizzle: start
+// address >> 4, leading offset 1 (unused for swizzled K-major), stride between 8-row
+// groups 1024 B, descriptor version 1, layout SWIZZLE_128B (2)
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | (1ull << 16) | (64ull << 32) | (1ull << 46) |
+         (2ull << 61);
+}
+
+// instruction descriptor: FP32 accumulator, A and B K-major, N = M = 128
+template <int PREC>
+__host__ __device__ constexpr uint32_t idesc() {
+  return (1u << 4) | ((PREC == kLpBf16x3 ? 1u : 2u) << 7) | ((PREC == kLpBf16x3 ? 1u : 2u) << 10) |
+         ((uint32_t)(TB >> 3) << 17) | ((uint32_t)(TB >> 4) << 24);
 }
 
 template <int PREC>
-__global__ void __launch_bounds__(LTHREADS, 1) lp_gemm_kernel(LpParams p) {
-  extern __shared__ __align__(128) char lsm[];
-  const uint32_t sbase = smem_u32(lsm);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wm = warp & 1, wn = warp >> 1;
-  const int g = lane >> 2, t4 = lane & 3;
-  const int mine = (p.ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
-  if (mine <= 0) return;
-  const int G = mine * p.kslabs;
-  auto slab_tile = [&](int gi, int &tm, int &tn, int &s) {
-    const int ti = gi / p.kslabs;
-    s = gi - ti * p.kslabs;
-    tile_coords(p, (int)blockIdx.x + ti * (int)gridDim.x, tm, tn);
-  };
-#pragma unroll
-  for (int gi = 0; gi < LSTAGES - 1; ++gi) {
-    if (gi < G) {
-      int tm, tn, s;
-      slab_tile(gi, tm, tn, s);
-      load_slab(p, sbase + gi * LSTAGE, tm, tn, s);
-    }
-    cp_commit();
-  }
-  // ldmatrix row/chunk of this lane for the A (x4: rows +8 by q&1, chunk by q>>1) and
-  // B (x4: rows +8 by q>>1, chunk by q&1) fragment loads
-  const int q = lane >> 3, rr = lane & 7;
-  const int a_row = wm * 64 + rr + 8 * (q & 1), a_ch = q >> 1;
-  const int b_row = wn * 32 + rr + 8 * (q >> 1), b_ch = q & 1;
-  float acc[4][4][4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
+__device__ __forceinline__ void umma(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
+  if (PREC == kLpBf16x3)
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+        "l"(a), "l"(b), "r"(idesc<PREC>()), "r"(acc));
+  else
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+        "l"(a), "l"(b), "r"(idesc<PREC>()), "r"(acc));
+}
 
-  for (int gi = 0; gi < G; ++gi) {
-    cp_wait<LSTAGES - 2>();
-    __syncthreads();
-    if (gi + LSTAGES - 1 < G) {
-      int tm, tn, s;
-      slab_tile(gi + LSTAGES - 1, tm, tn, s);
-      load_slab(p, sbase + ((gi + LSTAGES - 1) % LSTAGES) * LSTAGE, tm, tn, s);
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+        "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tma_store_2d(const void *tmap, const void *src, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];" ::"l"(tmap),
+      "r"(smem_u32(src)), "r"(x), "r"(y)
+      : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(TTHREADS, 1)
+    lp_gemm_tc_kernel(const __grid_constant__ CUtensorMap tAh, const __grid_constant__ CUtensorMap tAl,
+                      const __grid_constant__ CUtensorMap tBh, const __grid_constant__ CUtensorMap tBl,
+                      const __grid_constant__ CUtensorMap tC, const TcParams p) {
+  extern __shared__ __align__(16) unsigned char tsm_raw[];
+  // the swizzle pattern repeats every 1024 bytes: align the ring to it
+  unsigned char *tsm = tsm_raw + ((1024 - (smem_u32(tsm_raw) & 1023)) & 1023);
+  float *ctile = reinterpret_cast<float *>(tsm + TSTAGES * TSTAGE);
+  uint64_t *full = reinterpret_cast<uint64_t *>(tsm + TSTAGES * TSTAGE + TCTILE);
+  uint64_t *empty = full + TSTAGES;
+  uint64_t *tfull = empty + TSTAGES;   // [2]
+  uint64_t *tempty = tfull + 2;        // [2]
+  uint64_t *cfull = tempty + 2;
+  uint64_t *cempty = cfull + 1;
+  uint64_t *cready = cempty + 1;  // the four epilogue warps have written the C tile
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(cready + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < TSTAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
     }
-    cp_commit();
-    const uint32_t st = sbase + (gi % LSTAGES) * LSTAGE;
-#pragma unroll
-    for (int ks = 0; ks < 2; ++ks) {
-      uint32_t ah[4][4], al[4][4], bh[4][2], bl[4][2];
-#pragma unroll
-      for (int mt = 0; mt < 4; ++mt) {
-        const uint32_t off = swz(a_row + 16 * mt, 2 * ks + a_ch);
-        ldsm_x4(st + off, ah[mt][0], ah[mt][1], ah[mt][2], ah[mt][3]);
-        ldsm_x4(st + LPART + off, al[mt][0], al[mt][1], al[mt][2], al[mt][3]);
-      }
-#pragma unroll
-      for (int np = 0; np < 2; ++np) {
-        const uint32_t off = swz(b_row + 16 * np, 2 * ks + b_ch);
-        ldsm_x4(st + 2 * LPART + off, bh[2 * np][0], bh[2 * np][1], bh[2 * np + 1][0],
-                bh[2 * np + 1][1]);
-        ldsm_x4(st + 3 * LPART + off, bl[2 * np][0], bl[2 * np][1], bl[2 * np + 1][0],
-                bl[2 * np + 1][1]);
-      }
-#pragma unroll
-      for (int mt = 0; mt < 4; ++mt)
-#pragma unroll
-        for (int nt = 0; nt < 4; ++nt) {
-          mma<PREC>(acc[mt][nt], al[mt], bh[nt][0], bh[nt][1]);
-          mma<PREC>(acc[mt][nt], ah[mt], bl[nt][0], bl[nt][1]);
-          mma<PREC>(acc[mt][nt], ah[mt], bh[nt][0], bh[nt][1]);
-        }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], 4);
     }
-    if ((gi + 1) % p.kslabs == 0) {
-      // epilogue of this tile: C = beta*C + alpha*acc (column-major), lower mask
-      int tm, tn, s;
-      slab_tile(gi, tm, tn, s);
-      const int i0 = tm * LBM + wm * 64 + g, j0 = tn * LBN + wn * 32 + 2 * t4;
-      const bool lower = p.mode == kGemmLower;
-#pragma unroll
-      for (int mt = 0; mt < 4; ++mt) {
-        float cv[4][4];
-        if (p.beta != 0.f) {
-#pragma unroll
-          for (int nt = 0; nt < 4; ++nt)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              const int i = i0 + 16 * mt + 8 * (e >> 1), j = j0 + 8 * nt + (e & 1);
-              cv[nt][e] = ((!lower || i >= j) && i < p.M && j < p.N) ? p.C[i + (int64_t)j * p.ldc]
-                                                                      : 0.f;
-            }
-        }
-#pragma unroll
-        for (int nt = 0; nt < 4; ++nt)
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            const int i = i0 + 16 * mt + 8 * (e >> 1), j = j0 + 8 * nt + (e & 1);
-            float v = p.alpha * acc[mt][nt][e];
-            if (p.beta != 0.f) v = fmaf(p.beta, cv[nt][e], v);
-            if ((!lower || i >= j) && i < p.M && j < p.N) p.C[i + (int64_t)j * p.ldc] = v;
-            acc[mt][nt][e] = 0.f;
-          }
-      }
-    }
+    mbar_init(cfull, 1);
+    mbar_init(cempty, 1);
+    mbar_init(cready, 4);
+    fence_barrier_init();
   }
-  cp_wait<0>();
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  constexpr int ES = PREC == kLpBf16x3 ? 2 : 4;
+  constexpr int KEL = 128 / ES;  // K elements per stage
+
+  if (warp == 0 && lane == 0) {
+    // producer: the operand stages of tile t, then (once the previous tile's C has been
+    // stored) its C tile
+    int g = 0, tc = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x, ++tc) {
+      int tm, tn;
+      tile_coords(p, t, tm, tn);
+      for (int ks = 0; ks < p.kstages; ++ks, ++g) {
+        const int slot = g % TSTAGES;
+        const uint32_t ph = (g / TSTAGES) & 1;
+        if (!mbar_wait(&empty[slot], ph ^ 1, p.status)) {
+          ok = false;
+          break;
+        }
+        unsigned char *st = tsm + slot * TSTAGE;
+        mbar_arrive_expect_tx(&full[slot], TSTAGE);
+        tma_load_2d(st, &tAh, &full[slot], ks * KEL, tm * TB);
+        tma_load_2d(st + TPART, &tAl, &full[slot], ks * KEL, tm * TB);
+        tma_load_2d(st + 2 * TPART, &tBh, &full[slot], ks * KEL, tn * TB);
+        tma_load_2d(st + 3 * TPART, &tBl, &full[slot], ks * KEL, tn * TB);
+      }
+      if (!ok || !p.c_tma) continue;
+      if (!mbar_wait(cempty, (tc & 1) ^ 1, p.status)) break;
+      if (p.c_load) {
+        mbar_arrive_expect_tx(cfull, TCTILE);
+        tma_load_2d(ctile, &tC, cfull, tm * TB, tn * TB);
+      } else {
+        mbar_arrive(cfull);
+      }
+    }
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer
+    int g = 0, tc = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x, ++tc) {
+      const int buf = tc & 1;
+      if (!mbar_wait(&tempty[buf], ((tc >> 1) & 1) ^ 1, p.status)) break;
+      tc_fence_after();
+      const uint32_t d = tmem + buf * TB;
+      for (int ks = 0; ks < p.kstages; ++ks, ++g) {
+        const int slot = g % TSTAGES;
+        if (!mbar_wait(&full[slot], (g / TSTAGES) & 1, p.status)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t base = smem_u32(tsm + slot * TSTAGE);
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+          const uint64_t ah = sdesc(base + kk * 32), al = sdesc(base + TPART + kk * 32);
+          const uint64_t bh = sdesc(base + 2 * TPART + kk * 32),
+                         bl = sdesc(base + 3 * TPART + kk * 32);
+          umma<PREC>(d, ah, bh, (ks | kk) != 0);
+          umma<PREC>(d, ah, bl, 1);
+          umma<PREC>(d, al, bh, 1);
+        }
+        umma_commit(&empty[slot]);
+      }
+      if (ok) umma_commit(&tfull[buf]);
+    }
+  } else if (warp >= 2) {
+    // epilogue: warp w reads TMEM lanes 32 * (w % 4) .. + 31 (= tile rows)
+    const int q = warp & 3;
+    const int rl = q * 32 + lane;
+    int tc = 0;
+    for (int t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++tc) {
+      int tm, tn;
+      tile_coords(p, t, tm, tn);
+      const int buf = tc & 1;
+      if (!mbar_wait(&tfull[buf], (tc >> 1) & 1, p.status)) break;
+      tc_fence_after();
+      const int row = tm * TB + rl;
+      if (p.c_tma) {
+        if (!mbar_wait(cfull, tc & 1, p.status)) break;
+#pragma unroll 1
+        for (int c0 = 0; c0 < TB; c0 += 16) {
+          uint32_t v[16];
+          tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + buf * TB + c0, v);
+#pragma unroll
+          for (int r = 0; r < 16; ++r) {
+            const int col = tn * TB + c0 + r;
+            float *cs = ctile + (c0 + r) * TB + rl;
+            const float a = p.alpha * __uint_as_float(v[r]);
+            const float nv = p.beta == 0.f ? a : fmaf(p.beta, *cs, a);
+            if (p.mode != kGemmLower || row >= col) *cs = nv;
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&tempty[buf]);
+        // the four epilogue warps' shared-memory writes, then one TMA store of the tile
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(cready);
+        if (warp == 2) {
+          int ok = 1;
+          if (lane == 0) {
+            ok = mbar_wait(cready, tc & 1, p.status) ? 1 : 0;
+            if (ok) {
+              tma_store_2d(&tC, ctile, tm * TB, tn * TB);
+              mbar_arrive(cempty);
+            }
+          }
+          if (!__shfl_sync(0xffffffffu, ok, 0)) break;  // warp-uniform exit
+        }
+      } else {
+        const bool rok = row < p.M;
+#pragma unroll 1
+        for (int c0 = 0; c0 < TB; c0 += 16) {
+          float cv[16];
+#pragma unroll
+          for (int r = 0; r < 16; ++r) {
+            const int col = tn * TB + c0 + r;
+            cv[r] = (p.beta != 0.f && rok && col < p.N) ? p.C[row + (int64_t)col * p.ldc] : 0.f;
+          }
+          uint32_t v[16];
+          tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + buf * TB + c0, v);
+#pragma unroll
+          for (int r = 0; r < 16; ++r) {
+            const int col = tn * TB + c0 + r;
+            if (rok && col < p.N && (p.mode != kGemmLower || row >= col))
+              p.C[row + (int64_t)col * p.ldc] = fmaf(p.beta, cv[r], p.alpha * __uint_as_float(v[r]));
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&tempty[buf]);
+      }
+    }
+    // the last tile's store has been read out of shared memory; let it reach global memory
+    if (warp == 2 && lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(TMEM_COLS)
+                 : "memory");
+  }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -296,17 +393,64 @@ __global__ void __launch_bounds__(256) lp_split_kernel(const float *X, int64_t l
   }
 }
 
+PFN_cuTensorMapEncodeTiled_v12000 tc_encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// 2-D map over a K-major split operand: `rows` rows of K elements, `ldk` elements apart;
+// box = 128 bytes of K x 128 rows, 128-byte swizzle; rows and K beyond the extents read 0
+bool split_tmap(CUtensorMap *tm, const void *ptr, int prec, int64_t K, int64_t rows, int64_t ldk) {
+  auto fn = tc_encode_fn();
+  if (!fn) return false;
+  const int es = lp_esize(prec);
+  if (((uintptr_t)ptr & 15) || (ldk * es) % 16) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)std::max<int64_t>(K, 1), (cuuint64_t)std::max<int64_t>(rows, 1)};
+  cuuint64_t strides[1] = {(cuuint64_t)(ldk * es)};
+  cuuint32_t box[2] = {(cuuint32_t)(128 / es), (cuuint32_t)TB};
+  cuuint32_t estr[2] = {1, 1};
+  const CUtensorMapDataType dt =
+      prec == kLpBf16x3 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  return fn(tm, dt, 2, const_cast<void *>(ptr), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// map over the FP32 column-major C: box 128 rows x 128 columns, no swizzle
+bool c_tmap(CUtensorMap *tm, float *C, int64_t M, int64_t N, int64_t ldc) {
+  auto fn = tc_encode_fn();
+  if (!fn) return false;
+  if (((uintptr_t)C & 15) || (ldc * 4) % 16) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)std::max<int64_t>(M, 1), (cuuint64_t)std::max<int64_t>(N, 1)};
+  cuuint64_t strides[1] = {(cuuint64_t)(ldc * 4)};
+  cuuint32_t box[2] = {(cuuint32_t)TB, (cuuint32_t)TB};
+  cuuint32_t estr[2] = {1, 1};
+  return fn(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, C, dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <int PREC>
-int launch_lp(mo_ctx *ctx, LpParams &p, int grid) {
-  static int attr_mask = 0;
+int launch_tc(mo_ctx *ctx, const CUtensorMap (&m)[5], const TcParams &p, int grid) {
+  static std::atomic<uint64_t> attr_done{0};
   int dev = 0;
   cudaGetDevice(&dev);
-  if (!(attr_mask & (1 << (dev & 31)))) {
-    MO_CUDA_TRY(cudaFuncSetAttribute(lp_gemm_kernel<PREC>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, LSMEM));
-    attr_mask |= 1 << (dev & 31);
+  const uint64_t bit = 1ull << (dev & 63);
+  if (!(attr_done.load() & bit)) {
+    MO_CUDA_TRY(cudaFuncSetAttribute(lp_gemm_tc_kernel<PREC>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, TSMEM));
+    attr_done.fetch_or(bit);
   }
-  lp_gemm_kernel<PREC><<<grid, LTHREADS, LSMEM, ctx->stream>>>(p);
+  lp_gemm_tc_kernel<PREC><<<grid, TTHREADS, TSMEM, ctx->stream>>>(m[0], m[1], m[2], m[3], m[4], p);
   MO_CUDA_TRY(cudaGetLastError());
   return MO_OK;
 }
@@ -315,40 +459,45 @@ int launch_lp(mo_ctx *ctx, LpParams &p, int grid) {
 
 int lp_gemm(mo_ctx *ctx, int prec, const LpGemmArgs &a) {
   if (a.M <= 0 || a.N <= 0 || a.K <= 0) return MO_OK;
-  // the split operands must hold roundup(M or N, 128) rows and K % 32 == 0 columns
-  // (zeros past the true extents); C is written only inside M x N
+  // the split operands hold at least M (A) and N (B) rows of K elements, ldk apart,
+  // K % 32 == 0; C is written only inside M x N
   if (a.K % 32) return MO_EINVAL;
   if (prec != kLpBf16x3 && prec != kLpTf32x3) return MO_EINVAL;
   const int es = lp_esize(prec);
-  LpParams p;
+  TcParams p;
   p.M = a.M;
   p.N = a.N;
   p.K = a.K;
   p.alpha = a.alpha;
   p.beta = a.beta;
-  p.a_hi = (const char *)a.A.hi;
-  p.a_lo = (const char *)a.A.lo;
-  p.b_hi = (const char *)a.B.hi;
-  p.b_lo = (const char *)a.B.lo;
-  p.a_ldb = a.A.ldk * es;
-  p.b_ldb = a.B.ldk * es;
   p.C = a.C;
   p.ldc = a.ldc;
   p.mode = a.mode == kGemmLower ? kGemmLower : kGemm;
-  p.mt = (a.M + LBM - 1) / LBM;
-  p.nt = (a.N + LBN - 1) / LBN;
+  p.mt = (a.M + TB - 1) / TB;
+  p.nt = (a.N + TB - 1) / TB;
   if (p.mode == kGemmLower && p.nt > p.mt) return MO_EINVAL;
   p.ntiles = p.mode == kGemmLower ? p.nt * p.mt - p.nt * (p.nt - 1) / 2 : p.mt * p.nt;
-  p.kslabs = a.K * es / LROWB;
+  p.kstages = (a.K * es + 127) / 128;
+  p.status = &control(ctx)->status;
+  CUtensorMap m[5];
+  p.c_tma = c_tmap(&m[4], a.C, a.M, a.N, a.ldc) ? 1 : 0;
+  if (!p.c_tma) m[4] = CUtensorMap{};
+  p.c_load = (a.beta != 0.f || p.mode == kGemmLower) ? 1 : 0;
+  if (!split_tmap(&m[0], a.A.hi, prec, a.K, a.M, a.A.ldk) ||
+      !split_tmap(&m[1], a.A.lo, prec, a.K, a.M, a.A.ldk) ||
+      !split_tmap(&m[2], a.B.hi, prec, a.K, a.N, a.B.ldk) ||
+      !split_tmap(&m[3], a.B.lo, prec, a.K, a.N, a.B.ldk))
+    return MO_EINVAL;
   int grid = std::min(p.ntiles, ctx->sms);
   if (a.max_ctas > 0) grid = std::min(grid, a.max_ctas);
   ProfScope ps;
   prof_begin(ctx, ps, MO_PROF_LPGEMM);
-  const int rc = prec == kLpBf16x3 ? launch_lp<kLpBf16x3>(ctx, p, grid)
-                                   : launch_lp<kLpTf32x3>(ctx, p, grid);
-  const double tiles_flops = (double)p.ntiles * LBM * LBN * a.K * 2.0;
+  const int rc = prec == kLpBf16x3 ? launch_tc<kLpBf16x3>(ctx, m, p, grid)
+                                   : launch_tc<kLpTf32x3>(ctx, m, p, grid);
+  // flops of the three products; bytes of C (read if beta != 0, written) and the operands
+  const double tiles_flops = 3.0 * (double)p.ntiles * TB * TB * a.K * 2.0;
   prof_end(ctx, ps, tiles_flops,
-           (double)p.ntiles * LBM * LBN * 4.0 * (a.beta != 0.f ? 2.0 : 1.0) +
+           (double)p.ntiles * TB * TB * 4.0 * (a.beta != 0.f ? 2.0 : 1.0) +
                (double)(a.M + a.N) * a.K * es * 2.0);
   return rc;
 }
