@@ -1,21 +1,26 @@
 #!/usr/bin/env python
-"""Benchmark: FP64 Cholesky factor + solve at n = 16384 (64 RHS) on B200.
+"""Benchmark: Cholesky solve at n = 16384 (64 RHS) on B200, mixed precision + FP64
+refinement against the plain FP64 path on the same system.
 
-One step = DecomposeCHOL(A, LOWER) + SolveCHOL(B, A, LOWER) on a fresh device copy of
-A = G*G^T/n + 0.5*I (G iid N(0,1), seed 2) and B iid U[-1,1] (seed 3), through the C ABI
-(libmatops_b200.so).  Every step works on its own 2 GiB copy of A, so inputs are larger
-than L2 and nothing is reused between steps.
+System: A = G*G^T/n + 0.5*I (G iid N(0,1), seed 2), B iid U[-1,1] (seed 3), generated on
+the device.  Through the C ABI (libmatops_b200.so):
+  headline step  SolveCHOLMixed: TF32x3 split-product Cholesky on the tensor cores (FP64
+                 diagonal blocks), FP64 residuals and updates until the normwise backward
+                 error is <= 1e-14 (A is read, not modified; 2 GiB > L2 per step)
+  fp64_path      DecomposeCHOL + SolveCHOL in FP64 on fresh copies of A
 
 Reported on one JSON line (rank 0):
-  value / ms_per_step   device time of one step (CUDA events, max over ranks)
-  roofline              the DMMA GEMM engine (SYRK / TRSM updates) during the timed steps:
-                        algorithmic FLOPs / its summed event time vs the FP64 tensor-pipe peak
-                        measured on this device in the same run
-  e2e                   the same step through the public API with HOST buffers: upload A, B
-                        (pinned), factor, solve, download the factor and X
-  cpu_baseline          the reference's own C kernels (oracle/_ref) on this host, on a
+  value / ms_per_step   device time of one headline step (CUDA events, max over ranks)
+  roofline              the dominant kernel of the step, the tcgen05 split-product GEMM:
+                        its algorithmic bytes / summed event time vs measured HBM bandwidth
+                        (with its tensor-pipe fraction beside)
+  e2e                   the headline step through the public API with HOST buffers: upload
+                        A, B (pinned), solve, download X
+  cpu_baseline          the reference's own C kernels (oracle/_ref) on this host (FP64
+                        DecomposeCHOL + SolveCHOL; the reference has no mixed precision), on a
                         bounded sample scaled to n = 16384
-  extras                DGEMM 2048^3 (alpha 1.5, beta -0.5) as % of FP64 peak; LU + SolveLU
+  extras                DGEMM 2048^3 (alpha 1.5, beta -0.5) as % of FP64 peak; LU + SolveLU;
+                        the kappa sweep of the mixed solve; batched and adjoint workloads
 
 --impl reference times the reference's CPU path alone (rank 0) and prints its line.
 Multi-GPU (torchrun): independent replicas, one system per rank, no collective in the path.
@@ -99,6 +104,24 @@ def run_case(args):
                         torch.device("cuda", torch.cuda.current_device()), reps=max(1, args.steps))
         print(json.dumps({"case": args.case, **res}), flush=True)
         return 0
+    elif kind == "mixed":
+        # mixed:N:NRHS[:PREC] -- SolveCHOLMixed on A = G G^T/n + 0.5 I (PREC 2 = TF32x3, 1 = BF16x3)
+        n, nrhs = dims[0], dims[1]
+        prec = dims[2] if len(dims) > 2 else mo.PREC_TF32X3
+        G = mo.matrix(n, n)
+        G.normal_(generator=g)
+        A = mo.matrix(n, n)
+        mo.Mult(A, G, G, 1.0 / n, 0.0, mo.TRANSB)
+        A.diagonal().add_(0.5)
+        del G
+        B = mo.matrix(n, nrhs)
+        B.uniform_(-1.0, 1.0, generator=g)
+        X = mo.matrix(n, nrhs)
+
+        def fn():
+            info, err = mo.SolveCHOLMixed(X, A, B, LOWER, prec, mo.IR_AUTO, 1e-14, 40)
+            assert err is None and info.converged
+        flops = n ** 3 / 3.0
     elif kind == "adjoint":
         res = adjoint_leg(mo, torch.device("cuda", torch.cuda.current_device()),
                           reps=max(1, args.steps))
@@ -400,8 +423,16 @@ def adjoint_leg(mo, dev, n_single=8192, batch=512, n_batch=256, reps=3):
 
 
 def workload(n, nrhs):
-    return (f"DecomposeCHOL+SolveCHOL FP64, n={n}, {nrhs} RHS, A=G*G^T/n+0.5I "
-            f"(G~N(0,1) seed 2), B~U[-1,1] seed 3")
+    return (f"Cholesky solve, n={n}, {nrhs} RHS, A=G*G^T/n+0.5I (G~N(0,1) seed 2), "
+            f"B~U[-1,1] seed 3: mixed-precision factor + FP64 refinement to berr<=1e-14 "
+            f"(value), DecomposeCHOL+SolveCHOL FP64 (fp64_path)")
+
+
+def _measured_peak(key, fallback):
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))[key])
+    except Exception:
+        return fallback
 
 
 # --------------------------------------------------------------------------------------
@@ -584,10 +615,11 @@ def main():
     nsteps = W + K
     copies_bytes = nsteps * n * n * 8
     free = torch.cuda.mem_get_info(dev)[0]
-    fresh = copies_bytes < 0.7 * free
+    fresh = copies_bytes < 0.6 * free
     As = [A0.clone() for _ in range(nsteps)] if fresh else [mo.matrix(n, n)]
     Bs = [B0.clone() for _ in range(nsteps)]
 
+    # ---- the comparison arm: the plain FP64 path, DecomposeCHOL + SolveCHOL ----
     def step(i):
         A = As[i] if fresh else As[0]
         if not fresh:
@@ -605,46 +637,92 @@ def main():
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     barrier()
+    e0.record()
+    for i in range(W, nsteps):
+        step(i)
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    prof64 = mo.ProfileRead()
+    mo.ProfileEnable(False)
+    fp64_ms = max_over_ranks(e0.elapsed_time(e1) / K)
+    X = Bs[nsteps - 1]
+    R = B0.clone()
+    assert mo.Mult(R, A0, X, -1.0, 1.0, 0) is None
+    fp64_berr = float(R.norm() / (A0.norm() * X.norm() + B0.norm()))
+    del As, Bs, R
+    torch.cuda.empty_cache()
+    g_ms, g_fl = prof64.ms["gemm"] / K, prof64.flops["gemm"] / K
+    fp64_path = {
+        "ms": fp64_ms, "berr": fp64_berr, "tflops": n ** 3 / 3 / (fp64_ms * 1e-3) / 1e12,
+        "frac_fp64_peak": n ** 3 / 3 / (fp64_ms * 1e-3) / 1e12 / fp64_peak,
+        "gemm_engine_tflops": g_fl / (g_ms * 1e-3) / 1e12 if g_ms else None,
+        "per_class_ms_per_step": {k: v / K for k, v in prof64.ms.items() if prof64.launches[k]},
+        "launches_per_step": sum(prof64.launches.values()) / K,
+    }
+
+    # ---- the headline: TF32x3 factor + FP64 refinement to berr <= 1e-14, same A and B ----
+    Xm = mo.matrix(n, nrhs)
+
+    def mstep():
+        info, err = mo.SolveCHOLMixed(Xm, A0, B0, LOWER, mo.PREC_TF32X3, mo.IR_AUTO, 1e-14, 40)
+        assert err is None and info.converged and not info.fallback, (err, info)
+        return info
+
+    for _ in range(W):
+        mstep()
+    torch.cuda.synchronize()
+    barrier()
+    mo.ProfileRead()
+    mo.ProfileEnable(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    barrier()
+    infos = []
     with ClockSampler(dev) as clk:
         e0.record()
-        for i in range(W, nsteps):
-            step(i)
+        for _ in range(K):
+            infos.append(mstep())
         e1.record()
         torch.cuda.synchronize()
     barrier()
     prof = mo.ProfileRead()
     mo.ProfileEnable(False)
     ms = max_over_ranks(e0.elapsed_time(e1) / K)
-
-    # backward error of the last solve: ||B - A X|| / (||A|| ||X|| + ||B||)
-    X = Bs[nsteps - 1]
     R = B0.clone()
-    assert mo.Mult(R, A0, X, -1.0, 1.0, 0) is None
-    berr = float(R.norm() / (A0.norm() * X.norm() + B0.norm()))
-    del As, Bs, R
+    assert mo.Mult(R, A0, Xm, -1.0, 1.0, 0) is None
+    berr = float(R.norm() / (A0.norm() * Xm.norm() + B0.norm()))
+    del R
 
-    g_ms = prof.ms["gemm"] / K
-    g_fl = prof.flops["gemm"] / K
-    achieved = g_fl / (g_ms * 1e-3) / 1e12 if g_ms > 0 else 0.0
+    # roofline of the dominant kernel, the tcgen05 split-product GEMM (lp_gemm_tc_kernel):
+    # bytes = its C tile read + write and operand reads, flops = the three products
+    l_ms, l_fl, l_by = prof.ms["lpgemm"] / K, prof.flops["lpgemm"] / K, prof.bytes["lpgemm"] / K
+    l_n = prof.launches["lpgemm"] / K
+    hbm_peak = _measured_peak("hbm_gbs", 6650.0)
+    bf16_peak = _measured_peak("bf16_tflops", 1590.0)
+    achieved_gbs = l_by / (l_ms * 1e-3) / 1e9 if l_ms else 0.0
+    achieved_tf = l_fl / (l_ms * 1e-3) / 1e12 if l_ms else 0.0
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "gemm_engine_traffic.json")
+    tpath = os.path.join(ROOT, "profiles", "lp_gemm_tc_traffic.json")
     if os.path.exists(tpath):
         try:
             traffic = json.load(open(tpath)).get("bytes_per_launch")
         except Exception:
             traffic = None
     roofline = {
-        "bound": "tensor", "kernel": "dgemm_tile_kernel (SYRK/GEMM updates)",
-        "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-        "frac": achieved / fp64_peak if fp64_peak else None, "traffic": traffic,
-        "peak_source": "FP64 mma.sync (DMMA) loop measured on this device in this run "
-                       "(MEASURED_PEAKS.json has no FP64 figure)",
-        "share_of_step": g_ms / ms if ms else None,
-        "per_class_ms_per_step": {k: v / K for k, v in prof.ms.items()},
-        "per_class_tflops": {k: (prof.flops[k] / (prof.ms[k] * 1e-3) / 1e12 if prof.ms[k] else None)
-                             for k in prof.ms},
+        "bound": "hbm", "kernel": "lp_gemm_tc_kernel (TF32x3 trailing updates and panels)",
+        "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
+        "frac": achieved_gbs / hbm_peak, "traffic": traffic,
+        "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)",
+        "algorithmic_bytes_per_launch": l_by / l_n if l_n else None,
+        "avg_launch_ms": l_ms / l_n if l_n else None,
+        "tensor": {"achieved_tflops": achieved_tf, "tf32_dense_peak_tflops": bf16_peak / 2,
+                   "frac": achieved_tf / (bf16_peak / 2),
+                   "peak_source": "half of MEASURED_PEAKS.json bf16_tflops (TF32 runs at half the BF16 rate)"},
+        "share_of_step": l_ms / ms if ms else None,
+        "per_class_ms_per_step": {k: v / K for k, v in prof.ms.items() if prof.launches[k]},
     }
-    launches = sum(prof.launches.values())
+    launches = sum(prof.launches.values()) / K
 
     # ---- e2e: host buffers through the public API ----
     e2e = None
@@ -655,17 +733,15 @@ def main():
         Bh.copy_(B0.cpu())
         Ad = mo.matrix(n, n)
         Bd = mo.matrix(n, nrhs)
-        Lh = mo.host_matrix(n, n)
+        Xd = mo.matrix(n, nrhs)
         Xh = mo.host_matrix(n, nrhs)
 
         def e2e_step():
             mo.Upload(Ad, Ah)
             mo.Upload(Bd, Bh)
-            _, err = mo.DecomposeCHOL(Ad, LOWER, 64)
-            assert err is None
-            mo.SolveCHOL(Bd, Ad, LOWER)
-            mo.Download(Lh, Ad)
-            mo.Download(Xh, Bd)
+            info, err = mo.SolveCHOLMixed(Xd, Ad, Bd, LOWER, mo.PREC_TF32X3, mo.IR_AUTO, 1e-14, 40)
+            assert err is None and info.converged
+            mo.Download(Xh, Xd)
 
         e2e_step()
         torch.cuda.synchronize()
@@ -680,9 +756,10 @@ def main():
         barrier()
         e_ms = max_over_ranks(f0.elapsed_time(f1) / ke)
         e2e = {"value": e_ms * 1e-3, "unit": "s", "h2d_bytes_per_step": 8 * (n * n + n * nrhs),
-               "d2h_bytes_per_step": 8 * (n * n + n * nrhs), "steps": ke,
-               "what": "pinned host A,B -> upload, DecomposeCHOL, SolveCHOL, download L and X"}
-        del Ah, Bh, Ad, Bd, Lh, Xh
+               "d2h_bytes_per_step": 8 * n * nrhs, "steps": ke,
+               "what": "pinned host A, B -> upload, SolveCHOLMixed (TF32x3 + FP64 refinement), "
+                       "download X"}
+        del Ah, Bh, Ad, Bd, Xd, Xh
 
     # ---- extras: DGEMM 2048^3 and LU at n ----
     extras = {"mixed_ir": None}
@@ -759,13 +836,18 @@ def main():
         line = {
             "metric": METRIC, "value": ms * 1e-3, "unit": "s", "n_gpus": world, "steps": K,
             "warmup": W, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": workload(n, nrhs), "n": n, "nrhs": nrhs, "nb": 64,
-                       "l2": "fresh 2 GiB copy of A per step (inputs > L2)" if fresh
-                             else "A restored from a copy each step (2 GiB > L2)",
+            "vs_baseline": None, "dtype": "tf32x3+f64", "data": "synthetic",
+            "config": {"workload": workload(n, nrhs), "n": n, "nrhs": nrhs,
+                       "factor": "TF32x3 split products, FP32 storage, FP64 128x128 diagonal blocks",
+                       "refinement": "FP64 residual and update, classic IR / GMRES-IR (auto), tol 1e-14",
+                       "l2": "A (2 GiB FP64) is re-read from HBM by every step (inputs > L2)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-            "berr": berr, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": launches, "gpu_launches_by_class": prof.launches,
+            "berr": berr, "berr_inf": max(i.berr for i in infos),
+            "ir_iters": [i.iters for i in infos], "gmres_iters": [i.gmres_iters for i in infos],
+            "fp64_path": fp64_path, "speedup_vs_fp64": fp64_ms / ms,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": int(sum(prof.launches.values())),
+            "gpu_launches_by_class": prof.launches,
             "clocks": clk.summary(), "fp64_peak_tflops": fp64_peak, "extras": extras,
         }
         print(json.dumps(line), flush=True)

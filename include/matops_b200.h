@@ -94,8 +94,8 @@ MO_API int mo_set_syrk_blas_beta(mo_ctx *ctx, int on);
 #define MO_PROF_TRTRI 2    /* diagonal-block triangular inverses for TRSM               */
 #define MO_PROF_PANEL 3    /* LU panel (pivot search, interchanges, rank-1 updates)      */
 #define MO_PROF_LASWP 4    /* row interchanges outside the panel                        */
-#define MO_PROF_OTHER 5
-#define MO_PROF_LPGEMM 6   /* split-product (BF16x3 / TF32x3) GEMMs and operand splits  */
+#define MO_PROF_OTHER 5    /* everything else, incl. operand splits and FP32 conversions */
+#define MO_PROF_LPGEMM 6   /* split-product (BF16x3 / TF32x3) tcgen05 GEMMs              */
 #define MO_PROF_IR 7       /* refinement: FP64 residuals, norms, GMRES vector kernels   */
 #define MO_PROF_BATCH 8    /* batched factor + solve launches (whole graph)              */
 #define MO_PROF_CLASSES 9

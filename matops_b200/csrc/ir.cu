@@ -236,6 +236,50 @@ __global__ void vfill_kernel(double *dst, double v, int64_t count) {
   if (e < count) dst[e] = v;
 }
 
+// S = the symmetric matrix whose lower (UP == false) or upper triangle A stores, written in
+// full (n x n, ld n); 32 x 32 tiles through shared memory so both the reads of the stored
+// triangle and the mirrored writes are coalesced
+template <bool UP>
+__global__ void sym_full_kernel(const double *A, int64_t lda, int n, double *S) {
+  __shared__ double T[32][33];
+  const int bi = blockIdx.x, bj = blockIdx.y;  // tile row, tile column of S
+  if (UP ? bi > bj : bi < bj) return;          // tiles on the stored side write both copies
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
+  for (int r = ty; r < 32; r += 8) {
+    const int i = bi * 32 + tx, j = bj * 32 + r;
+    double v = 0.0;
+    if (i < n && j < n) {
+      const bool stored = UP ? i <= j : i >= j;
+      v = stored ? A[i + (int64_t)j * lda] : A[j + (int64_t)i * lda];
+    }
+    T[r][tx] = v;
+    if (i < n && j < n) S[i + (int64_t)j * n] = v;
+  }
+  if (bi == bj) return;
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {  // mirrored tile: S(j, i) = S(i, j)
+    const int i = bj * 32 + tx, j = bi * 32 + r;
+    if (i < n && j < n) S[i + (int64_t)j * n] = T[tx][r];
+  }
+}
+
+// out[j] = sum_i |S(i, j)| (= the row sums, S symmetric); one CTA per column
+__global__ void __launch_bounds__(256) abs_colsum_kernel(const double *S, int n, double *out) {
+  __shared__ double red[8];
+  const int j = blockIdx.x;
+  double t = 0.0;
+  for (int i = threadIdx.x; i < n; i += 256) t += fabs(S[i + (int64_t)j * n]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double u = 0.0;
+    for (int w = 0; w < 8; ++w) u += red[w];
+    out[j] = u;
+  }
+}
+
 // ---------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------
@@ -254,13 +298,35 @@ struct Solver {
   double *norms;          // [0, nr): |r|, [nr, 2nr): |x|, [2nr, 3nr): |b|, 3nr: |A|
   int *flags;             // trsm_few block flags
   int nblk_dot, pstride;
+  double *S = nullptr;    // full symmetric copy of A (many right-hand sides only)
 };
+
+// products with A through the FP64 GEMM engine on the symmetric copy pay off above this
+// many right-hand sides (one 128-column tile pass against a 16-column pass per group)
+constexpr int kGemmResidualMinRhs = 33;
 
 dim3 vgrid(int n, int nr) { return dim3((n + 255) / 256, nr); }
 
 int sym_apply(Solver &s, const double *X, int64_t ldx, const double *Bv, double *Y, double sa,
               bool abs_a, int nr) {
   mo_ctx *ctx = s.ctx;
+  if (s.S) {
+    if (abs_a) {  // row sums of |A| (X is the ones vector)
+      ProfScope ps;
+      prof_begin(ctx, ps, MO_PROF_IR);
+      abs_colsum_kernel<<<s.n, 256, 0, ctx->stream>>>(s.S, s.n, Y);
+      prof_end(ctx, ps, (double)s.n * s.n, 8.0 * s.n * (double)s.n);
+      MO_CUDA_TRY(cudaGetLastError());
+      return MO_OK;
+    }
+    if (Bv) {
+      vcopy_kernel<<<vgrid(s.n, nr), 256, 0, ctx->stream>>>(Y, s.n, Bv, s.n, s.n, nr);
+      MO_CUDA_TRY(cudaGetLastError());
+    }
+    const View Yv{Y, s.n, nr, s.n}, Sv{s.S, s.n, s.n, s.n},
+        Xv{const_cast<double *>(X), s.n, nr, ldx};
+    return gemm(ctx, Yv, Sv, false, Xv, false, sa, Bv ? 1.0 : 0.0);
+  }
   ProfScope ps;
   prof_begin(ctx, ps, MO_PROF_IR);
   for (int c0 = 0; c0 < nr; c0 += RNR) {
@@ -426,10 +492,11 @@ size_t ir_bytes(int n, int nr, int prec, bool gmres_possible) {
   const size_t vec = align256((size_t)n * nr * 8);
   const int nblk_dot = (n + DOT_ROWS - 1) / DOT_ROWS;
   size_t b = lp_chol_bytes(n, prec) + 4 * vec;
+  if (nr >= kGemmResidualMinRhs) b += align256((size_t)n * n * 8);
   if (gmres_possible) b += (kGmresMax + 1) * vec;
   b += 2 * align256((size_t)(kGmresMax + 1) * nr * 8) + align256((size_t)nr * 8);
   b += align256((size_t)nblk_dot * (kGmresMax + 2) * nr * 8);
-  b += align256((size_t)(3 * nr + 1) * 8) + align256((size_t)((n + 63) / 64 + 64) * 4) + 4096;
+  b += align256((size_t)(3 * nr + 1) * 8) + align256((size_t)(128 * ((n + 63) / 64) + 64) * 4) + 4096;
   return b;
 }
 
@@ -535,8 +602,18 @@ int dsposv(mo_ctx *ctx, const View &X, const View &A, const View &B, bool upper,
   s.pstride = (kGmresMax + 2) * nr;
   s.partial = (double *)take((size_t)s.nblk_dot * s.pstride * 8);
   s.norms = (double *)take((size_t)(3 * nr + 1) * 8);
-  s.flags = (int *)take((size_t)((n + 63) / 64 + 64) * 4);
+  s.flags = (int *)take((size_t)(128 * ((n + 63) / 64) + 64) * 4);
   int rc;
+  if (nr >= kGemmResidualMinRhs) {
+    s.S = (double *)take((size_t)n * n * 8);
+    const dim3 tg((n + 31) / 32, (n + 31) / 32);
+    ProfScope ps;
+    prof_begin(ctx, ps, MO_PROF_IR);
+    if (upper) sym_full_kernel<true><<<tg, 256, 0, st>>>(A.d, A.ld, n, s.S);
+    else sym_full_kernel<false><<<tg, 256, 0, st>>>(A.d, A.ld, n, s.S);
+    prof_end(ctx, ps, 0.0, 8.0 * n * (double)n * 1.5);
+    MO_CUDA_TRY(cudaGetLastError());
+  }
   // b, |b|, |A|_inf (row sums of |A| through the same symmetric kernel, with x = 1)
   vcopy_kernel<<<vgrid(n, nr), 256, 0, st>>>(s.b, n, B.d, B.ld, n, nr);
   vfill_kernel<<<(n + 255) / 256, 256, 0, st>>>(s.d, 1.0, n);

@@ -215,7 +215,7 @@ int lp_chol_setup(int n, int prec, void *mem, LpChol &f) {
 int lp_chol_convert(mo_ctx *ctx, const LpChol &f, View A, bool upper, double shift) {
   const dim3 grid(f.NP / 32, f.NP / 32);
   ProfScope ps;
-  prof_begin(ctx, ps, MO_PROF_LPGEMM);
+  prof_begin(ctx, ps, MO_PROF_OTHER);
   lp_convert_kernel<<<grid, 256, 0, ctx->stream>>>(A.d, A.ld, f.n, upper, f.W, f.ldw, f.NP,
                                                    shift);
   prof_end(ctx, ps, 0.0, 8.0 * f.n * (double)f.n / 2 + 4.0 * (double)f.NP * f.NP);

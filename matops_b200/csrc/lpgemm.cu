@@ -509,7 +509,7 @@ int lp_split(mo_ctx *ctx, int prec, const float *X, int64_t ld, int rows, int co
   if (out.ldk % 8 || out.ldk < ((cols + 7) & ~7)) return MO_EINVAL;
   const dim3 grid((rows + 63) / 64, (cols + 31) / 32);
   ProfScope ps;
-  prof_begin(ctx, ps, MO_PROF_LPGEMM);
+  prof_begin(ctx, ps, MO_PROF_OTHER);
   if (prec == kLpBf16x3)
     lp_split_kernel<kLpBf16x3><<<grid, 256, 0, ctx->stream>>>(X, ld, rows, cols, (char *)out.hi,
                                                                (char *)out.lo, out.ldk);
@@ -526,7 +526,7 @@ int lp_split_cols(mo_ctx *ctx, int prec, const float *X, int64_t ld, int rows, i
   if (rows <= 0 || cols <= 0) return MO_OK;
   const dim3 grid(rows, (cols + 255) / 256);
   ProfScope ps;
-  prof_begin(ctx, ps, MO_PROF_LPGEMM);
+  prof_begin(ctx, ps, MO_PROF_OTHER);
   if (prec == kLpBf16x3)
     lp_split_cols_kernel<kLpBf16x3><<<grid, 256, 0, ctx->stream>>>(X, ld, rows, cols,
                                                                     (char *)out.hi,

@@ -74,7 +74,9 @@ int trsm(mo_ctx *ctx, View B, View A, int flags, double alpha) {
   const int nblk = (N + NBT - 1) / NBT;
   const size_t inv_bytes = (size_t)nblk * NBT * NBT * sizeof(double);
   double *inv = nullptr;
-  int rc = workspace(ctx, inv_bytes + sizeof(int) * (2 * nblk + 64), (void **)&inv);
+  // step flags of the few-column solve: up to 4 column groups x 64-row blocks, 32 ints apart
+  const size_t flag_ints = (size_t)4 * 32 * ((N + 63) / 64) + 64;
+  int rc = workspace(ctx, inv_bytes + sizeof(int) * flag_ints, (void **)&inv);
   if (rc) return rc;
   // few right-hand sides: one cooperative launch instead of a sweep of 2*nblk GEMMs
   if (nblk > 1 && nrhs <= 64)

@@ -1,14 +1,19 @@
 // Triangular solve with few right-hand sides (<= 64) in one cooperative launch.
 //
-// op(A) X = alpha*B with op(A) n x n triangular, split into 64-row blocks.  CTA c owns the
-// blocks of steps c, c+P, ... (steps run top-down for a lower op(A), bottom-up for upper).
-// For each owned step s it keeps its block of B in DMMA accumulator fragments, subtracts
-// op(A)[s, s'] X_s' for every earlier step s' as soon as that step's flag is published,
-// multiplies by the inverse of the diagonal block and publishes X_s (written over B) with
-// its flag.  The critical path is one 64 x 64 x nrhs update plus one 64 x 64 x nrhs product
-// per step on the FP64 tensor pipe (mma.sync m16n8k4); the next block of op(A) is prefetched
-// with cp.async while the CTA waits.  Blocks of op(A) are staged with coalesced reads (also
-// for op(A) = A^T).  Every wait is bounded and reports MO_EDEVTIMEOUT.
+// op(A) X = alpha*B with op(A) n x n triangular, split into 64-row blocks.  The columns of
+// B are cut into groups of at most 16, each solved by its own set of CTAs with its own
+// step flags, so the work on the dependency chain per step is that of 16 columns.  Within
+// a set, CTA c owns the blocks of steps c, c+P, ... (top-down for a lower op(A), bottom-up
+// for upper).  For each owned step s it keeps its block of B in DMMA accumulator fragments
+// and subtracts op(A)[s, s'] X_s' for the earlier steps s' in rounds: it waits for the
+// oldest missing step's flag, takes every consecutive published step up to a chunk of
+// (FP32 op(A): 3, FP64: 2) blocks, and applies them as one K = 64 x chunk product, while
+// the next chunk of op(A) streams in by cp.async (and, once every earlier step is known
+// published, the next chunk's X rows stream into registers).  Then X_s = inv(op(A)_ss) (B_s - ...) is
+// published (written over B) with its flag.  The critical path per step is one 64 x 64 x 16
+// update plus one 64 x 64 x 16 product on the FP64 tensor pipe (mma.sync m16n8k4).  Blocks of
+// op(A) are staged with coalesced reads (also for op(A) = A^T).  Every wait is bounded and
+// reports MO_EDEVTIMEOUT.
 //
 // B is addressed with a row and a column stride, so a right-side solve with few rows,
 // X op(A) = alpha*B, runs as op(A)^T X^T = alpha*B^T on the transposed view.
@@ -26,8 +31,6 @@ constexpr int IB = 128;   // order of the precomputed inverse blocks (trtri_bloc
 constexpr int FEW_THREADS = 128;  // 4 warps x 16 rows
 constexpr int MAX_RHS = 64;
 constexpr int LDL = TB + 4;   // smem row stride (== 4 mod 16 doubles: 2-way at most)
-constexpr int LDX = MAX_RHS + 4;
-constexpr int FEW_SMEM = (3 * TB * LDL + TB * LDX) * 8;  // inverse, 2 x op(A) block, X
 
 struct FewArgs {
   const void *A;  // double, or float for the mixed-precision factor (FP64 arithmetic)
@@ -39,12 +42,23 @@ struct FewArgs {
   int64_t brs, bcs;  // element (i, c) of B at B[i*brs + c*bcs]
   int nrhs;
   double alpha;
+  int groups;         // independent column groups of B (gw columns each), one per CTA set
+  int gw;
   const double *inv;  // 128 x 128 inverses of op(A)'s diagonal blocks (ld 128)
   bool inv_t;         // inv holds the inverses of A's blocks: read them transposed
-  int *flags;         // [nblk]
+  int *flags;         // [groups * nblk]
   int epoch;
   int *status;
 };
+
+// step flags sit one per 128-byte line, and pollers read them with acquire loads (not
+// atomics), so polling CTAs do not queue at the L2 ahead of the publishing store
+constexpr int FLAG_STRIDE = 32;
+__device__ __forceinline__ int flag_load(const int *f) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(f) : "memory");
+  return v;
+}
 
 __device__ __forceinline__ int step_block(const FewArgs &p, int s) {
   return p.lower_eff ? s : p.nblk - 1 - s;
@@ -63,19 +77,26 @@ __device__ __forceinline__ void cp_async_el(float *dst, const float *src, uint32
                : "memory");
 }
 
-// issue cp.async copies of op(A)[rb*64 .., cb*64 ..] into L (row-major, ld LDL); zero past N
+// issue cp.async copies of `cnt` blocks of op(A) -- block row rb, the block columns of
+// steps s0 .. s0 + cnt - 1 -- into the chunk buffer L (row-major, ld ldl, block j at
+// column j * 64); zero past N
 template <typename TA>
-__device__ __forceinline__ void stage_block(const FewArgs &p, TA *L, int rb, int cb) {
-  const int r0 = rb * TB, c0 = cb * TB;
+__device__ __forceinline__ void stage_chunk(const FewArgs &p, TA *L, int ldl, int rb, int s0,
+                                            int cnt) {
+  const int r0 = rb * TB;
   const TA *A = static_cast<const TA *>(p.A);
-  for (int e = threadIdx.x; e < TB * TB; e += blockDim.x) {
-    const int i = e % TB, j = e / TB;  // consecutive threads -> consecutive A addresses
-    if (!p.trans) {
-      const bool ok = r0 + i < p.N && c0 + j < p.N;
-      cp_async_el(L + i * LDL + j, ok ? A + (r0 + i) + (int64_t)(c0 + j) * p.lda : A, ok);
-    } else {
-      const bool ok = c0 + i < p.N && r0 + j < p.N;
-      cp_async_el(L + j * LDL + i, ok ? A + (c0 + i) + (int64_t)(r0 + j) * p.lda : A, ok);
+  for (int j = 0; j < cnt; ++j) {
+    const int c0 = step_block(p, s0 + j) * TB;
+    TA *Lj = L + j * TB;
+    for (int e = threadIdx.x; e < TB * TB; e += blockDim.x) {
+      const int i = e % TB, k = e / TB;  // consecutive threads -> consecutive A addresses
+      if (!p.trans) {
+        const bool ok = r0 + i < p.N && c0 + k < p.N;
+        cp_async_el(Lj + i * ldl + k, ok ? A + (r0 + i) + (int64_t)(c0 + k) * p.lda : A, ok);
+      } else {
+        const bool ok = c0 + i < p.N && r0 + k < p.N;
+        cp_async_el(Lj + k * ldl + i, ok ? A + (c0 + i) + (int64_t)(r0 + k) * p.lda : A, ok);
+      }
     }
   }
 }
@@ -93,39 +114,76 @@ __device__ __forceinline__ void stage_inverse(const FewArgs &p, double *I, int r
   }
 }
 
-// acc[nt] (+)= sign * M(16 rows of this warp, 64) * X(64, 8 nt ..)
+// acc[nt] (+)= sign * M(16 rows of this warp, K) * X(K, 8 nt ..)
 template <int NT, typename TM>
-__device__ __forceinline__ void block_mma(double (&acc)[NT][4], const TM *M, const double *X,
-                                          double sign) {
+__device__ __forceinline__ void block_mma(double (&acc)[NT][4], const TM *M, int ldm,
+                                          const double *X, int ldx, int K, double sign) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
-  const TM *m0 = M + (16 * warp + g) * LDL + t;
-  const TM *m1 = m0 + 8 * LDL;
-  const double *xb = X + t * LDX + g;
+  const TM *m0 = M + (16 * warp + g) * ldm + t;
+  const TM *m1 = m0 + 8 * ldm;
+  const double *xb = X + t * ldx + g;
 #pragma unroll 4
-  for (int k = 0; k < TB; k += 4) {
+  for (int k = 0; k < K; k += 4) {
     const double a0 = sign * (double)m0[k], a1 = sign * (double)m1[k];
 #pragma unroll
-    for (int nt = 0; nt < NT; ++nt) dmma_16x8x4(acc[nt], a0, a1, xb[k * LDX + 8 * nt]);
+    for (int nt = 0; nt < NT; ++nt) dmma_16x8x4(acc[nt], a0, a1, xb[k * ldx + 8 * nt]);
   }
+}
+
+// Shared memory: the owned block's inverse, two chunk buffers of CH blocks of op(A), and
+// two buffers for the X rows of a chunk.
+template <typename TA>
+constexpr int few_ch() { return sizeof(TA) == 4 ? 3 : 2; }
+template <typename TA>
+constexpr int few_ldc() { return few_ch<TA>() * TB + 4; }
+template <typename TA, int NT>
+constexpr int few_smem() {
+  return TB * LDL * 8 + 2 * TB * few_ldc<TA>() * (int)sizeof(TA) +
+         2 * few_ch<TA>() * TB * (8 * NT + 4) * 8;
 }
 
 template <typename TA, int NT>
 __global__ void __launch_bounds__(FEW_THREADS, 1) trsm_few_kernel(FewArgs p) {
+  constexpr int CH = few_ch<TA>(), LDC = few_ldc<TA>(), LDXS = 8 * NT + 4;
+  constexpr int XPT = CH * TB * 8 * NT / FEW_THREADS;  // X values per thread per chunk
   extern __shared__ double sm[];
-  double *I = sm;                                       // inverse of the owned diagonal block
-  TA *Lb0 = reinterpret_cast<TA *>(sm + TB * LDL);      // op(A) blocks, double-buffered
-  TA *Lb1 = reinterpret_cast<TA *>(sm + 2 * TB * LDL);
-  double *Xs = sm + 3 * TB * LDL;    // X of a step (row-major, ld LDX)
-  __shared__ int s_abort;
+  double *I = sm;                                                   // owned block's inverse
+  TA *const Lc0 = reinterpret_cast<TA *>(sm + TB * LDL);            // op(A) chunks
+  TA *const Lc1 = Lc0 + TB * LDC;
+  double *const Xs0 = reinterpret_cast<double *>(Lc1 + TB * LDC);   // X rows of a chunk
+  double *const Xs1 = Xs0 + CH * TB * LDXS;
+  __shared__ int s_abort, s_ready, s_known;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
   if (threadIdx.x == 0) s_abort = 0;
   __syncthreads();
-  for (int s = blockIdx.x; s < p.nblk; s += gridDim.x) {
+  // column group of this CTA: B columns [gid * gw, gid * gw + nrhs), its own step flags
+  const int gid = blockIdx.x % p.groups, gcta = gridDim.x / p.groups;
+  double *B = p.B + (int64_t)gid * p.gw * p.bcs;
+  const int nrhs = min(p.gw, p.nrhs - gid * p.gw);
+  int *flags = p.flags + (size_t)gid * p.nblk * FLAG_STRIDE;
+  // X rows of steps s0 .. s0 + cnt - 1 (published by other CTAs), read past L1
+  auto x_load = [&](double (&v)[XPT], int s0, int cnt) {
+    const int rows = cnt * TB;
+#pragma unroll
+    for (int u = 0; u < XPT; ++u) {
+      const int e = threadIdx.x + u * FEW_THREADS;
+      const int k = e / (8 * NT), c = e % (8 * NT);
+      const int xr = k < rows ? step_block(p, s0 + k / TB) * TB + k % TB : p.N;
+      v[u] = (xr < p.N && c < nrhs) ? __ldcg(B + xr * p.brs + c * p.bcs) : 0.0;
+    }
+  };
+  auto x_store = [&](const double (&v)[XPT], double *X) {
+#pragma unroll
+    for (int u = 0; u < XPT; ++u) {
+      const int e = threadIdx.x + u * FEW_THREADS;
+      X[(e / (8 * NT)) * LDXS + e % (8 * NT)] = v[u];
+    }
+  };
+  for (int s = blockIdx.x / p.groups; s < p.nblk; s += gcta) {
     const int pb = step_block(p, s);
     stage_inverse(p, I, pb);
-    if (s > 0) stage_block(p, Lb0, pb, step_block(p, 0));
     // B block in accumulator layout: rows 16w+g (+8), columns 8nt+2t (+1)
     double acc[NT][4];
 #pragma unroll
@@ -134,49 +192,67 @@ __global__ void __launch_bounds__(FEW_THREADS, 1) trsm_few_kernel(FewArgs p) {
       for (int q = 0; q < 4; ++q) {
         const int row = pb * TB + 16 * warp + g + 8 * (q >> 1);
         const int col = 8 * nt + 2 * t + (q & 1);
-        acc[nt][q] = (row < p.N && col < p.nrhs) ? p.alpha * p.B[row * p.brs + col * p.bcs] : 0.0;
+        acc[nt][q] = (row < p.N && col < nrhs) ? p.alpha * __ldcg(B + row * p.brs + col * p.bcs)
+                                               : 0.0;
       }
-    for (int s2 = 0; s2 < s; ++s2) {
-      const int qb = step_block(p, s2);
-      cp_async_join();  // op(A) block of s2 (and, the first time, the inverse) have landed
-      __syncthreads();  // ... for every thread; the other buffer is free again
-      if (s2 + 1 < s) stage_block(p, (s2 & 1) ? Lb0 : Lb1, pb, step_block(p, s2 + 1));
-      if (threadIdx.x == 0) {
-        uint32_t it = 0;
-        while (atomicAdd(&p.flags[s2], 0) != p.epoch) {
-          if (++it > MO_SPIN_LIMIT) {
-            set_status(p.status, MO_EDEVTIMEOUT);
-            s_abort = 1;
-            break;
+    // Subtract op(A)[s, s2] X_s2 for every earlier step s2, up to CH steps per round.  Steps
+    // publish their flags in order, so once the newest earlier step (s - 1) is published
+    // every round proceeds without polling, and the X rows of the next round are loaded
+    // into registers while the current round's product runs.
+    if (threadIdx.x == 0)
+      s_known = (s > 0 && flag_load(&flags[(s - 1) * FLAG_STRIDE]) == p.epoch) ? s - 1 : -1;
+    int s2 = 0, cnt = min(CH, s), buf = 0;
+    bool x_ok = false;
+    if (s > 0) stage_chunk(p, Lc0, LDC, pb, 0, cnt);
+    __syncthreads();
+    int known = s_known;
+    while (s2 < s) {
+      int ready = cnt;
+      if (!x_ok) {
+        if (s2 + cnt - 1 > known) {
+          if (threadIdx.x == 0) {
+            uint32_t it = 0;
+            while (flag_load(&flags[s2 * FLAG_STRIDE]) != p.epoch) {
+              if (++it > MO_SPIN_LIMIT) {
+                set_status(p.status, MO_EDEVTIMEOUT);
+                s_abort = 1;
+                break;
+              }
+            }
+            int r = 1;
+            while (r < cnt && flag_load(&flags[(s2 + r) * FLAG_STRIDE]) == p.epoch) ++r;
+            s_ready = r;
+            s_known = flag_load(&flags[(s - 1) * FLAG_STRIDE]) == p.epoch ? s - 1 : s2 + r - 1;
+            __threadfence();
           }
+          __syncthreads();
+          if (s_abort) {
+            cp_async_join();
+            return;
+          }
+          ready = s_ready;
+          known = s_known;
         }
-        __threadfence();
+        double v[XPT];
+        x_load(v, s2, ready);
+        x_store(v, buf ? Xs1 : Xs0);
       }
+      cp_async_join();  // this round's blocks of op(A) (and the inverse) have landed
       __syncthreads();
-      if (s_abort) {
-        cp_async_join();
-        return;
+      const int nxt = s2 + ready, ncnt = min(CH, s - nxt);
+      const bool nx_ok = ncnt > 0 && nxt + ncnt - 1 <= known;
+      double v[XPT];
+      if (ncnt > 0) {
+        stage_chunk(p, buf ? Lc0 : Lc1, LDC, pb, nxt, ncnt);
+        if (nx_ok) x_load(v, nxt, ncnt);
       }
-      // X of step s2 (written by another CTA): L2 reads, 16 in flight per thread
-      for (int e0 = threadIdx.x; e0 < TB * 8 * NT; e0 += 16 * FEW_THREADS) {
-        double v[16];
-#pragma unroll
-        for (int u = 0; u < 16; ++u) {
-          const int e = e0 + u * FEW_THREADS;
-          const int k = e / (8 * NT), c = e % (8 * NT);
-          const int xr = qb * TB + k;
-          v[u] = (e < TB * 8 * NT && xr < p.N && c < p.nrhs)
-                     ? __ldcg(p.B + xr * p.brs + c * p.bcs) : 0.0;
-        }
-#pragma unroll
-        for (int u = 0; u < 16; ++u) {
-          const int e = e0 + u * FEW_THREADS;
-          if (e < TB * 8 * NT) Xs[(e / (8 * NT)) * LDX + e % (8 * NT)] = v[u];
-        }
-      }
+      block_mma<NT>(acc, buf ? Lc1 : Lc0, LDC, buf ? Xs1 : Xs0, LDXS, ready * TB, -1.0);
+      if (nx_ok) x_store(v, buf ? Xs0 : Xs1);
       __syncthreads();
-      block_mma<NT>(acc, (s2 & 1) ? Lb1 : Lb0, Xs, -1.0);
-      __syncthreads();
+      s2 = nxt;
+      cnt = ncnt;
+      buf ^= 1;
+      x_ok = nx_ok;
     }
     // X_s = inv(op(A)_ss) * acc
     cp_async_join();
@@ -184,25 +260,25 @@ __global__ void __launch_bounds__(FEW_THREADS, 1) trsm_few_kernel(FewArgs p) {
     for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
       for (int q = 0; q < 4; ++q)
-        Xs[(16 * warp + g + 8 * (q >> 1)) * LDX + 8 * nt + 2 * t + (q & 1)] = acc[nt][q];
+        Xs0[(16 * warp + g + 8 * (q >> 1)) * LDXS + 8 * nt + 2 * t + (q & 1)] = acc[nt][q];
     __syncthreads();
     double x[NT][4];
 #pragma unroll
     for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
       for (int q = 0; q < 4; ++q) x[nt][q] = 0.0;
-    block_mma<NT>(x, I, Xs, 1.0);
+    block_mma<NT>(x, I, LDL, Xs0, LDXS, TB, 1.0);
 #pragma unroll
     for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const int row = pb * TB + 16 * warp + g + 8 * (q >> 1);
         const int col = 8 * nt + 2 * t + (q & 1);
-        if (row < p.N && col < p.nrhs) p.B[row * p.brs + col * p.bcs] = x[nt][q];
+        if (row < p.N && col < nrhs) B[row * p.brs + col * p.bcs] = x[nt][q];
       }
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) atomicExch(&p.flags[s], p.epoch);
+    if (threadIdx.x == 0) atomicExch(&flags[s * FLAG_STRIDE], p.epoch);
   }
 }
 
@@ -212,16 +288,19 @@ int launch_few(mo_ctx *ctx, FewArgs &p) {
   int dev = 0;
   cudaGetDevice(&dev);
   const void *kern = (const void *)trsm_few_kernel<TA, NT>;
+  constexpr int smem = few_smem<TA, NT>();
   if (!(attr_mask & (1 << (dev & 31)))) {
-    MO_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, FEW_SMEM));
+    MO_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     attr_mask |= 1 << (dev & 31);
   }
   int occ = 0;
-  MO_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, FEW_THREADS, FEW_SMEM));
+  MO_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, FEW_THREADS, smem));
   if (occ < 1) return MO_EINVAL;
-  const int grid = std::min(p.nblk, occ * ctx->sms);
+  // every column group gets the same number of CTAs
+  const int per = std::max(1, std::min(p.nblk, occ * ctx->sms / p.groups));
+  const int grid = per * p.groups;
   void *args[] = {&p};
-  MO_CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(FEW_THREADS), args, FEW_SMEM,
+  MO_CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(FEW_THREADS), args, smem,
                                           ctx->stream));
   return MO_OK;
 }
@@ -264,20 +343,18 @@ int few_run(mo_ctx *ctx, View B, const void *A, bool a32, int64_t lda, int N, in
   p.flags = flag_buf;
   p.epoch = ++ctx->sk_epoch;
   p.status = reinterpret_cast<int *>(ctx->d_status);
-  MO_CUDA_TRY(cudaMemsetAsync(flag_buf, 0, sizeof(int) * p.nblk, ctx->stream));
+  // more than 16 columns: groups of 16 solved side by side by separate CTA sets, so the
+  // per-step work on the dependency chain is that of 16 columns
+  p.gw = nrhs > 16 ? 16 : nrhs;
+  p.groups = (nrhs + p.gw - 1) / p.gw;
+  MO_CUDA_TRY(cudaMemsetAsync(flag_buf, 0, sizeof(int) * p.nblk * p.groups * FLAG_STRIDE,
+                              ctx->stream));
   ProfScope ps;
   prof_begin(ctx, ps, a32 ? MO_PROF_IR : MO_PROF_GEMM);
-  const int nt = (nrhs + 7) / 8;
+  const int nt = (p.gw + 7) / 8;
   int rc;
-  if (a32) {
-    if (nt <= 2) rc = launch_few<float, 2>(ctx, p);
-    else if (nt <= 4) rc = launch_few<float, 4>(ctx, p);
-    else rc = launch_few<float, 8>(ctx, p);
-  } else {
-    if (nt <= 2) rc = launch_few<double, 2>(ctx, p);
-    else if (nt <= 4) rc = launch_few<double, 4>(ctx, p);
-    else rc = launch_few<double, 8>(ctx, p);
-  }
+  if (a32) rc = nt == 1 ? launch_few<float, 1>(ctx, p) : launch_few<float, 2>(ctx, p);
+  else rc = nt == 1 ? launch_few<double, 1>(ctx, p) : launch_few<double, 2>(ctx, p);
   prof_end(ctx, ps, (double)N * N * nrhs,
            (a32 ? 4.0 : 8.0) * (double)N * N / 2 + 8.0 * 2.0 * N * nrhs);
   return rc;
@@ -286,7 +363,7 @@ int few_run(mo_ctx *ctx, View B, const void *A, bool a32, int64_t lda, int N, in
 }  // namespace
 
 // Left solve (right solves via the transposed view of B) with nrhs <= 64.  `inv` receives
-// the 128 x 128 diagonal-block inverses; `flag_buf` holds one int per 64-row block.
+// the 128 x 128 diagonal-block inverses; `flag_buf` holds 4 x 32 ints per 64-row block.
 int trsm_few(mo_ctx *ctx, View B, View A, int flags, double alpha, double *inv, int *flag_buf) {
   const bool right = (flags & MO_RIGHT) != 0;
   const bool upper = (flags & MO_UPPER) != 0;

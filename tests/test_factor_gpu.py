@@ -121,3 +121,18 @@ def test_solve_lu(gpu, oracle, rng, flags, n, nrhs):
     assert fro(X - Br) / fro(Br) <= 1e-9
     if flags == 0:
         assert fro(B - A @ X) / (fro(A) * fro(X) + fro(B)) <= 10 * n * EPS
+
+
+@pytest.mark.parametrize("nrhs", [17, 48, 64])
+def test_solve_chol_grouped_columns(gpu, oracle, rng, nrhs):
+    # more than 16 right-hand sides: the few-column solve runs column groups side by side
+    n = 1100
+    A = colmajor(spd(rng, n))
+    B = colmajor(rng.uniform(-1, 1, (n, nrhs)))
+    Ag, Bg = dev(gpu, A), dev(gpu, B)
+    gpu.DecomposeCHOL(Ag, LO, 64)
+    gpu.SolveCHOL(Bg, Ag, LO)
+    Ar, Br = A.copy(order="F"), B.copy(order="F")
+    oracle.DecomposeCHOL(Ar, LO, 64)
+    oracle.SolveCHOL(Br, Ar, LO)
+    assert fro(Bg.cpu().numpy() - Br) / fro(Br) <= 1e-10

@@ -216,3 +216,24 @@ def test_lp_gemm_lower_leaves_upper(gpu, rng):
     bound = _split_bound(TF32X3, k, A64, A64.T) + 2.0 ** -23 * (np.abs(ref) + np.abs(C0))
     il = np.tril_indices(m)
     assert np.all(np.abs(got[il] - ref[il]) <= bound[il])
+
+
+@pytest.mark.parametrize("flags", [LO, UP])
+@pytest.mark.parametrize("n,nrhs", [(700, 64), (385, 37)])
+def test_mixed_solve_many_rhs(gpu, oracle, rng, flags, n, nrhs):
+    # above 32 right-hand sides the residual runs through the FP64 GEMM engine on a
+    # symmetric copy of A and the triangular solves split the columns into groups of 16
+    A = kappa_matrix(rng, n, 1e4)
+    B = rng.standard_normal((n, nrhs))
+    Afill = A.copy()
+    if flags == LO:
+        Afill[np.triu_indices(n, 1)] = 1e30
+    else:
+        Afill[np.tril_indices(n, -1)] = 1e30
+    Xg = gpu.matrix(n, nrhs)
+    info, err = gpu.SolveCHOLMixed(Xg, gpu.to_device(Afill), gpu.to_device(B), flags, TF32X3)
+    assert err is None and info.converged and not info.fallback, info
+    X = Xg.cpu().numpy()
+    assert berr_inf(A, X, B) <= 1.5e-14
+    Xr = fp64_solution(oracle, A, B)
+    assert fro(X - Xr) / fro(Xr) <= 1e-9
