@@ -7,7 +7,7 @@
 //
 //   Cholesky (lower, right-looking, panel width NB):
 //     diag   : NB x NB block in registers of warp 0 (lane i holds row i), column
-//              Cholesky by shuffles (sqrt, true division); a NaN pivot stops the matrix
+//              Cholesky by shuffles (reciprocal square root); a NaN pivot stops the matrix
 //              with info = column + 1 (the reference panics, chol.go:33-36)
 //     panel  : rows below, one thread per row: x = a * L11^-T by forward substitution
 //     update : A22 -= L21 L21^T on 64 x 64 lower tiles, K = NB, operands staged in
@@ -92,18 +92,20 @@ __device__ __forceinline__ int warp_chol(double (&r)[NB], int lane, double *badv
 #pragma unroll
   for (int k = 0; k < NB; ++k) {
     const double akk = __shfl_sync(0xffffffffu, r[k], k);
-    const double d = sqrt(akk);
-    if (isnan(d)) {  // uniform across the warp
+    const double rs = rsqrt(akk);  // one reciprocal square root on the chain per column
+    if (isnan(rs)) {  // uniform across the warp
       *badv = akk;
       return k;
     }
-    if (lane == k) r[k] = d;
-    if (lane > k) r[k] = r[k] / d;
+    // shuffles and updates use the multiplier lk (zero on lanes <= k): the pivot's square
+    // root is off the chain
+    const double lk = lane > k ? r[k] * rs : 0.0;
 #pragma unroll
     for (int j = k + 1; j < NB; ++j) {
-      const double ljk = __shfl_sync(0xffffffffu, r[k], j);
-      r[j] = fma(-r[k], ljk, r[j]);
+      const double ljk = __shfl_sync(0xffffffffu, lk, j);
+      r[j] = fma(-lk, ljk, r[j]);
     }
+    r[k] = lane == k ? sqrt(akk) : (lane > k ? lk : r[k]);
   }
   return -1;
 }

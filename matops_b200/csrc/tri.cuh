@@ -112,32 +112,40 @@ __device__ __forceinline__ void tri_syrk_update(double *S, int NP, int r0, int k
 }
 
 // Cholesky of a 32 x 32 lower block held by one warp, lane i holding row i in r[0..31]
-// (column-by-column, sqrt and true division as calgo/dvec_util.c:230-246 does).  The
+// (column-by-column; the reference divides by the square root, calgo/dvec_util.c:230-246,
+// here the column is multiplied by the reciprocal square root, equal to rounding).  The
 // rank-1 updates run on every lane without a lane test: a lane only modifies entries
 // right of its diagonal, which are never read, and this keeps the unrolled body free of
 // divergent branches (measured 4.4x faster than guarding each update with lane >= j).
 // With `checked`, the column loop stops at the first NaN pivot and returns its index.
 template <bool checked>
-__device__ __forceinline__ int warp_potrf32(double (&r)[SUB], int lane, double *badv) {
+__device__ __forceinline__ int warp_potrf32(double (&r)[SUB], int lane, double *badv,
+                                            double *col) {
   int bad = -1;
 #pragma unroll
   for (int k = 0; k < SUB; ++k) {
     const double akk = __shfl_sync(0xffffffffu, r[k], k);
-    const double d = sqrt(akk);
+    // the column is scaled by rsqrt(akk) (one reciprocal square root on the dependency
+    // chain instead of a square root followed by a division); the stored pivot is
+    // sqrt(akk), which nothing on the chain waits for
+    const double rs = rsqrt(akk);
     if (checked) {
-      if (isnan(d)) {  // uniform: every lane sees the same akk
+      if (isnan(rs)) {  // uniform: every lane sees the same akk
         bad = k;
         *badv = akk;
         break;
       }
     }
-    if (lane == k) r[k] = d;
-    if (lane > k) r[k] = r[k] / d;
+    // the multipliers (zero on lanes <= k) go through shared memory: every lane reads the
+    // column with broadcast loads that issue back to back, where a chain of shuffles would
+    // pay each shuffle's latency in turn
+    const double lk = lane > k ? r[k] * rs : 0.0;
+    col[lane] = lk;
+    __syncwarp();
 #pragma unroll
-    for (int j = k + 1; j < SUB; ++j) {
-      const double ljk = __shfl_sync(0xffffffffu, r[k], j);
-      r[j] = fma(-r[k], ljk, r[j]);
-    }
+    for (int j = k + 1; j < SUB; ++j) r[j] = fma(-lk, col[j], r[j]);
+    __syncwarp();
+    r[k] = lane == k ? sqrt(akk) : (lane > k ? lk : r[k]);
   }
   return bad;
 }
@@ -154,6 +162,7 @@ __device__ __forceinline__ int warp_potrf32(double (&r)[SUB], int lane, double *
 __device__ inline void tri_potrf_lower(double *S, int NP, int *bad_col, double *bad_val) {
   __shared__ int s_bad;
   __shared__ double s_rd[SUB];
+  __shared__ double s_col[SUB];
   if (threadIdx.x == 0) s_bad = -1;
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -163,7 +172,7 @@ __device__ inline void tri_potrf_lower(double *S, int NP, int *bad_col, double *
 #pragma unroll
       for (int j = 0; j < SUB; ++j) r[j] = (j <= lane) ? S[(jb + lane) * LDS + jb + j] : 0.0;
       double unused;
-      warp_potrf32<false>(r, lane, &unused);
+      warp_potrf32<false>(r, lane, &unused, s_col);
       double dg = r[0];
 #pragma unroll
       for (int j = 1; j < SUB; ++j) dg = (j == lane) ? r[j] : dg;
@@ -172,7 +181,7 @@ __device__ inline void tri_potrf_lower(double *S, int NP, int *bad_col, double *
 #pragma unroll
         for (int j = 0; j < SUB; ++j) r[j] = (j <= lane) ? S[(jb + lane) * LDS + jb + j] : 0.0;
         double badv = 0.0;
-        const int bad = warp_potrf32<true>(r, lane, &badv);
+        const int bad = warp_potrf32<true>(r, lane, &badv, s_col);
         if (lane == 0) {
           s_bad = jb + bad;
           *bad_val = badv;

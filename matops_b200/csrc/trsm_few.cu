@@ -1,18 +1,19 @@
 // Triangular solve with few right-hand sides (<= 64) in one cooperative launch.
 //
 // op(A) X = alpha*B with op(A) n x n triangular, split into 64-row blocks.  The columns of
-// B are cut into groups of at most 16, each solved by its own set of CTAs with its own
-// step flags, so the work on the dependency chain per step is that of 16 columns.  Within
-// a set, CTA c owns the blocks of steps c, c+P, ... (top-down for a lower op(A), bottom-up
-// for upper).  For each owned step s it keeps its block of B in DMMA accumulator fragments
-// and subtracts op(A)[s, s'] X_s' for the earlier steps s' in rounds: it waits for the
-// oldest missing step's flag, takes every consecutive published step up to a chunk of
-// (FP32 op(A): 3, FP64: 2) blocks, and applies them as one K = 64 x chunk product, while
-// the next chunk of op(A) streams in by cp.async (and, once every earlier step is known
-// published, the next chunk's X rows stream into registers).  Then X_s = inv(op(A)_ss) (B_s - ...) is
-// published (written over B) with its flag.  The critical path per step is one 64 x 64 x 16
-// update plus one 64 x 64 x 16 product on the FP64 tensor pipe (mma.sync m16n8k4).  Blocks of
-// op(A) are staged with coalesced reads (also for op(A) = A^T).  Every wait is bounded and
+// B are cut into groups of at most MO_FEW_GROUP (32), each solved by its own set of CTAs
+// with its own step flags, so the work on the dependency chain per step is that of one
+// group.  Within a set, CTA c owns the blocks of steps c, c+P, ... (top-down for a lower
+// op(A), bottom-up for upper).  For each owned step s it keeps its block of B in DMMA
+// accumulator fragments and subtracts op(A)[s, s'] X_s' for the earlier steps s' in
+// rounds: it waits for the oldest missing step's flag, takes every consecutive published
+// step up to a chunk of 1-3 blocks (as deep as shared memory allows), and applies them as
+// one K = 64 x chunk product while the next chunk of op(A) streams in by cp.async (and,
+// once every earlier step is known published, the next chunk's X rows stream into
+// registers).  Then X_s = inv(op(A)_ss) (B_s - ...) is published (written over B) with
+// its flag.  The critical path per step is one 64 x 64 x group update plus one
+// 64 x 64 x group product on the FP64 tensor pipe (mma.sync m16n8k4).  Blocks of op(A)
+// are staged with coalesced reads (also for op(A) = A^T).  Every wait is bounded and
 // reports MO_EDEVTIMEOUT.
 //
 // B is addressed with a row and a column stride, so a right-side solve with few rows,
@@ -30,6 +31,9 @@ constexpr int TB = 64;    // block order of the sweep
 constexpr int IB = 128;   // order of the precomputed inverse blocks (trtri_blocks)
 constexpr int FEW_THREADS = 128;  // 4 warps x 16 rows
 constexpr int MAX_RHS = 64;
+#ifndef MO_FEW_GROUP
+#define MO_FEW_GROUP 32  // columns per group (measured: 32 beats 16 and 64 at n = 16384, 64 RHS)
+#endif
 constexpr int LDL = TB + 4;   // smem row stride (== 4 mod 16 doubles: 2-way at most)
 
 struct FewArgs {
@@ -133,19 +137,23 @@ __device__ __forceinline__ void block_mma(double (&acc)[NT][4], const TM *M, int
 
 // Shared memory: the owned block's inverse, two chunk buffers of CH blocks of op(A), and
 // two buffers for the X rows of a chunk.
-template <typename TA>
-constexpr int few_ch() { return sizeof(TA) == 4 ? 3 : 2; }
-template <typename TA>
-constexpr int few_ldc() { return few_ch<TA>() * TB + 4; }
 template <typename TA, int NT>
-constexpr int few_smem() {
-  return TB * LDL * 8 + 2 * TB * few_ldc<TA>() * (int)sizeof(TA) +
-         2 * few_ch<TA>() * TB * (8 * NT + 4) * 8;
+constexpr int few_smem_ch(int ch) {
+  return TB * LDL * 8 + 2 * TB * (ch * TB + 4) * (int)sizeof(TA) + 2 * ch * TB * (8 * NT + 4) * 8;
 }
+// the deepest chunk (up to 3 blocks) that fits in 225 KB of shared memory
+template <typename TA, int NT>
+constexpr int few_ch() {
+  return few_smem_ch<TA, NT>(3) <= 225 * 1024 ? 3 : (few_smem_ch<TA, NT>(2) <= 225 * 1024 ? 2 : 1);
+}
+template <typename TA, int NT>
+constexpr int few_ldc() { return few_ch<TA, NT>() * TB + 4; }
+template <typename TA, int NT>
+constexpr int few_smem() { return few_smem_ch<TA, NT>(few_ch<TA, NT>()); }
 
 template <typename TA, int NT>
 __global__ void __launch_bounds__(FEW_THREADS, 1) trsm_few_kernel(FewArgs p) {
-  constexpr int CH = few_ch<TA>(), LDC = few_ldc<TA>(), LDXS = 8 * NT + 4;
+  constexpr int CH = few_ch<TA, NT>(), LDC = few_ldc<TA, NT>(), LDXS = 8 * NT + 4;
   constexpr int XPT = CH * TB * 8 * NT / FEW_THREADS;  // X values per thread per chunk
   extern __shared__ double sm[];
   double *I = sm;                                                   // owned block's inverse
@@ -343,9 +351,9 @@ int few_run(mo_ctx *ctx, View B, const void *A, bool a32, int64_t lda, int N, in
   p.flags = flag_buf;
   p.epoch = ++ctx->sk_epoch;
   p.status = reinterpret_cast<int *>(ctx->d_status);
-  // more than 16 columns: groups of 16 solved side by side by separate CTA sets, so the
-  // per-step work on the dependency chain is that of 16 columns
-  p.gw = nrhs > 16 ? 16 : nrhs;
+  // more than MO_FEW_GROUP columns: groups solved side by side by separate CTA sets, so
+  // the per-step work on the dependency chain is that of one group
+  p.gw = nrhs > MO_FEW_GROUP ? MO_FEW_GROUP : nrhs;
   p.groups = (nrhs + p.gw - 1) / p.gw;
   MO_CUDA_TRY(cudaMemsetAsync(flag_buf, 0, sizeof(int) * p.nblk * p.groups * FLAG_STRIDE,
                               ctx->stream));
@@ -353,8 +361,17 @@ int few_run(mo_ctx *ctx, View B, const void *A, bool a32, int64_t lda, int N, in
   prof_begin(ctx, ps, a32 ? MO_PROF_IR : MO_PROF_GEMM);
   const int nt = (p.gw + 7) / 8;
   int rc;
-  if (a32) rc = nt == 1 ? launch_few<float, 1>(ctx, p) : launch_few<float, 2>(ctx, p);
-  else rc = nt == 1 ? launch_few<double, 1>(ctx, p) : launch_few<double, 2>(ctx, p);
+  if (a32) {
+    if (nt == 1) rc = launch_few<float, 1>(ctx, p);
+    else if (nt == 2) rc = launch_few<float, 2>(ctx, p);
+    else if (nt <= 4) rc = launch_few<float, 4>(ctx, p);
+    else rc = launch_few<float, 8>(ctx, p);
+  } else {
+    if (nt == 1) rc = launch_few<double, 1>(ctx, p);
+    else if (nt == 2) rc = launch_few<double, 2>(ctx, p);
+    else if (nt <= 4) rc = launch_few<double, 4>(ctx, p);
+    else rc = launch_few<double, 8>(ctx, p);
+  }
   prof_end(ctx, ps, (double)N * N * nrhs,
            (a32 ? 4.0 : 8.0) * (double)N * N / 2 + 8.0 * 2.0 * N * nrhs);
   return rc;
