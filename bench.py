@@ -702,13 +702,15 @@ def main():
     bf16_peak = _measured_peak("bf16_tflops", 1590.0)
     achieved_gbs = l_by / (l_ms * 1e-3) / 1e9 if l_ms else 0.0
     achieved_tf = l_fl / (l_ms * 1e-3) / 1e12 if l_ms else 0.0
+    # DRAM traffic per launch: the measured traffic / algorithmic-bytes ratio of the ncu
+    # capture summarized in profiles/lp_gemm_tc_kernel_traffic.md, times this run's
+    # algorithmic bytes per launch
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "lp_gemm_tc_traffic.json")
-    if os.path.exists(tpath):
-        try:
-            traffic = json.load(open(tpath)).get("bytes_per_launch")
-        except Exception:
-            traffic = None
+    tpath = os.path.join(ROOT, "profiles", "lp_gemm_tc_kernel_traffic.md")
+    if os.path.exists(tpath) and l_n:
+        for ln in open(tpath):
+            if ln.startswith("traffic_over_algorithmic:"):
+                traffic = float(ln.split(":")[1]) * l_by / l_n
     roofline = {
         "bound": "hbm", "kernel": "lp_gemm_tc_kernel (TF32x3 trailing updates and panels)",
         "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
