@@ -502,6 +502,28 @@ def run_reference(args, rank):
 
 
 # --------------------------------------------------------------------------------------
+# replicas: one independent system per rank, no collective in the data path; the ranks
+# only meet at barriers and for the max over ranks of the device time
+# --------------------------------------------------------------------------------------
+
+def rank_barrier(world: int) -> None:
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def rank_max(x: float, world: int, device) -> float:
+    """Max over ranks of a per-rank time (the slowest replica sets the job's time)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# --------------------------------------------------------------------------------------
 # clocks during the timed region (NVML, read-only)
 # --------------------------------------------------------------------------------------
 
@@ -589,15 +611,10 @@ def main():
                                 device_id=dev)
 
     def barrier():
-        if world > 1:
-            dist.barrier()
+        rank_barrier(world)
 
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return rank_max(x, world, dev)
 
     n, nrhs, K, W = args.n, args.nrhs, args.steps, args.warmup
     fp64_peak = mo.MeasureFP64Peak(300.0)
