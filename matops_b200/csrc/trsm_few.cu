@@ -50,6 +50,7 @@ struct FewArgs {
   int gw;
   const double *inv;  // 128 x 128 inverses of op(A)'s diagonal blocks (ld 128)
   bool inv_t;         // inv holds the inverses of A's blocks: read them transposed
+  bool vec;           // A's base and leading dimension allow 16-byte copies
   int *flags;         // [groups * nblk]
   int epoch;
   int *status;
@@ -81,25 +82,48 @@ __device__ __forceinline__ void cp_async_el(float *dst, const float *src, uint32
                : "memory");
 }
 
-// issue cp.async copies of `cnt` blocks of op(A) -- block row rb, the block columns of
-// steps s0 .. s0 + cnt - 1 -- into the chunk buffer L (row-major, ld ldl, block j at
-// column j * 64); zero past N
+// Blocks of op(A) sit in the chunk buffer in the orientation of their source, so that
+// 16-byte copies fill them: for op(A) = A (column-major A, contiguous along op(A)'s rows)
+// block element (i, k) is at [k * ldb + i]; for op(A) = A^T at [i * ldb + k].  ldb keeps
+// the DMMA fragment reads free of bank conflicts (few_block_ld).
 template <typename TA>
-__device__ __forceinline__ void stage_chunk(const FewArgs &p, TA *L, int ldl, int rb, int s0,
-                                            int cnt) {
+__host__ __device__ constexpr int few_block_ld(bool trans) {
+  return sizeof(TA) == 4 ? (trans ? 68 : 72) : 68;
+}
+
+__device__ __forceinline__ void cp_async_16(void *dst, const void *src, uint32_t bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src),
+               "r"(bytes)
+               : "memory");
+}
+
+// issue cp.async copies of `cnt` blocks of op(A) -- block row rb, the block columns of
+// steps s0 .. s0 + cnt - 1 -- into the chunk buffer L (block j at j * 64 * ldb); zero past N
+template <typename TA>
+__device__ __forceinline__ void stage_chunk(const FewArgs &p, TA *L, int rb, int s0, int cnt) {
+  constexpr int V = 16 / sizeof(TA);  // elements per 16-byte copy
+  const int ldb = few_block_ld<TA>(p.trans);
   const int r0 = rb * TB;
   const TA *A = static_cast<const TA *>(p.A);
   for (int j = 0; j < cnt; ++j) {
     const int c0 = step_block(p, s0 + j) * TB;
-    TA *Lj = L + j * TB;
-    for (int e = threadIdx.x; e < TB * TB; e += blockDim.x) {
-      const int i = e % TB, k = e / TB;  // consecutive threads -> consecutive A addresses
-      if (!p.trans) {
-        const bool ok = r0 + i < p.N && c0 + k < p.N;
-        cp_async_el(Lj + i * ldl + k, ok ? A + (r0 + i) + (int64_t)(c0 + k) * p.lda : A, ok);
-      } else {
-        const bool ok = c0 + i < p.N && r0 + k < p.N;
-        cp_async_el(Lj + k * ldl + i, ok ? A + (c0 + i) + (int64_t)(r0 + k) * p.lda : A, ok);
+    TA *Lj = L + (size_t)j * TB * ldb;
+    if (p.vec) {
+      // chunk e: V consecutive source elements along the contiguous direction
+      for (int e = threadIdx.x; e < TB * TB / V; e += blockDim.x) {
+        const int u = (e % (TB / V)) * V, w = e / (TB / V);  // contiguous index, other index
+        // non-trans: rows r0 + u.. of column c0 + w; trans: rows c0 + u.. of column r0 + w
+        const int cr = p.trans ? c0 + u : r0 + u, cc = p.trans ? r0 + w : c0 + w;
+        const int nv = (cc < p.N) ? max(0, min(V, p.N - cr)) : 0;
+        const TA *src = nv ? A + cr + (int64_t)cc * p.lda : A;
+        cp_async_16(Lj + w * ldb + u, src, (uint32_t)(nv * sizeof(TA)));
+      }
+    } else {
+      for (int e = threadIdx.x; e < TB * TB; e += blockDim.x) {
+        const int u = e % TB, w = e / TB;
+        const int cr = p.trans ? c0 + u : r0 + u, cc = p.trans ? r0 + w : c0 + w;
+        const bool ok = cr < p.N && cc < p.N;
+        cp_async_el(Lj + w * ldb + u, ok ? A + cr + (int64_t)cc * p.lda : A, ok);
       }
     }
   }
@@ -118,28 +142,34 @@ __device__ __forceinline__ void stage_inverse(const FewArgs &p, double *I, int r
   }
 }
 
-// acc[nt] (+)= sign * M(16 rows of this warp, K) * X(K, 8 nt ..)
+// acc[nt] (+)= sign * M(16 rows of this warp, nb blocks of 64 columns) * X(64 nb, 8 nt ..)
+// M element (row, col) of block j at M[j * mbs + row * rs + col * cs]; X element (k, c) at
+// X[c * ldx + k] (column-major).
 template <int NT, typename TM>
-__device__ __forceinline__ void block_mma(double (&acc)[NT][4], const TM *M, int ldm,
-                                          const double *X, int ldx, int K, double sign) {
+__device__ __forceinline__ void block_mma(double (&acc)[NT][4], const TM *M, int rs, int cs,
+                                          int mbs, int nb, const double *X, int ldx,
+                                          double sign) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
-  const TM *m0 = M + (16 * warp + g) * ldm + t;
-  const TM *m1 = m0 + 8 * ldm;
-  const double *xb = X + t * ldx + g;
+  for (int j = 0; j < nb; ++j) {
+    const TM *m0 = M + (size_t)j * mbs + (16 * warp + g) * rs + t * cs;
+    const TM *m1 = m0 + 8 * rs;
+    const double *xb = X + g * ldx + j * TB + t;
 #pragma unroll 4
-  for (int k = 0; k < K; k += 4) {
-    const double a0 = sign * (double)m0[k], a1 = sign * (double)m1[k];
+    for (int k = 0; k < TB; k += 4) {
+      const double a0 = sign * (double)m0[k * cs], a1 = sign * (double)m1[k * cs];
 #pragma unroll
-    for (int nt = 0; nt < NT; ++nt) dmma_16x8x4(acc[nt], a0, a1, xb[k * ldx + 8 * nt]);
+      for (int nt = 0; nt < NT; ++nt) dmma_16x8x4(acc[nt], a0, a1, xb[8 * nt * ldx + k]);
+    }
   }
 }
 
 // Shared memory: the owned block's inverse, two chunk buffers of CH blocks of op(A), and
-// two buffers for the X rows of a chunk.
+// two buffers for the X rows of a chunk (column-major, ld CH * 64 + 4).
 template <typename TA, int NT>
 constexpr int few_smem_ch(int ch) {
-  return TB * LDL * 8 + 2 * TB * (ch * TB + 4) * (int)sizeof(TA) + 2 * ch * TB * (8 * NT + 4) * 8;
+  return TB * LDL * 8 + 2 * ch * TB * few_block_ld<TA>(false) * (int)sizeof(TA) +
+         2 * 8 * NT * (ch * TB + 4) * 8;
 }
 // the deepest chunk (up to 3 blocks) that fits in 225 KB of shared memory
 template <typename TA, int NT>
@@ -147,20 +177,22 @@ constexpr int few_ch() {
   return few_smem_ch<TA, NT>(3) <= 225 * 1024 ? 3 : (few_smem_ch<TA, NT>(2) <= 225 * 1024 ? 2 : 1);
 }
 template <typename TA, int NT>
-constexpr int few_ldc() { return few_ch<TA, NT>() * TB + 4; }
-template <typename TA, int NT>
 constexpr int few_smem() { return few_smem_ch<TA, NT>(few_ch<TA, NT>()); }
 
 template <typename TA, int NT>
 __global__ void __launch_bounds__(FEW_THREADS, 1) trsm_few_kernel(FewArgs p) {
-  constexpr int CH = few_ch<TA, NT>(), LDC = few_ldc<TA, NT>(), LDXS = 8 * NT + 4;
+  constexpr int CH = few_ch<TA, NT>(), LDXK = CH * TB + 4;  // X chunk: column-major, ld LDXK
+  constexpr int CBLK = TB * few_block_ld<TA>(false);        // chunk buffer elements per block
   constexpr int XPT = CH * TB * 8 * NT / FEW_THREADS;  // X values per thread per chunk
   extern __shared__ double sm[];
   double *I = sm;                                                   // owned block's inverse
   TA *const Lc0 = reinterpret_cast<TA *>(sm + TB * LDL);            // op(A) chunks
-  TA *const Lc1 = Lc0 + TB * LDC;
-  double *const Xs0 = reinterpret_cast<double *>(Lc1 + TB * LDC);   // X rows of a chunk
-  double *const Xs1 = Xs0 + CH * TB * LDXS;
+  TA *const Lc1 = Lc0 + CH * CBLK;
+  double *const Xs0 = reinterpret_cast<double *>(Lc1 + CH * CBLK);  // X rows of a chunk
+  double *const Xs1 = Xs0 + 8 * NT * LDXK;
+  // orientation of the op(A) blocks in the chunk buffers (see stage_chunk)
+  const int lb = few_block_ld<TA>(p.trans);
+  const int mrs = p.trans ? lb : 1, mcs = p.trans ? 1 : lb, mbs = TB * lb;
   __shared__ int s_abort, s_ready, s_known;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
@@ -177,7 +209,7 @@ __global__ void __launch_bounds__(FEW_THREADS, 1) trsm_few_kernel(FewArgs p) {
 #pragma unroll
     for (int u = 0; u < XPT; ++u) {
       const int e = threadIdx.x + u * FEW_THREADS;
-      const int k = e / (8 * NT), c = e % (8 * NT);
+      const int k = e % (CH * TB), c = e / (CH * TB);  // coalesced down each column of B
       const int xr = k < rows ? step_block(p, s0 + k / TB) * TB + k % TB : p.N;
       v[u] = (xr < p.N && c < nrhs) ? __ldcg(B + xr * p.brs + c * p.bcs) : 0.0;
     }
@@ -186,7 +218,7 @@ __global__ void __launch_bounds__(FEW_THREADS, 1) trsm_few_kernel(FewArgs p) {
 #pragma unroll
     for (int u = 0; u < XPT; ++u) {
       const int e = threadIdx.x + u * FEW_THREADS;
-      X[(e / (8 * NT)) * LDXS + e % (8 * NT)] = v[u];
+      X[(e / (CH * TB)) * LDXK + e % (CH * TB)] = v[u];
     }
   };
   for (int s = blockIdx.x / p.groups; s < p.nblk; s += gcta) {
@@ -211,7 +243,7 @@ __global__ void __launch_bounds__(FEW_THREADS, 1) trsm_few_kernel(FewArgs p) {
       s_known = (s > 0 && flag_load(&flags[(s - 1) * FLAG_STRIDE]) == p.epoch) ? s - 1 : -1;
     int s2 = 0, cnt = min(CH, s), buf = 0;
     bool x_ok = false;
-    if (s > 0) stage_chunk(p, Lc0, LDC, pb, 0, cnt);
+    if (s > 0) stage_chunk(p, Lc0, pb, 0, cnt);
     __syncthreads();
     int known = s_known;
     while (s2 < s) {
@@ -251,10 +283,10 @@ __global__ void __launch_bounds__(FEW_THREADS, 1) trsm_few_kernel(FewArgs p) {
       const bool nx_ok = ncnt > 0 && nxt + ncnt - 1 <= known;
       double v[XPT];
       if (ncnt > 0) {
-        stage_chunk(p, buf ? Lc0 : Lc1, LDC, pb, nxt, ncnt);
+        stage_chunk(p, buf ? Lc0 : Lc1, pb, nxt, ncnt);
         if (nx_ok) x_load(v, nxt, ncnt);
       }
-      block_mma<NT>(acc, buf ? Lc1 : Lc0, LDC, buf ? Xs1 : Xs0, LDXS, ready * TB, -1.0);
+      block_mma<NT>(acc, buf ? Lc1 : Lc0, mrs, mcs, mbs, ready, buf ? Xs1 : Xs0, LDXK, -1.0);
       if (nx_ok) x_store(v, buf ? Xs0 : Xs1);
       __syncthreads();
       s2 = nxt;
@@ -268,14 +300,14 @@ __global__ void __launch_bounds__(FEW_THREADS, 1) trsm_few_kernel(FewArgs p) {
     for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
       for (int q = 0; q < 4; ++q)
-        Xs0[(16 * warp + g + 8 * (q >> 1)) * LDXS + 8 * nt + 2 * t + (q & 1)] = acc[nt][q];
+        Xs0[(8 * nt + 2 * t + (q & 1)) * LDXK + 16 * warp + g + 8 * (q >> 1)] = acc[nt][q];
     __syncthreads();
     double x[NT][4];
 #pragma unroll
     for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
       for (int q = 0; q < 4; ++q) x[nt][q] = 0.0;
-    block_mma<NT>(x, I, LDL, Xs0, LDXS, TB, 1.0);
+    block_mma<NT>(x, I, LDL, 1, 0, 1, Xs0, LDXK, 1.0);
 #pragma unroll
     for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
@@ -339,6 +371,7 @@ int few_run(mo_ctx *ctx, View B, const void *A, bool a32, int64_t lda, int N, in
   }
   p.A = A;
   p.lda = lda;
+  p.vec = ((uintptr_t)A % 16 == 0) && ((lda * (a32 ? 4 : 8)) % 16 == 0);
   p.trans = tr;
   p.lower_eff = lower_eff;
   p.N = N;
