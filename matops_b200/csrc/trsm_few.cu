@@ -148,8 +148,9 @@ __device__ __forceinline__ void stage_inverse(const FewArgs &p, double *I, int r
 template <int NT, typename TM>
 __device__ __forceinline__ void block_mma(double (&acc)[NT][4], const TM *M, int rs, int cs,
                                           int mbs, int nb, const double *X, int ldx,
-                                          double sign) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+                                          double sign, int warp = -1) {
+  if (warp < 0) warp = threadIdx.x >> 5;  // the 16-row group of the 64-row block
+  const int lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
   for (int j = 0; j < nb; ++j) {
     const TM *m0 = M + (size_t)j * mbs + (16 * warp + g) * rs + t * cs;
@@ -349,6 +350,225 @@ int launch_few(mo_ctx *ctx, FewArgs &p) {
 
 namespace {
 
+// ---------------------------------------------------------------------------------------
+// Pairs of consecutive steps per CTA (FP32 op(A), the mixed-precision preconditioner).
+// 8 warps: warps 0-3 hold step 2q's block, warps 4-7 step 2q + 1's.  The rounds over the
+// earlier steps stage both block rows of a block column (one column per round) and share
+// its X rows; then X_2q = inv * (B - ...) is published and, inside the CTA, step 2q + 1
+// subtracts op(A)[2q + 1, 2q] X_2q straight from shared memory: every other hand-off on
+// the dependency chain skips the flag, the L2 round trip and the fence.
+// ---------------------------------------------------------------------------------------
+constexpr int PAIR_THREADS = 256;
+constexpr int PAIR_CBLK = TB * 72;  // floats per staged 64 x 64 block (largest orientation ld)
+
+template <int NT>
+constexpr int pair_smem() {
+  // two inverses | op(A)[2q + 1, 2q] | two chunk buffers of two blocks | two X buffers
+  return 2 * TB * LDL * 8 + PAIR_CBLK * 4 + 2 * 2 * PAIR_CBLK * 4 + 2 * 8 * NT * (TB + 4) * 8;
+}
+
+template <int NT>
+__global__ void __launch_bounds__(PAIR_THREADS, 1) trsm_pair_kernel(FewArgs p) {
+  constexpr int LDXK = TB + 4;                        // X buffers: column-major 64 x 8NT
+  constexpr int XPT = TB * 8 * NT / PAIR_THREADS;    // X values per thread per block
+  extern __shared__ double sm[];
+  double *const I0 = sm, *const I1 = sm + TB * LDL;
+  float *const Ad = reinterpret_cast<float *>(sm + 2 * TB * LDL);
+  float *const Lc0 = Ad + PAIR_CBLK;                  // block (pb0, col), then (pb1, col)
+  float *const Lc1 = Lc0 + 2 * PAIR_CBLK;
+  double *const Xs0 = reinterpret_cast<double *>(Lc1 + 2 * PAIR_CBLK);
+  double *const Xs1 = Xs0 + 8 * NT * LDXK;
+  __shared__ int s_abort, s_known;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int half = warp >> 2, wr = warp & 3;
+  const int g = lane >> 2, t = lane & 3;
+  if (threadIdx.x == 0) s_abort = 0;
+  __syncthreads();
+  const int gid = blockIdx.x % p.groups, gcta = gridDim.x / p.groups;
+  double *B = p.B + (int64_t)gid * p.gw * p.bcs;
+  const int nrhs = min(p.gw, p.nrhs - gid * p.gw);
+  int *flags = p.flags + (size_t)gid * p.nblk * FLAG_STRIDE;
+  const int lb = few_block_ld<float>(p.trans);
+  const int mrs = p.trans ? lb : 1, mcs = p.trans ? 1 : lb;
+  auto x_load = [&](double (&v)[XPT], int s0) {  // X rows of step s0, read past L1
+#pragma unroll
+    for (int u = 0; u < XPT; ++u) {
+      const int e = threadIdx.x + u * PAIR_THREADS;
+      const int k = e % TB, c = e / TB;
+      const int xr = step_block(p, s0) * TB + k;
+      v[u] = (xr < p.N && c < nrhs) ? __ldcg(B + xr * p.brs + c * p.bcs) : 0.0;
+    }
+  };
+  auto x_store = [&](const double (&v)[XPT], double *X) {
+#pragma unroll
+    for (int u = 0; u < XPT; ++u) {
+      const int e = threadIdx.x + u * PAIR_THREADS;
+      X[(e / TB) * LDXK + e % TB] = v[u];
+    }
+  };
+  auto stage_pair = [&](float *L, int pb0, int pb1, bool has1, int col_step) {
+    stage_chunk(p, L, pb0, col_step, 1);
+    if (has1) stage_chunk(p, L + PAIR_CBLK, pb1, col_step, 1);
+  };
+  const int npair = (p.nblk + 1) / 2;
+  for (int q = blockIdx.x / p.groups; q < npair; q += gcta) {
+    const int s0 = 2 * q, s1 = 2 * q + 1;
+    const bool has1 = s1 < p.nblk;
+    const int pb0 = step_block(p, s0), pb1 = has1 ? step_block(p, s1) : pb0;
+    stage_inverse(p, I0, pb0);
+    if (has1) {
+      stage_inverse(p, I1, pb1);
+      stage_chunk(p, Ad, pb1, s0, 1);  // op(A)[step 2q + 1, step 2q]
+    }
+    const int pbh = half ? pb1 : pb0;
+    const bool live = half == 0 || has1;
+    double acc[NT][4];
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int row = pbh * TB + 16 * wr + g + 8 * (r >> 1);
+        const int col = 8 * nt + 2 * t + (r & 1);
+        acc[nt][r] = (live && row < p.N && col < nrhs)
+                         ? p.alpha * __ldcg(B + row * p.brs + col * p.bcs) : 0.0;
+      }
+    // subtract op(A)[step, s2] X_s2 for every earlier step s2, one block column per round
+    if (threadIdx.x == 0)
+      s_known = (s0 > 0 && flag_load(&flags[(s0 - 1) * FLAG_STRIDE]) == p.epoch) ? s0 - 1 : -1;
+    int s2 = 0, buf = 0;
+    bool x_ok = false;
+    if (s0 > 0) stage_pair(Lc0, pb0, pb1, has1, 0);
+    __syncthreads();
+    int known = s_known;
+    while (s2 < s0) {
+      if (!x_ok) {
+        if (s2 > known) {
+          if (threadIdx.x == 0) {
+            uint32_t it = 0;
+            while (flag_load(&flags[s2 * FLAG_STRIDE]) != p.epoch) {
+              if (++it > MO_SPIN_LIMIT) {
+                set_status(p.status, MO_EDEVTIMEOUT);
+                s_abort = 1;
+                break;
+              }
+            }
+            s_known = flag_load(&flags[(s0 - 1) * FLAG_STRIDE]) == p.epoch ? s0 - 1 : s2;
+            __threadfence();
+          }
+          __syncthreads();
+          if (s_abort) {
+            cp_async_join();
+            return;
+          }
+          known = s_known;
+        }
+        double v[XPT];
+        x_load(v, s2);
+        x_store(v, buf ? Xs1 : Xs0);
+      }
+      cp_async_join();
+      __syncthreads();
+      const int nxt = s2 + 1;
+      const bool nx_ok = nxt < s0 && nxt <= known;
+      double v[XPT];
+      if (nxt < s0) {
+        stage_pair(buf ? Lc0 : Lc1, pb0, pb1, has1, nxt);
+        if (nx_ok) x_load(v, nxt);
+      }
+      if (live)
+        block_mma<NT>(acc, (buf ? Lc1 : Lc0) + half * PAIR_CBLK, mrs, mcs, 0, 1,
+                      buf ? Xs1 : Xs0, LDXK, -1.0, wr);
+      if (nx_ok) x_store(v, buf ? Xs0 : Xs1);
+      __syncthreads();
+      s2 = nxt;
+      buf ^= 1;
+      x_ok = nx_ok;
+    }
+    cp_async_join();  // the inverses and op(A)[2q + 1, 2q]
+    // step 2q: X_2q = inv(op(A)_2q) * acc (warps 0-3), kept in Xs1 for step 2q + 1
+    if (half == 0) {
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+          Xs0[(8 * nt + 2 * t + (r & 1)) * LDXK + 16 * wr + g + 8 * (r >> 1)] = acc[nt][r];
+    }
+    __syncthreads();
+    if (half == 0) {
+      double x[NT][4];
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) x[nt][r] = 0.0;
+      block_mma<NT>(x, I0, LDL, 1, 0, 1, Xs0, LDXK, 1.0, wr);
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int rr = 16 * wr + g + 8 * (r >> 1), col = 8 * nt + 2 * t + (r & 1);
+          Xs1[col * LDXK + rr] = x[nt][r];
+          if (pb0 * TB + rr < p.N && col < nrhs) B[(pb0 * TB + rr) * p.brs + col * p.bcs] = x[nt][r];
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) atomicExch(&flags[s0 * FLAG_STRIDE], p.epoch);
+    if (has1) {
+      // step 2q + 1 (warps 4-7): acc -= op(A)[2q + 1, 2q] X_2q, then X = inv * acc
+      if (half == 1) {
+        block_mma<NT>(acc, Ad, mrs, mcs, 0, 1, Xs1, LDXK, -1.0, wr);
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+            Xs0[(8 * nt + 2 * t + (r & 1)) * LDXK + 16 * wr + g + 8 * (r >> 1)] = acc[nt][r];
+      }
+      __syncthreads();
+      if (half == 1) {
+        double x[NT][4];
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+          for (int r = 0; r < 4; ++r) x[nt][r] = 0.0;
+        block_mma<NT>(x, I1, LDL, 1, 0, 1, Xs0, LDXK, 1.0, wr);
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const int rr = 16 * wr + g + 8 * (r >> 1), col = 8 * nt + 2 * t + (r & 1);
+            if (pb1 * TB + rr < p.N && col < nrhs) B[(pb1 * TB + rr) * p.brs + col * p.bcs] = x[nt][r];
+          }
+      }
+      __threadfence();
+      __syncthreads();
+      if (threadIdx.x == 0) atomicExch(&flags[s1 * FLAG_STRIDE], p.epoch);
+    }
+  }
+}
+
+template <int NT>
+int launch_pair(mo_ctx *ctx, FewArgs &p) {
+  static int attr_mask = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const void *kern = (const void *)trsm_pair_kernel<NT>;
+  constexpr int smem = pair_smem<NT>();
+  if (!(attr_mask & (1 << (dev & 31)))) {
+    MO_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr_mask |= 1 << (dev & 31);
+  }
+  int occ = 0;
+  MO_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, PAIR_THREADS, smem));
+  if (occ < 1) return MO_EINVAL;
+  const int npair = (p.nblk + 1) / 2;
+  const int per = std::max(1, std::min(npair, occ * ctx->sms / p.groups));
+  const int grid = per * p.groups;
+  void *args[] = {&p};
+  MO_CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(PAIR_THREADS), args, smem,
+                                          ctx->stream));
+  return MO_OK;
+}
+
 // flags -> (B strides, effective transposition and sweep direction) and the launch
 int few_run(mo_ctx *ctx, View B, const void *A, bool a32, int64_t lda, int N, int flags,
             double alpha, const double *inv, bool inv_t, int *flag_buf) {
@@ -394,7 +614,12 @@ int few_run(mo_ctx *ctx, View B, const void *A, bool a32, int64_t lda, int N, in
   prof_begin(ctx, ps, a32 ? MO_PROF_IR : MO_PROF_GEMM);
   const int nt = (p.gw + 7) / 8;
   int rc;
-  if (a32) {
+  if (a32 && p.nblk >= 4) {
+    // FP32 factor (the preconditioner of the mixed-precision solve): pairs of steps per CTA
+    if (nt == 1) rc = launch_pair<1>(ctx, p);
+    else if (nt == 2) rc = launch_pair<2>(ctx, p);
+    else rc = launch_pair<4>(ctx, p);
+  } else if (a32) {
     if (nt == 1) rc = launch_few<float, 1>(ctx, p);
     else if (nt == 2) rc = launch_few<float, 2>(ctx, p);
     else if (nt <= 4) rc = launch_few<float, 4>(ctx, p);
