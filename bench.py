@@ -649,8 +649,6 @@ def main():
         step(i)
     torch.cuda.synchronize()
     barrier()
-    mo.ProfileRead()  # reset counters
-    mo.ProfileEnable(True)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     barrier()
@@ -660,22 +658,29 @@ def main():
     e1.record()
     torch.cuda.synchronize()
     barrier()
-    prof64 = mo.ProfileRead()
-    mo.ProfileEnable(False)
     fp64_ms = max_over_ranks(e0.elapsed_time(e1) / K)
     X = Bs[nsteps - 1]
     R = B0.clone()
     assert mo.Mult(R, A0, X, -1.0, 1.0, 0) is None
     fp64_berr = float(R.norm() / (A0.norm() * X.norm() + B0.norm()))
+    # one more step, untimed, with per-kernel-class tracing (CUDA events around each launch)
+    As[0].copy_(A0)
+    Bs[0].copy_(B0)
+    torch.cuda.synchronize()
+    mo.ProfileRead()
+    mo.ProfileEnable(True)
+    step(0)
+    prof64 = mo.ProfileRead()
+    mo.ProfileEnable(False)
     del As, Bs, R
     torch.cuda.empty_cache()
-    g_ms, g_fl = prof64.ms["gemm"] / K, prof64.flops["gemm"] / K
+    g_ms, g_fl = prof64.ms["gemm"], prof64.flops["gemm"]
     fp64_path = {
         "ms": fp64_ms, "berr": fp64_berr, "tflops": n ** 3 / 3 / (fp64_ms * 1e-3) / 1e12,
         "frac_fp64_peak": n ** 3 / 3 / (fp64_ms * 1e-3) / 1e12 / fp64_peak,
         "gemm_engine_tflops": g_fl / (g_ms * 1e-3) / 1e12 if g_ms else None,
-        "per_class_ms_per_step": {k: v / K for k, v in prof64.ms.items() if prof64.launches[k]},
-        "launches_per_step": sum(prof64.launches.values()) / K,
+        "per_class_ms_traced_step": {k: v for k, v in prof64.ms.items() if prof64.launches[k]},
+        "launches_per_step": sum(prof64.launches.values()),
     }
 
     # ---- the headline: TF32x3 factor + FP64 refinement to berr <= 1e-14, same A and B ----
@@ -690,8 +695,7 @@ def main():
         mstep()
     torch.cuda.synchronize()
     barrier()
-    mo.ProfileRead()
-    mo.ProfileEnable(True)
+    mo.ProfileRead()  # resets the launch counters (tracing stays off while timing)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     barrier()
@@ -703,9 +707,15 @@ def main():
         e1.record()
         torch.cuda.synchronize()
     barrier()
+    timed_launches = mo.ProfileRead().launches
+    ms = max_over_ranks(e0.elapsed_time(e1) / K)
+    # per-kernel-class device time from extra, untimed steps with tracing on
+    PT = 2
+    mo.ProfileEnable(True)
+    for _ in range(PT):
+        mstep()
     prof = mo.ProfileRead()
     mo.ProfileEnable(False)
-    ms = max_over_ranks(e0.elapsed_time(e1) / K)
     R = B0.clone()
     assert mo.Mult(R, A0, Xm, -1.0, 1.0, 0) is None
     berr = float(R.norm() / (A0.norm() * Xm.norm() + B0.norm()))
@@ -713,8 +723,8 @@ def main():
 
     # roofline of the dominant kernel, the tcgen05 split-product GEMM (lp_gemm_tc_kernel):
     # bytes = its C tile read + write and operand reads, flops = the three products
-    l_ms, l_fl, l_by = prof.ms["lpgemm"] / K, prof.flops["lpgemm"] / K, prof.bytes["lpgemm"] / K
-    l_n = prof.launches["lpgemm"] / K
+    l_ms, l_fl, l_by = prof.ms["lpgemm"] / PT, prof.flops["lpgemm"] / PT, prof.bytes["lpgemm"] / PT
+    l_n = prof.launches["lpgemm"] / PT
     hbm_peak = _measured_peak("hbm_gbs", 6650.0)
     bf16_peak = _measured_peak("bf16_tflops", 1590.0)
     achieved_gbs = l_by / (l_ms * 1e-3) / 1e9 if l_ms else 0.0
@@ -739,9 +749,10 @@ def main():
                    "frac": achieved_tf / (bf16_peak / 2),
                    "peak_source": "half of MEASURED_PEAKS.json bf16_tflops (TF32 runs at half the BF16 rate)"},
         "share_of_step": l_ms / ms if ms else None,
-        "per_class_ms_per_step": {k: v / K for k, v in prof.ms.items() if prof.launches[k]},
+        "per_class_ms_per_traced_step": {k: v / PT for k, v in prof.ms.items() if prof.launches[k]},
+        "note": "achieved and per-class times come from 2 extra steps traced with CUDA events "
+                "around every launch; the headline value is timed with tracing off",
     }
-    launches = sum(prof.launches.values()) / K
 
     # ---- e2e: host buffers through the public API ----
     e2e = None
@@ -865,8 +876,8 @@ def main():
             "ir_iters": [i.iters for i in infos], "gmres_iters": [i.gmres_iters for i in infos],
             "fp64_path": fp64_path, "speedup_vs_fp64": fp64_ms / ms,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": int(sum(prof.launches.values())),
-            "gpu_launches_by_class": prof.launches,
+            "gpu_launches": int(sum(timed_launches.values())),
+            "gpu_launches_by_class": timed_launches,
             "clocks": clk.summary(), "fp64_peak_tflops": fp64_peak, "extras": extras,
         }
         print(json.dumps(line), flush=True)

@@ -286,6 +286,9 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
         for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0;
 
+    // a warp whose 32 columns all lie past N (narrow C, e.g. a residual with few
+    // right-hand sides) keeps the stage hand-shake but issues no loads or MMAs
+    const bool idle = n0 + wn * 32 >= p.N;
     for (int kt = u.k0; kt < u.k1; ++kt, ++it) {
       const int s = it % STAGES;
       const uint32_t ph = (it / STAGES) & 1;
@@ -293,7 +296,7 @@ __global__ void __launch_bounds__(THREADS, 1)
       const double *As = tiles + s * 2 * TILE_DOUBLES;
       const double *Bs = As + TILE_DOUBLES;
 #pragma unroll
-      for (int kk = 0; kk < BK; kk += 4) {
+      for (int kk = 0; kk < BK && !idle; kk += 4) {
         const int q = kk >> 2, q2 = q & 1;
         double a[4][2], b[4];
 #pragma unroll

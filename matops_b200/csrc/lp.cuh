@@ -41,6 +41,10 @@ struct LpGemmArgs {
   int64_t ldc = 0;
   int mode = kGemm;
   int max_ctas = 0;
+  // optional: also write rows out_row0 .. M - 1 of the result, split, to `out` (K-major:
+  // out row r - out_row0 holds C's row r, columns 0 .. N - 1); needs a TMA-compatible C
+  LpSplit out{};
+  int out_row0 = 0;
 };
 int lp_gemm(mo_ctx *ctx, int prec, const LpGemmArgs &a);
 

@@ -8,9 +8,11 @@
 // driver (potrf.cu) with the same one-step look-ahead:
 //   diag   : W11 -> FP64, Cholesky + inverse in shared memory; L11 back to W (FP32), the
 //            FP64 inverse kept for the refinement solves, the split inverse for (panel)
-//   panel  : L21 = A21 * L11^-T   (A21 split, split-product GEMM, written over A21)
-//   split  : L21 -> K-major hi/lo panel P
-//   update : W22 -= P P^T (lower), the next block column first on the look-ahead path
+//   panel  : L21 = A21 * L11^-T   (split-product GEMM, written over A21; its epilogue also
+//            writes the K-major hi/lo panel P)
+//   update : W22 -= P P^T (lower), the next block column first on the look-ahead path; that
+//            launch's epilogue writes the next step's split A21, so no separate split pass
+//            sits on the step-to-step chain
 // A NaN pivot stops the factorization; its global column is reported like
 // DecomposeCHOL's (info = column + 1).
 #include <cuda_bf16.h>
@@ -141,7 +143,9 @@ int set_lp_diag_smem() {
   return MO_OK;
 }
 
-// diagonal block + panel of step k on ctx->stream; P receives the split L21
+// diagonal block + panel of step k on ctx->stream; P receives the split L21.  The split
+// A21 (f.PA) is made here for the first panel only: later ones come out of the previous
+// step's next-block-column update (see lp_chol_factor).
 int lp_panel(mo_ctx *ctx, LpChol &f, int k, int *d_info, double *d_bad, const LpSplit &P) {
   float *Wkk = f.W + k + (int64_t)k * f.ldw;
   double *inv = f.inv + (size_t)(k / NB) * NB * NB;
@@ -158,8 +162,9 @@ int lp_panel(mo_ctx *ctx, LpChol &f, int k, int *d_info, double *d_bad, const Lp
   const int rest = f.NP - k - NB;
   if (rest <= 0) return MO_OK;
   float *A21 = Wkk + NB;
-  int rc = lp_split(ctx, f.prec, A21, f.ldw, rest, NB, f.PA);
-  if (rc) return rc;
+  int rc;
+  if (k == 0 && (rc = lp_split(ctx, f.prec, A21, f.ldw, rest, NB, f.PA))) return rc;
+  // L21 = A21 L11^-T, written to W and, split, to P by the GEMM's epilogue
   LpGemmArgs g;
   g.M = rest;
   g.N = NB;
@@ -170,8 +175,9 @@ int lp_panel(mo_ctx *ctx, LpChol &f, int k, int *d_info, double *d_bad, const Lp
   g.B = f.Linv;
   g.C = A21;
   g.ldc = f.ldw;
-  if ((rc = lp_gemm(ctx, f.prec, g))) return rc;
-  return lp_split(ctx, f.prec, A21, f.ldw, rest, NB, P);
+  g.out = P;
+  g.out_row0 = 0;
+  return lp_gemm(ctx, f.prec, g);
 }
 
 }  // namespace
@@ -257,6 +263,10 @@ int lp_chol_factor(mo_ctx *ctx, LpChol &f, int *d_info, double *d_bad) {
     g.C = W22;
     g.ldc = f.ldw;
     g.mode = kGemmLower;
+    // rows below its top 128 x 128 block are the next step's A21: the epilogue splits them
+    // into f.PA for the next panel (which runs after this launch, on the look-ahead stream)
+    g.out = f.PA;
+    g.out_row0 = NB;
     if ((rc = lp_gemm(ctx, f.prec, g))) return rc;
     if ((rc = stream_wait(ctx, s1, s0, ctx->ev_fork))) return rc;
     // 2. the next step's diagonal block and panel on the look-ahead stream

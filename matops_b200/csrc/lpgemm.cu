@@ -53,6 +53,9 @@ struct TcParams {
   int kstages;  // ceil(K * esize / 128)
   int c_tma;    // C moves through shared memory by TMA (else plain loads and stores)
   int c_load;   // the C tile is read (beta != 0, or lower mode)
+  char *shi, *slo;  // optional split copy of rows >= srow0 of the result (K-major)
+  int64_t sldk;
+  int srow0;
   int *status;
 };
 
@@ -85,6 +88,16 @@ template <int PREC>
 __host__ __device__ constexpr uint32_t idesc() {
   return (1u << 4) | ((PREC == kLpBf16x3 ? 1u : 2u) << 7) | ((PREC == kLpBf16x3 ? 1u : 2u) << 10) |
          ((uint32_t)(TB >> 3) << 17) | ((uint32_t)(TB >> 4) << 24);
+}
+
+__device__ __forceinline__ void split_bf16(float x, __nv_bfloat16 &hi, __nv_bfloat16 &lo) {
+  hi = __float2bfloat16_rn(x);
+  lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+}
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
 }
 
 template <int PREC>
@@ -267,6 +280,39 @@ __global__ void __launch_bounds__(TTHREADS, 1)
             if (p.mode != kGemmLower || row >= col) *cs = nv;
           }
         }
+        // split copy of this thread's row (it wrote that row of the tile itself)
+        if (p.shi != nullptr && row < p.M && row >= p.srow0) {
+          constexpr int ES = PREC == kLpBf16x3 ? 2 : 4;
+          const int64_t obase = ((int64_t)(row - p.srow0) * p.sldk + tn * TB) * ES;
+#pragma unroll 1
+          for (int c0 = 0; c0 < TB && tn * TB + c0 < p.N; c0 += 8) {
+            float x[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+              x[u] = tn * TB + c0 + u < p.N ? ctile[(c0 + u) * TB + rl] : 0.f;
+            if (PREC == kLpBf16x3) {
+              __align__(16) __nv_bfloat16 h[8], l[8];
+#pragma unroll
+              for (int u = 0; u < 8; ++u) split_bf16(x[u], h[u], l[u]);
+              *reinterpret_cast<uint4 *>(p.shi + obase + c0 * ES) = *reinterpret_cast<const uint4 *>(h);
+              *reinterpret_cast<uint4 *>(p.slo + obase + c0 * ES) = *reinterpret_cast<const uint4 *>(l);
+            } else {
+              __align__(16) uint32_t h[8], l[8];
+#pragma unroll
+              for (int u = 0; u < 8; ++u) {
+                h[u] = to_tf32(x[u]);
+                l[u] = to_tf32(x[u] - __uint_as_float(h[u]));
+              }
+#pragma unroll
+              for (int v = 0; v < 2; ++v) {
+                *reinterpret_cast<uint4 *>(p.shi + obase + (c0 + 4 * v) * ES) =
+                    *reinterpret_cast<const uint4 *>(h + 4 * v);
+                *reinterpret_cast<uint4 *>(p.slo + obase + (c0 + 4 * v) * ES) =
+                    *reinterpret_cast<const uint4 *>(l + 4 * v);
+              }
+            }
+          }
+        }
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(&tempty[buf]);
@@ -326,16 +372,6 @@ __global__ void __launch_bounds__(TTHREADS, 1)
 // split: X (FP32 column-major) -> K-major hi/lo.  A CTA takes 64 rows x 32 columns,
 // stages them transposed in shared memory and writes 8 consecutive k per thread and part.
 // ---------------------------------------------------------------------------------------
-__device__ __forceinline__ void split_bf16(float x, __nv_bfloat16 &hi, __nv_bfloat16 &lo) {
-  hi = __float2bfloat16_rn(x);
-  lo = __float2bfloat16_rn(x - __bfloat162float(hi));
-}
-__device__ __forceinline__ uint32_t to_tf32(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return r;
-}
-
 // by_col: out row r = column r of X (X is cols x rows, column-major): no transpose
 template <int PREC>
 __global__ void __launch_bounds__(256) lp_split_cols_kernel(const float *X, int64_t ld, int rows,
@@ -483,6 +519,11 @@ int lp_gemm(mo_ctx *ctx, int prec, const LpGemmArgs &a) {
   p.c_tma = c_tmap(&m[4], a.C, a.M, a.N, a.ldc) ? 1 : 0;
   if (!p.c_tma) m[4] = CUtensorMap{};
   p.c_load = (a.beta != 0.f || p.mode == kGemmLower) ? 1 : 0;
+  p.shi = (char *)a.out.hi;
+  p.slo = (char *)a.out.lo;
+  p.sldk = a.out.ldk;
+  p.srow0 = a.out_row0;
+  if (p.shi && (!p.c_tma || a.out.ldk % 8 || a.N > a.out.ldk)) return MO_EINVAL;
   if (!split_tmap(&m[0], a.A.hi, prec, a.K, a.M, a.A.ldk) ||
       !split_tmap(&m[1], a.A.lo, prec, a.K, a.M, a.A.ldk) ||
       !split_tmap(&m[2], a.B.hi, prec, a.K, a.N, a.B.ldk) ||
@@ -498,7 +539,8 @@ int lp_gemm(mo_ctx *ctx, int prec, const LpGemmArgs &a) {
   const double tiles_flops = 3.0 * (double)p.ntiles * TB * TB * a.K * 2.0;
   prof_end(ctx, ps, tiles_flops,
            (double)p.ntiles * TB * TB * 4.0 * (a.beta != 0.f ? 2.0 : 1.0) +
-               (double)(a.M + a.N) * a.K * es * 2.0);
+               (double)(a.M + a.N) * a.K * es * 2.0 +
+               (p.shi ? (double)std::max(0, a.M - a.out_row0) * a.N * es * 2.0 : 0.0));
   return rc;
 }
 
