@@ -28,11 +28,12 @@ namespace {
 //   warps 2-5 epilogue: tcgen05.ld of their 32-lane quarter of the accumulator (TMEM lane
 //             = tile row), C = alpha * acc + beta * C, coalesced along the column
 // The accumulator is double-buffered, so the MMAs of tile t + 1 overlap the epilogue of
-// tile t.  C (FP32, column-major) moves through a 64 KB shared tile: the producer loads
-// it by TMA after the tile's operand stages, the epilogue combines it with the
-// accumulator in place and one thread stores it back by TMA (when C's base and leading
-// dimension allow TMA; otherwise the epilogue reads and writes C directly).  Every wait
-// is bounded (MO_SPIN_LIMIT) and reports MO_EDEVTIMEOUT.
+// tile t.  C (FP32, column-major) moves through shared memory in two 64-column halves,
+// each with its own 32 KB buffer: the producer loads a half by TMA after the tile's
+// operand stages, the epilogue combines it with the accumulator in place and one thread
+// stores it back by TMA, so one half's transfer overlaps the other half's epilogue (when
+// C's base and leading dimension allow TMA; otherwise the epilogue reads and writes C
+// directly).  Every wait is bounded (MO_SPIN_LIMIT) and reports MO_EDEVTIMEOUT.
 constexpr int TB = 128;                  // tile rows = tile columns
 constexpr int TSTAGES = 2;
 constexpr int TPART = TB * 128;          // one operand part of a stage: 128 rows x 128 B
@@ -159,10 +160,12 @@ __global__ void __launch_bounds__(TTHREADS, 1)
   uint64_t *empty = full + TSTAGES;
   uint64_t *tfull = empty + TSTAGES;   // [2]
   uint64_t *tempty = tfull + 2;        // [2]
-  uint64_t *cfull = tempty + 2;
-  uint64_t *cempty = cfull + 1;
-  uint64_t *cready = cempty + 1;  // the four epilogue warps have written the C tile
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(cready + 1);
+  // the C tile moves in two 64-column halves with their own buffers and barriers, so one
+  // half's load or store overlaps the other half's epilogue
+  uint64_t *cfull = tempty + 2;    // [2]
+  uint64_t *cempty = cfull + 2;    // [2]
+  uint64_t *cready = cempty + 2;   // [2] the four epilogue warps have written that half
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(cready + 2);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < TSTAGES; ++s) {
@@ -173,9 +176,11 @@ __global__ void __launch_bounds__(TTHREADS, 1)
       mbar_init(&tfull[b], 1);
       mbar_init(&tempty[b], 4);
     }
-    mbar_init(cfull, 1);
-    mbar_init(cempty, 1);
-    mbar_init(cready, 4);
+    for (int h = 0; h < 2; ++h) {
+      mbar_init(&cfull[h], 1);
+      mbar_init(&cempty[h], 1);
+      mbar_init(&cready[h], 4);
+    }
     fence_barrier_init();
   }
   if (warp == 1) {
@@ -195,7 +200,7 @@ __global__ void __launch_bounds__(TTHREADS, 1)
   if (warp == 0 && lane == 0) {
     // producer: the operand stages of tile t, then (once the previous tile's C has been
     // stored) its C tile
-    int g = 0, tc = 0;
+    int g = 0, tc = 0, cu[2] = {0, 0};  // cu: uses of each C half buffer
     bool ok = true;
     for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x, ++tc) {
       int tm, tn;
@@ -215,12 +220,19 @@ __global__ void __launch_bounds__(TTHREADS, 1)
         tma_load_2d(st + 3 * TPART, &tBl, &full[slot], ks * KEL, tn * TB);
       }
       if (!ok || !p.c_tma) continue;
-      if (!mbar_wait(cempty, (tc & 1) ^ 1, p.status)) break;
-      if (p.c_load) {
-        mbar_arrive_expect_tx(cfull, TCTILE);
-        tma_load_2d(ctile, &tC, cfull, tm * TB, tn * TB);
-      } else {
-        mbar_arrive(cfull);
+      const int nh = tn * TB + TB / 2 < p.N ? 2 : 1;  // the second half only if it has columns
+      for (int h = 0; h < nh; ++h) {
+        if (!mbar_wait(&cempty[h], (cu[h] & 1) ^ 1, p.status)) {
+          ok = false;
+          break;
+        }
+        if (p.c_load) {
+          mbar_arrive_expect_tx(&cfull[h], TCTILE / 2);
+          tma_load_2d(ctile + h * TB * (TB / 2), &tC, &cfull[h], tm * TB, tn * TB + h * (TB / 2));
+        } else {
+          mbar_arrive(&cfull[h]);
+        }
+        ++cu[h];
       }
     }
   } else if (warp == 1 && lane == 0) {
@@ -257,7 +269,7 @@ __global__ void __launch_bounds__(TTHREADS, 1)
     // epilogue: warp w reads TMEM lanes 32 * (w % 4) .. + 31 (= tile rows)
     const int q = warp & 3;
     const int rl = q * 32 + lane;
-    int tc = 0;
+    int tc = 0, cu[2] = {0, 0};  // cu: uses of each C half buffer
     for (int t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++tc) {
       int tm, tn;
       tile_coords(p, t, tm, tn);
@@ -266,71 +278,83 @@ __global__ void __launch_bounds__(TTHREADS, 1)
       tc_fence_after();
       const int row = tm * TB + rl;
       if (p.c_tma) {
-        if (!mbar_wait(cfull, tc & 1, p.status)) break;
-#pragma unroll 1
-        for (int c0 = 0; c0 < TB; c0 += 16) {
-          uint32_t v[16];
-          tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + buf * TB + c0, v);
-#pragma unroll
-          for (int r = 0; r < 16; ++r) {
-            const int col = tn * TB + c0 + r;
-            float *cs = ctile + (c0 + r) * TB + rl;
-            const float a = p.alpha * __uint_as_float(v[r]);
-            const float nv = p.beta == 0.f ? a : fmaf(p.beta, *cs, a);
-            if (p.mode != kGemmLower || row >= col) *cs = nv;
+        const int nh = tn * TB + TB / 2 < p.N ? 2 : 1;
+        bool fail = false;
+        for (int h = 0; h < nh && !fail; ++h) {
+          float *cb = ctile + h * TB * (TB / 2);  // this half: column-major 128 x 64
+          if (!mbar_wait(&cfull[h], cu[h] & 1, p.status)) {
+            fail = true;
+            break;
           }
-        }
-        // split copy of this thread's row (it wrote that row of the tile itself)
-        if (p.shi != nullptr && row < p.M && row >= p.srow0) {
-          constexpr int ES = PREC == kLpBf16x3 ? 2 : 4;
-          const int64_t obase = ((int64_t)(row - p.srow0) * p.sldk + tn * TB) * ES;
 #pragma unroll 1
-          for (int c0 = 0; c0 < TB && tn * TB + c0 < p.N; c0 += 8) {
-            float x[8];
+          for (int c0 = h * (TB / 2); c0 < (h + 1) * (TB / 2); c0 += 16) {
+            uint32_t v[16];
+            tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + buf * TB + c0, v);
 #pragma unroll
-            for (int u = 0; u < 8; ++u)
-              x[u] = tn * TB + c0 + u < p.N ? ctile[(c0 + u) * TB + rl] : 0.f;
-            if (PREC == kLpBf16x3) {
-              __align__(16) __nv_bfloat16 h[8], l[8];
+            for (int r = 0; r < 16; ++r) {
+              const int col = tn * TB + c0 + r;
+              float *cs = cb + (c0 - h * (TB / 2) + r) * TB + rl;
+              const float a = p.alpha * __uint_as_float(v[r]);
+              const float nv = p.beta == 0.f ? a : fmaf(p.beta, *cs, a);
+              if (p.mode != kGemmLower || row >= col) *cs = nv;
+            }
+          }
+          // split copy of this thread's row (it wrote that row of the half itself)
+          if (p.shi != nullptr && row < p.M && row >= p.srow0) {
+            constexpr int ES = PREC == kLpBf16x3 ? 2 : 4;
+            const int64_t obase = ((int64_t)(row - p.srow0) * p.sldk + tn * TB) * ES;
+#pragma unroll 1
+            for (int c0 = h * (TB / 2); c0 < (h + 1) * (TB / 2) && tn * TB + c0 < p.N; c0 += 8) {
+              float x[8];
 #pragma unroll
-              for (int u = 0; u < 8; ++u) split_bf16(x[u], h[u], l[u]);
-              *reinterpret_cast<uint4 *>(p.shi + obase + c0 * ES) = *reinterpret_cast<const uint4 *>(h);
-              *reinterpret_cast<uint4 *>(p.slo + obase + c0 * ES) = *reinterpret_cast<const uint4 *>(l);
-            } else {
-              __align__(16) uint32_t h[8], l[8];
+              for (int u = 0; u < 8; ++u)
+                x[u] = tn * TB + c0 + u < p.N ? cb[(c0 - h * (TB / 2) + u) * TB + rl] : 0.f;
+              if (PREC == kLpBf16x3) {
+                __align__(16) __nv_bfloat16 hh[8], ll[8];
 #pragma unroll
-              for (int u = 0; u < 8; ++u) {
-                h[u] = to_tf32(x[u]);
-                l[u] = to_tf32(x[u] - __uint_as_float(h[u]));
-              }
+                for (int u = 0; u < 8; ++u) split_bf16(x[u], hh[u], ll[u]);
+                *reinterpret_cast<uint4 *>(p.shi + obase + c0 * ES) = *reinterpret_cast<const uint4 *>(hh);
+                *reinterpret_cast<uint4 *>(p.slo + obase + c0 * ES) = *reinterpret_cast<const uint4 *>(ll);
+              } else {
+                __align__(16) uint32_t hh[8], ll[8];
 #pragma unroll
-              for (int v = 0; v < 2; ++v) {
-                *reinterpret_cast<uint4 *>(p.shi + obase + (c0 + 4 * v) * ES) =
-                    *reinterpret_cast<const uint4 *>(h + 4 * v);
-                *reinterpret_cast<uint4 *>(p.slo + obase + (c0 + 4 * v) * ES) =
-                    *reinterpret_cast<const uint4 *>(l + 4 * v);
+                for (int u = 0; u < 8; ++u) {
+                  hh[u] = to_tf32(x[u]);
+                  ll[u] = to_tf32(x[u] - __uint_as_float(hh[u]));
+                }
+#pragma unroll
+                for (int v = 0; v < 2; ++v) {
+                  *reinterpret_cast<uint4 *>(p.shi + obase + (c0 + 4 * v) * ES) =
+                      *reinterpret_cast<const uint4 *>(hh + 4 * v);
+                  *reinterpret_cast<uint4 *>(p.slo + obase + (c0 + 4 * v) * ES) =
+                      *reinterpret_cast<const uint4 *>(ll + 4 * v);
+                }
               }
             }
           }
-        }
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&tempty[buf]);
-        // the four epilogue warps' shared-memory writes, then one TMA store of the tile
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncwarp();
-        if (lane == 0) mbar_arrive(cready);
-        if (warp == 2) {
-          int ok = 1;
-          if (lane == 0) {
-            ok = mbar_wait(cready, tc & 1, p.status) ? 1 : 0;
-            if (ok) {
-              tma_store_2d(&tC, ctile, tm * TB, tn * TB);
-              mbar_arrive(cempty);
-            }
+          if (h == nh - 1) {  // the accumulator has been read out
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty[buf]);
           }
-          if (!__shfl_sync(0xffffffffu, ok, 0)) break;  // warp-uniform exit
+          // the four epilogue warps' shared-memory writes, then one TMA store of the half
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&cready[h]);
+          if (warp == 2) {
+            int ok = 1;
+            if (lane == 0) {
+              ok = mbar_wait(&cready[h], cu[h] & 1, p.status) ? 1 : 0;
+              if (ok) {
+                tma_store_2d(&tC, cb, tm * TB, tn * TB + h * (TB / 2));
+                mbar_arrive(&cempty[h]);
+              }
+            }
+            if (!__shfl_sync(0xffffffffu, ok, 0)) fail = true;  // warp-uniform exit
+          }
+          ++cu[h];
         }
+        if (fail) break;
       } else {
         const bool rok = row < p.M;
 #pragma unroll 1
@@ -461,14 +485,14 @@ bool split_tmap(CUtensorMap *tm, const void *ptr, int prec, int64_t K, int64_t r
             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// map over the FP32 column-major C: box 128 rows x 128 columns, no swizzle
+// map over the FP32 column-major C: box 128 rows x 64 columns (half a tile), no swizzle
 bool c_tmap(CUtensorMap *tm, float *C, int64_t M, int64_t N, int64_t ldc) {
   auto fn = tc_encode_fn();
   if (!fn) return false;
   if (((uintptr_t)C & 15) || (ldc * 4) % 16) return false;
   cuuint64_t dims[2] = {(cuuint64_t)std::max<int64_t>(M, 1), (cuuint64_t)std::max<int64_t>(N, 1)};
   cuuint64_t strides[1] = {(cuuint64_t)(ldc * 4)};
-  cuuint32_t box[2] = {(cuuint32_t)TB, (cuuint32_t)TB};
+  cuuint32_t box[2] = {(cuuint32_t)TB, (cuuint32_t)(TB / 2)};  // one 64-column half
   cuuint32_t estr[2] = {1, 1};
   return fn(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, C, dims, strides, box, estr,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
