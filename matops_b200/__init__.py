@@ -8,7 +8,7 @@ from .api import (  # noqa: F401
     LEFT, LOWER, NONE, NOTRANS, RIGHT, TRANS, TRANSA, TRANSB, UNIT, UPPER,
     BlockingParams, DecomposeBlockSize, DecomposeCHOL, DecomposeLU, MatopsError, MatopsPanic,
     Mult, NumWorkers, RankUpdateSym, SetPanicOnError, SolveCHOL, SolveLU, SolveTrm, Sync,
-    matrix, to_device, view, Upload, Download, host_matrix, Profile, ProfileEnable, ProfileRead,
+    matrix, to_device, view, Upload, UploadTriangle, Download, host_matrix, Profile, ProfileEnable, ProfileRead,
     MeasureFP64Peak, PREC_BF16X3, PREC_TF32X3, IR_AUTO, IR_CLASSIC, IR_GMRES, IR_NO_FALLBACK,
     IRInfo, SolveCHOLMixed, LPGemm, BATCH_CHOL, BATCH_LU, BATCH_MAX_N, BatchPlan,
     DecomposeCHOLAdjoint, DecomposeCHOLAdjointBatched, SolveCHOLAdjoint,

@@ -57,6 +57,7 @@ def lib() -> ctypes.CDLL:
         "mo_malloc": [p, ctypes.POINTER(p), sz],
         "mo_free": [p, p],
         "mo_upload": [p, M, p, i64],
+        "mo_upload_tri": [p, M, p, i64, i],
         "mo_download": [p, p, i64, M],
         "mo_upload_bytes": [p, p, p, sz],
         "mo_download_bytes": [p, p, p, sz],

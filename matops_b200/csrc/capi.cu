@@ -260,6 +260,28 @@ int mo_upload(mo_ctx *ctx, mo_matrix dst, const double *src, int64_t ld_src) {
   return MO_OK;
 }
 
+int mo_upload_tri(mo_ctx *ctx, mo_matrix dst, const double *src, int64_t ld_src, int flags) {
+  int rc = mo::enter(ctx);
+  if (rc) return rc;
+  View v;
+  if ((rc = mo::to_view(dst, v))) return rc;
+  if (v.rows != v.cols) return MO_ESIZE;
+  if (v.rows == 0) return MO_OK;
+  if (!src || ld_src < v.rows) return MO_EINVAL;
+  const bool upper = (flags & MO_UPPER) != 0;
+  const int64_t n = v.rows;
+  // one 2-D copy per 128-column block: rows j0..n-1 (lower) or 0..j0+w-1 (upper), so the
+  // bytes moved are n (n + 128) / 2 elements instead of n^2
+  for (int64_t j0 = 0; j0 < n; j0 += 128) {
+    const int64_t w = n - j0 < 128 ? n - j0 : 128;
+    const int64_t r0 = upper ? 0 : j0, nr = upper ? j0 + w : n - j0;
+    MO_CUDA_TRY(cudaMemcpy2DAsync(v.d + r0 + j0 * v.ld, v.ld * 8, src + r0 + j0 * ld_src,
+                                  ld_src * 8, (size_t)nr * 8, w, cudaMemcpyHostToDevice,
+                                  ctx->stream));
+  }
+  return MO_OK;
+}
+
 int mo_download(mo_ctx *ctx, double *dst, int64_t ld_dst, mo_matrix src) {
   int rc = mo::enter(ctx);
   if (rc) return rc;

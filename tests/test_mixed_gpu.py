@@ -237,3 +237,31 @@ def test_mixed_solve_many_rhs(gpu, oracle, rng, flags, n, nrhs):
     assert berr_inf(A, X, B) <= 1.5e-14
     Xr = fp64_solution(oracle, A, B)
     assert fro(X - Xr) / fro(Xr) <= 1e-9
+
+
+@pytest.mark.parametrize("flags", [LO, UP])
+@pytest.mark.parametrize("n", [1, 100, 128, 300])
+def test_upload_triangle_then_solve(gpu, rng, flags, n):
+    """mo_upload_tri moves the stored triangle in 128-column blocks (each block's
+    diagonal square whole) and leaves the rest of the device matrix as it was; the
+    mixed solve on that upload meets the refinement tolerance."""
+    A = spd(rng, n)
+    B = rng.standard_normal((n, 2))
+    host_big = gpu.host_matrix(n + 5, n)
+    Ah = host_big[2:2 + n, :]
+    Ah.copy_(torch.as_tensor(A))
+    Ad = gpu.matrix(n, n, fill=7.0)
+    gpu.UploadTriangle(Ad, Ah, flags)
+    gpu.Sync()
+    out = Ad.cpu().numpy()
+    i, j = np.indices((n, n))
+    blk0 = (j // 128) * 128
+    copied = (i >= blk0) if flags == LO else (i < np.minimum(blk0 + 128, n))
+    assert np.array_equal(out[copied], A[copied])
+    assert np.all(out[~copied] == 7.0)
+    stored = (i >= j) if flags == LO else (i <= j)
+    assert np.all(copied[stored])
+    Xd = gpu.matrix(n, 2)
+    info, err = gpu.SolveCHOLMixed(Xd, Ad, gpu.to_device(B), flags, TF32X3)
+    assert err is None and info.converged, info
+    assert berr_inf(A, Xd.cpu().numpy(), B) <= 1.5e-14
