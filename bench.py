@@ -877,6 +877,7 @@ def main():
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "berr": berr, "berr_inf": max(i.berr for i in infos),
             "ir_iters": [i.iters for i in infos], "gmres_iters": [i.gmres_iters for i in infos],
+            "ir_berr_history": infos[0].history,
             "fp64_path": fp64_path, "speedup_vs_fp64": fp64_ms / ms,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(sum(timed_launches.values())),

@@ -6,6 +6,9 @@
 // mma.sync.m16n8k4.f64 and hand stages back through mbarriers.  Operands whose base or
 // leading dimension breaks TMA's 16-byte rules (arbitrary FloatMatrix views) use the
 // same kernel with an 8-byte cp.async producer writing the identical swizzled layout.
+// A C at most 64 columns wide and at least 2048 rows tall (the FP64 residual of a solve
+// with few right-hand sides) takes 256x64 tiles in a 5-stage ring instead, with the
+// consumer warps arranged 4 x 2, so that none of them idles on columns past N.
 //
 // Arithmetic (calgo/dmmat_gemm.c:364-415 semantics): C = beta*C + alpha*sum_k, with
 // beta == 0 never reading C.  SYRK modes restrict tiles and elements to one triangle and
@@ -32,9 +35,20 @@ constexpr int CONSUMER_WARPS = 8;
 constexpr int THREADS = 384;
 constexpr int PRODUCER_REGS = 40, CONSUMER_REGS = 232;
 static_assert(THREADS * 168 >= 128 * PRODUCER_REGS + 256 * CONSUMER_REGS, "register split");
-constexpr int TILE_DOUBLES = 128 * BK;                     // one operand slab: 16 KB
-constexpr uint32_t STAGE_BYTES = 2 * TILE_DOUBLES * 8;     // A slab + B slab
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 2 * STAGES * 8;
+// Tile geometry of one instantiation.  NARROW (C at most 64 columns wide, e.g. a residual
+// B - A X with few right-hand sides): 256 x 64 tiles, warps in a 4 x 2 grid of the same
+// 64 x 32 warp tiles, so all eight consumer warps issue MMAs where a 128 x 128 tile would
+// leave half of them idle.
+template <bool NARROW>
+struct Geo {
+  static constexpr int TBM = NARROW ? 256 : 128, TBN = NARROW ? 64 : 128;
+  static constexpr int NSTAGES = NARROW ? 5 : STAGES;
+  static constexpr int A_DBL = TBM * BK, B_DBL = TBN * BK, STAGE_DBL = A_DBL + B_DBL;
+  static constexpr uint32_t SBYTES = STAGE_DBL * 8;
+  static constexpr int SMEM = NSTAGES * SBYTES + 1024 + 2 * NSTAGES * 8;
+  static constexpr int WN = TBN / 32;  // warp columns
+};
+static_assert(Geo<true>::SMEM <= 227 * 1024 && Geo<false>::SMEM <= 227 * 1024, "shared memory");
 
 // Swizzled shared-memory layouts (TMA SWIZZLE_128B: 16-byte chunk ^= 128-byte row % 8).
 // K-major slab: 128 rows (m or n) of 16 k-values (128 B per row).
@@ -68,14 +82,15 @@ struct KParams {
   int epoch;
 };
 
-// cp.async producer for one 128 x 16 slab of an operand whose element (mn, k) lives at
-// src[k + mn*ld] (KMAJ) or src[mn + k*ld] (!KMAJ); out-of-range elements are zero-filled.
-template <bool KMAJ>
+// cp.async producer for one ROWS x 16 slab (ROWS = 64 or 128) of an operand whose element
+// (mn, k) lives at src[k + mn*ld] (KMAJ) or src[mn + k*ld] (!KMAJ); out-of-range elements
+// are zero-filled.
+template <bool KMAJ, int ROWS = 128>
 __device__ __forceinline__ void load_slab_cpasync(double *dst, const double *src, int64_t ld,
                                                   int mn0, int k0, int MN, int K, int lane) {
   if constexpr (KMAJ) {
 #pragma unroll 8
-    for (int i = 0; i < 64; ++i) {
+    for (int i = 0; i < ROWS / 2; ++i) {
       int mn = 2 * i + (lane >> 4), k = lane & 15;
       int gm = mn0 + mn, gk = k0 + k;
       bool ok = gm < MN && gk < K;
@@ -86,7 +101,7 @@ __device__ __forceinline__ void load_slab_cpasync(double *dst, const double *src
 #pragma unroll 4
     for (int k = 0; k < 16; ++k)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
+      for (int j = 0; j < ROWS / 32; ++j) {
         int mn = 32 * j + lane;
         int gm = mn0 + mn, gk = k0 + k;
         bool ok = gm < MN && gk < K;
@@ -167,14 +182,16 @@ __device__ __forceinline__ void consumer_bar() {
   asm volatile("bar.sync 1, 256;" ::: "memory");
 }
 
-template <bool A_KMAJ, bool B_KMAJ, bool USE_TMA>
+template <bool A_KMAJ, bool B_KMAJ, bool USE_TMA, bool NARROW>
 __global__ void __launch_bounds__(THREADS, 1)
     dgemm_tile_kernel(const __grid_constant__ CUtensorMap tmA,
                       const __grid_constant__ CUtensorMap tmB, const KParams p) {
+  using G = Geo<NARROW>;
+  constexpr int STAGES = G::NSTAGES;
   extern __shared__ unsigned char smem_raw[];
   const uintptr_t base = (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023);
   double *tiles = reinterpret_cast<double *>(base);
-  uint64_t *full = reinterpret_cast<uint64_t *>(base + STAGES * STAGE_BYTES);
+  uint64_t *full = reinterpret_cast<uint64_t *>(base + STAGES * G::SBYTES);
   uint64_t *empty = full + STAGES;
   __shared__ int s_abort;
 
@@ -198,7 +215,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     for (int ui = 0; unit_at(p, ui, u); ++ui) {
       int tm, tn;
       tile_coords(p, u.tile, tm, tn);
-      const int m0 = tm * BM, n0 = tn * BN;
+      const int m0 = tm * G::TBM, n0 = tn * G::TBN;
       for (int kt = u.k0; kt < u.k1; ++kt, ++it) {
         const int s = it % STAGES;
         const uint32_t ph = (it / STAGES) & 1;
@@ -206,31 +223,38 @@ __global__ void __launch_bounds__(THREADS, 1)
           if constexpr (!USE_TMA) asm volatile("cp.async.wait_all;" ::: "memory");
           return;
         }
-        double *As = tiles + s * 2 * TILE_DOUBLES;
-        double *Bs = As + TILE_DOUBLES;
+        double *As = tiles + s * G::STAGE_DBL;
+        double *Bs = As + G::A_DBL;
         const int k0 = kt * BK;
         if constexpr (USE_TMA) {
           if (lane == 0) {
-            mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
+            mbar_arrive_expect_tx(&full[s], G::SBYTES);
+            // K-major maps carry 128-row boxes (64 rows for a narrow B), MN-major maps
+            // 16 x 16 boxes
             if (A_KMAJ) {
-              tma_load_2d(As, &tmA, &full[s], k0, m0);
+#pragma unroll
+              for (int h = 0; h < G::TBM / 128; ++h)
+                tma_load_2d(As + h * 128 * BK, &tmA, &full[s], k0, m0 + 128 * h);
             } else {
 #pragma unroll
-              for (int bb = 0; bb < 8; ++bb)
+              for (int bb = 0; bb < G::TBM / 16; ++bb)
                 tma_load_2d(As + bb * 256, &tmA, &full[s], m0 + 16 * bb, k0);
             }
             if (B_KMAJ) {
               tma_load_2d(Bs, &tmB, &full[s], k0, n0);
             } else {
 #pragma unroll
-              for (int bb = 0; bb < 8; ++bb)
+              for (int bb = 0; bb < G::TBN / 16; ++bb)
                 tma_load_2d(Bs + bb * 256, &tmB, &full[s], n0 + 16 * bb, k0);
             }
           }
           __syncwarp();
         } else {
-          load_slab_cpasync<A_KMAJ>(As, p.A, p.lda, m0, k0, p.M, p.K, lane);
-          load_slab_cpasync<B_KMAJ>(Bs, p.B, p.ldb, n0, k0, p.N, p.K, lane);
+#pragma unroll
+          for (int h = 0; h < G::TBM / 128; ++h)
+            load_slab_cpasync<A_KMAJ>(As + h * 128 * BK, p.A, p.lda, m0 + 128 * h, k0, p.M, p.K,
+                                      lane);
+          load_slab_cpasync<B_KMAJ, G::TBN>(Bs, p.B, p.ldb, n0, k0, p.N, p.K, lane);
           cp_async_arrive_noinc(&full[s]);
         }
       }
@@ -243,7 +267,8 @@ __global__ void __launch_bounds__(THREADS, 1)
   asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(CONSUMER_REGS));
   const int ct = threadIdx.x - 128;  // consumer thread 0..255
   const int cw = warp - 4;
-  const int wm = cw >> 2, wn = cw & 3;  // 2 x 4 grid of 64 x 32 warp tiles
+  // 2 x 4 (4 x 2 when narrow) grid of 64 x 32 warp tiles
+  const int wm = cw >> (NARROW ? 1 : 2), wn = cw & (G::WN - 1);
   const int g = lane >> 2, t = lane & 3;
   // Fragment offsets into the swizzled slabs, split into a per-thread part computed once
   // and compile-time constants (mt, nt, kk).  K-major: element (mn, k) at
@@ -267,7 +292,7 @@ __global__ void __launch_bounds__(THREADS, 1)
   for (int ui = 0; unit_at(p, ui, u); ++ui) {
     int tm, tn;
     tile_coords(p, u.tile, tm, tn);
-    const int m0 = tm * BM, n0 = tn * BN;
+    const int m0 = tm * G::TBM, n0 = tn * G::TBN;
     // warm L2 with this warp's C sub-tile (64 rows x 32 cols: 4 lines of 128 B per column)
     if (u.owner && (p.beta != 0.0 || p.beta_block > 0)) {
 #pragma unroll
@@ -293,8 +318,8 @@ __global__ void __launch_bounds__(THREADS, 1)
       const int s = it % STAGES;
       const uint32_t ph = (it / STAGES) & 1;
       if (!mbar_wait(&full[s], ph, p.status)) return;
-      const double *As = tiles + s * 2 * TILE_DOUBLES;
-      const double *Bs = As + TILE_DOUBLES;
+      const double *As = tiles + s * G::STAGE_DBL;
+      const double *Bs = As + G::A_DBL;
 #pragma unroll
       for (int kk = 0; kk < BK && !idle; kk += 4) {
         const int q = kk >> 2, q2 = q & 1;
@@ -438,13 +463,14 @@ bool make_tmap(CUtensorMap *tm, const double *ptr, uint64_t inner, uint64_t oute
   return r == CUDA_SUCCESS;
 }
 
-template <bool AK, bool BKM, bool TMA>
+template <bool AK, bool BKM, bool TMA, bool NARROW>
 int launch_inst(const KParams &kp, const CUtensorMap &ta, const CUtensorMap &tb, int grid,
                 cudaStream_t st) {
+  constexpr int SMEM_BYTES = Geo<NARROW>::SMEM;
   static std::atomic<uint64_t> attr_done{0};
   int dev = 0;
   cudaGetDevice(&dev);
-  auto kern = dgemm_tile_kernel<AK, BKM, TMA>;
+  auto kern = dgemm_tile_kernel<AK, BKM, TMA, NARROW>;
   const uint64_t bit = 1ull << (dev & 63);
   if (!(attr_done.load() & bit)) {
     // setmaxnreg.inc only draws on the registers the CTA was launched with: refuse to
@@ -461,13 +487,13 @@ int launch_inst(const KParams &kp, const CUtensorMap &ta, const CUtensorMap &tb,
   return MO_OK;
 }
 
-template <bool TMA>
+template <bool TMA, bool NARROW>
 int dispatch(bool ak, bool bk, const KParams &kp, const CUtensorMap &ta, const CUtensorMap &tb,
              int grid, cudaStream_t st) {
-  if (ak) return bk ? launch_inst<true, true, TMA>(kp, ta, tb, grid, st)
-                    : launch_inst<true, false, TMA>(kp, ta, tb, grid, st);
-  return bk ? launch_inst<false, true, TMA>(kp, ta, tb, grid, st)
-            : launch_inst<false, false, TMA>(kp, ta, tb, grid, st);
+  if (ak) return bk ? launch_inst<true, true, TMA, NARROW>(kp, ta, tb, grid, st)
+                    : launch_inst<true, false, TMA, NARROW>(kp, ta, tb, grid, st);
+  return bk ? launch_inst<false, true, TMA, NARROW>(kp, ta, tb, grid, st)
+            : launch_inst<false, false, TMA, NARROW>(kp, ta, tb, grid, st);
 }
 
 }  // namespace
@@ -497,7 +523,10 @@ int launch_gemm(const GemmArgs &a, cudaStream_t stream) {
   kp.mode = a.mode;
   kp.beta_block = a.beta_block;
   kp.status = a.status;
-  const int tiles_m = (a.M + BM - 1) / BM, tiles_n = (a.N + BN - 1) / BN;
+  // narrow C (a residual with few right-hand sides): 256 x 64 tiles
+  const bool narrow = a.mode == kGemm && a.N <= 64 && a.M >= 2048;
+  const int tbm = narrow ? Geo<true>::TBM : BM, tbn = narrow ? Geo<true>::TBN : BN;
+  const int tiles_m = (a.M + tbm - 1) / tbm, tiles_n = (a.N + tbn - 1) / tbn;
   kp.tiles_m = tiles_m;
   kp.tiles_n = tiles_n;
   long long T;
@@ -544,13 +573,16 @@ int launch_gemm(const GemmArgs &a, cudaStream_t stream) {
   if (use_tma) {
     bool okA = ak ? make_tmap(&ta, a.A, kp.K, a.M, a.lda, 16, 128)
                   : make_tmap(&ta, a.A, a.M, kp.K, a.lda, 16, 16);
-    bool okB = bk ? make_tmap(&tb, a.B, kp.K, a.N, a.ldb, 16, 128)
+    bool okB = bk ? make_tmap(&tb, a.B, kp.K, a.N, a.ldb, 16, (uint32_t)tbn)
                   : make_tmap(&tb, a.B, a.N, kp.K, a.ldb, 16, 16);
-    if (okA && okB) return dispatch<true>(ak, bk, kp, ta, tb, grid, stream);
+    if (okA && okB)
+      return narrow ? dispatch<true, true>(ak, bk, kp, ta, tb, grid, stream)
+                    : dispatch<true, false>(ak, bk, kp, ta, tb, grid, stream);
   }
   memset(&ta, 0, sizeof(ta));
   memset(&tb, 0, sizeof(tb));
-  return dispatch<false>(ak, bk, kp, ta, tb, grid, stream);
+  return narrow ? dispatch<false, true>(ak, bk, kp, ta, tb, grid, stream)
+                : dispatch<false, false>(ak, bk, kp, ta, tb, grid, stream);
 }
 
 }  // namespace mo

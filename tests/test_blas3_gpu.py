@@ -26,7 +26,9 @@ def host(t):
 @pytest.mark.parametrize("m,n,k", [(2048, 2048, 2048), (137, 91, 213), (1, 1, 1), (128, 128, 16),
                                    (129, 257, 65), (300, 5, 1000), (7, 300, 3),
                                    # few-wave shapes: K split over CTAs (stream-K partial sums)
-                                   (1536, 1536, 256), (1280, 1408, 400), (1000, 700, 1333)])
+                                   (1536, 1536, 256), (1280, 1408, 400), (1000, 700, 1333),
+                                   # narrow C (N <= 64, M >= 2048): 256 x 64 tiles
+                                   (2048, 64, 512), (2500, 33, 700), (4099, 1, 129), (3000, 64, 16)])
 def test_mult(gpu, oracle, rng, flags, m, n, k):
     A = colmajor(rng.uniform(-1, 1, (k, m) if flags & TA else (m, k)))
     B = colmajor(rng.uniform(-1, 1, (n, k) if flags & TB else (k, n)))
@@ -43,6 +45,30 @@ def test_mult(gpu, oracle, rng, flags, m, n, k):
         assert oracle.Mult(Cr, A, B, alpha, beta, flags) == 0
     err = fro(host(Cg) - Cr)
     assert err <= gemm_bound(k, alpha, beta, A, B, C0), err
+
+
+@pytest.mark.parametrize("flags", [0, TA, TB])
+def test_mult_narrow_unaligned_views(gpu, oracle, rng, flags):
+    """Narrow C (256 x 64 tiles) on views at odd offsets and odd leading dimensions: the
+    cp.async producer fills the 256-row A slab and the 64-row B slab."""
+    m, n, k = 2305, 47, 333
+    Abig = colmajor(rng.uniform(-1, 1, (k + 3, m + 2) if flags & TA else (m + 3, k + 2)), ld=None)
+    Bbig = colmajor(rng.uniform(-1, 1, (n + 3, k + 2) if flags & TB else (k + 3, n + 2)))
+    Cbig = colmajor(rng.uniform(-1, 1, (m + 3, n + 2)))
+    Ag, Bg, Cg = dev(gpu, Abig), dev(gpu, Bbig), dev(gpu, Cbig)
+    sa = (slice(1, 1 + k), slice(1, 1 + m)) if flags & TA else (slice(1, 1 + m), slice(1, 1 + k))
+    sb = (slice(1, 1 + n), slice(1, 1 + k)) if flags & TB else (slice(1, 1 + k), slice(1, 1 + n))
+    sc = (slice(1, 1 + m), slice(1, 1 + n))
+    A, B, C0 = Abig[sa], Bbig[sb], Cbig[sc].copy()
+    assert gpu.Mult(Cg[sc], Ag[sa], Bg[sb], 0.75, 1.25, flags) is None
+    opA = A.T if flags & TA else A
+    opB = B.T if flags & TB else B
+    Cr = 1.25 * C0 + 0.75 * (opA @ opB)
+    out = host(Cg)
+    assert fro(out[sc] - Cr) <= gemm_bound(k, 0.75, 1.25, A, B, C0)
+    keep = np.ones(out.shape, bool)
+    keep[sc] = False
+    assert np.array_equal(out[keep], Cbig[keep])
 
 
 @pytest.mark.parametrize("off", [(0, 0), (1, 0), (0, 1), (1, 1), (3, 5)])
