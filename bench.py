@@ -4,9 +4,10 @@ refinement against the plain FP64 path on the same system.
 
 System: A = G*G^T/n + 0.5*I (G iid N(0,1), seed 2), B iid U[-1,1] (seed 3), generated on
 the device.  Through the C ABI (libmatops_b200.so):
-  headline step  SolveCHOLMixed: TF32x3 split-product Cholesky on the tensor cores (FP64
-                 diagonal blocks), FP64 residuals and updates until the normwise backward
-                 error is <= 1e-14 (A is read, not modified; 2 GiB > L2 per step)
+  headline step  SolveCHOLMixed: BF16x3 split-product Cholesky on the tensor cores (FP32
+                 accumulation and storage, FP64 diagonal blocks; --prec tf32x3 for the
+                 TF32 split), FP64 residuals and updates until the normwise backward error
+                 is <= 1e-14 (A is read, not modified; 2 GiB > L2 per step)
   fp64_path      DecomposeCHOL + SolveCHOL in FP64 on fresh copies of A
 
 Reported on one JSON line (rank 0):
@@ -50,6 +51,9 @@ def parse():
     ap.add_argument("--n", type=int, default=16384)
     ap.add_argument("--nrhs", type=int, default=64)
     ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--prec", default="bf16x3", choices=["tf32x3", "bf16x3"],
+                    help="split format of the headline's low-precision factor (BF16x3 measured "
+                         "35.8 ms vs TF32x3 37.2 ms at n=16384, both 3 corrections)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--case", default=None,
@@ -683,11 +687,12 @@ def main():
         "launches_per_step": sum(prof64.launches.values()),
     }
 
-    # ---- the headline: TF32x3 factor + FP64 refinement to berr <= 1e-14, same A and B ----
+    # ---- the headline: split-product factor + FP64 refinement to berr <= 1e-14, same A, B ----
+    hprec = mo.PREC_TF32X3 if args.prec == "tf32x3" else mo.PREC_BF16X3
     Xm = mo.matrix(n, nrhs)
 
     def mstep():
-        info, err = mo.SolveCHOLMixed(Xm, A0, B0, LOWER, mo.PREC_TF32X3, mo.IR_AUTO, 1e-14, 40)
+        info, err = mo.SolveCHOLMixed(Xm, A0, B0, LOWER, hprec, mo.IR_AUTO, 1e-14, 40)
         assert err is None and info.converged and not info.fallback, (err, info)
         return info
 
@@ -739,15 +744,19 @@ def main():
             if ln.startswith("traffic_over_algorithmic:"):
                 traffic = float(ln.split(":")[1]) * l_by / l_n
     roofline = {
-        "bound": "hbm", "kernel": "lp_gemm_tc_kernel (TF32x3 trailing updates and panels)",
+        "bound": "hbm", "kernel": f"lp_gemm_tc_kernel ({args.prec.upper()} trailing updates and panels)",
         "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
         "frac": achieved_gbs / hbm_peak, "traffic": traffic,
         "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)",
         "algorithmic_bytes_per_launch": l_by / l_n if l_n else None,
         "avg_launch_ms": l_ms / l_n if l_n else None,
-        "tensor": {"achieved_tflops": achieved_tf, "tf32_dense_peak_tflops": bf16_peak / 2,
-                   "frac": achieved_tf / (bf16_peak / 2),
-                   "peak_source": "half of MEASURED_PEAKS.json bf16_tflops (TF32 runs at half the BF16 rate)"},
+        "tensor": ({"achieved_tflops": achieved_tf, "tf32_dense_peak_tflops": bf16_peak / 2,
+                    "frac": achieved_tf / (bf16_peak / 2),
+                    "peak_source": "half of MEASURED_PEAKS.json bf16_tflops (TF32 runs at half the BF16 rate)"}
+                   if args.prec == "tf32x3" else
+                   {"achieved_tflops": achieved_tf, "bf16_dense_peak_tflops": bf16_peak,
+                    "frac": achieved_tf / bf16_peak,
+                    "peak_source": "MEASURED_PEAKS.json bf16_tflops"}),
         "share_of_step": l_ms / ms if ms else None,
         "per_class_ms_per_traced_step": {k: v / PT for k, v in prof.ms.items() if prof.launches[k]},
         "note": "achieved and per-class times come from 2 extra steps traced with CUDA events "
@@ -772,7 +781,7 @@ def main():
         def e2e_step():
             mo.UploadTriangle(Ad, Ah, LOWER)
             mo.Upload(Bd, Bh)
-            info, err = mo.SolveCHOLMixed(Xd, Ad, Bd, LOWER, mo.PREC_TF32X3, mo.IR_AUTO, 1e-14, 40)
+            info, err = mo.SolveCHOLMixed(Xd, Ad, Bd, LOWER, hprec, mo.IR_AUTO, 1e-14, 40)
             assert err is None and info.converged
             mo.Download(Xh, Xd)
 
@@ -869,9 +878,9 @@ def main():
         line = {
             "metric": METRIC, "value": ms * 1e-3, "unit": "s", "n_gpus": world, "steps": K,
             "warmup": W, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "tf32x3+f64", "data": "synthetic",
+            "vs_baseline": None, "dtype": f"{args.prec}+f64", "data": "synthetic",
             "config": {"workload": workload(n, nrhs), "n": n, "nrhs": nrhs,
-                       "factor": "TF32x3 split products, FP32 storage, FP64 128x128 diagonal blocks",
+                       "factor": f"{args.prec.upper()} split products, FP32 storage, FP64 128x128 diagonal blocks",
                        "refinement": "FP64 residual and update, classic IR / GMRES-IR (auto), tol 1e-14",
                        "l2": "A (2 GiB FP64) is re-read from HBM by every step (inputs > L2)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},

@@ -118,6 +118,7 @@ __device__ __forceinline__ void tri_syrk_update(double *S, int NP, int r0, int k
 // right of its diagonal, which are never read, and this keeps the unrolled body free of
 // divergent branches (measured 4.4x faster than guarding each update with lane >= j).
 // With `checked`, the column loop stops at the first NaN pivot and returns its index.
+// `col` is 2 x 32 doubles of shared memory (two alternating multiplier columns).
 template <bool checked>
 __device__ __forceinline__ int warp_potrf32(double (&r)[SUB], int lane, double *badv,
                                             double *col) {
@@ -138,13 +139,15 @@ __device__ __forceinline__ int warp_potrf32(double (&r)[SUB], int lane, double *
     }
     // the multipliers (zero on lanes <= k) go through shared memory: every lane reads the
     // column with broadcast loads that issue back to back, where a chain of shuffles would
-    // pay each shuffle's latency in turn
+    // pay each shuffle's latency in turn.  Columns alternate between two buffers, so the
+    // next column's store need not wait for every lane to finish reading this one (the
+    // __syncwarp of column k + 1 orders column k's reads before column k + 2's stores).
+    double *c = col + (k & 1) * SUB;
     const double lk = lane > k ? r[k] * rs : 0.0;
-    col[lane] = lk;
+    c[lane] = lk;
     __syncwarp();
 #pragma unroll
-    for (int j = k + 1; j < SUB; ++j) r[j] = fma(-lk, col[j], r[j]);
-    __syncwarp();
+    for (int j = k + 1; j < SUB; ++j) r[j] = fma(-lk, c[j], r[j]);
     r[k] = lane == k ? sqrt(akk) : (lane > k ? lk : r[k]);
   }
   return bad;
@@ -162,7 +165,7 @@ __device__ __forceinline__ int warp_potrf32(double (&r)[SUB], int lane, double *
 __device__ inline void tri_potrf_lower(double *S, int NP, int *bad_col, double *bad_val) {
   __shared__ int s_bad;
   __shared__ double s_rd[SUB];
-  __shared__ double s_col[SUB];
+  __shared__ double s_col[2 * SUB];
   if (threadIdx.x == 0) s_bad = -1;
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;

@@ -34,6 +34,9 @@ constexpr int MAX_RHS = 64;
 #ifndef MO_FEW_GROUP
 #define MO_FEW_GROUP 32  // columns per group (measured: 32 beats 16 and 64 at n = 16384, 64 RHS)
 #endif
+#ifndef MO_PAIR_GROUP
+#define MO_PAIR_GROUP 32  // columns per group of the paired-step kernel (measured: 32 beats 64)
+#endif
 constexpr int LDL = TB + 4;   // smem row stride (== 4 mod 16 doubles: 2-way at most)
 
 struct FewArgs {
@@ -367,6 +370,8 @@ constexpr int pair_smem() {
   return 2 * TB * LDL * 8 + PAIR_CBLK * 4 + 2 * 2 * PAIR_CBLK * 4 + 2 * 8 * NT * (TB + 4) * 8;
 }
 
+static_assert(pair_smem<8>() <= 227 * 1024 - 64, "pair kernel shared memory");
+
 template <int NT>
 __global__ void __launch_bounds__(PAIR_THREADS, 1) trsm_pair_kernel(FewArgs p) {
   constexpr int LDXK = TB + 4;                        // X buffers: column-major 64 x 8NT
@@ -606,7 +611,9 @@ int few_run(mo_ctx *ctx, View B, const void *A, bool a32, int64_t lda, int N, in
   p.status = reinterpret_cast<int *>(ctx->d_status);
   // more than MO_FEW_GROUP columns: groups solved side by side by separate CTA sets, so
   // the per-step work on the dependency chain is that of one group
-  p.gw = nrhs > MO_FEW_GROUP ? MO_FEW_GROUP : nrhs;
+  const bool pair = a32 && p.nblk >= 4;
+  const int gmax = pair ? MO_PAIR_GROUP : MO_FEW_GROUP;
+  p.gw = nrhs > gmax ? gmax : nrhs;
   p.groups = (nrhs + p.gw - 1) / p.gw;
   MO_CUDA_TRY(cudaMemsetAsync(flag_buf, 0, sizeof(int) * p.nblk * p.groups * FLAG_STRIDE,
                               ctx->stream));
@@ -614,11 +621,12 @@ int few_run(mo_ctx *ctx, View B, const void *A, bool a32, int64_t lda, int N, in
   prof_begin(ctx, ps, a32 ? MO_PROF_IR : MO_PROF_GEMM);
   const int nt = (p.gw + 7) / 8;
   int rc;
-  if (a32 && p.nblk >= 4) {
+  if (pair) {
     // FP32 factor (the preconditioner of the mixed-precision solve): pairs of steps per CTA
     if (nt == 1) rc = launch_pair<1>(ctx, p);
     else if (nt == 2) rc = launch_pair<2>(ctx, p);
-    else rc = launch_pair<4>(ctx, p);
+    else if (nt <= 4) rc = launch_pair<4>(ctx, p);
+    else rc = launch_pair<8>(ctx, p);
   } else if (a32) {
     if (nt == 1) rc = launch_few<float, 1>(ctx, p);
     else if (nt == 2) rc = launch_few<float, 2>(ctx, p);
