@@ -738,7 +738,9 @@ def main():
     # capture summarized in profiles/lp_gemm_tc_kernel_traffic.md, times this run's
     # algorithmic bytes per launch
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "lp_gemm_tc_kernel_traffic.md")
+    tpath = os.path.join(ROOT, "profiles", f"lp_gemm_tc_kernel_traffic_{args.prec}.md")
+    if not os.path.exists(tpath):
+        tpath = os.path.join(ROOT, "profiles", "lp_gemm_tc_kernel_traffic.md")
     if os.path.exists(tpath) and l_n:
         for ln in open(tpath):
             if ln.startswith("traffic_over_algorithmic:"):
@@ -747,6 +749,7 @@ def main():
         "bound": "hbm", "kernel": f"lp_gemm_tc_kernel ({args.prec.upper()} trailing updates and panels)",
         "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
         "frac": achieved_gbs / hbm_peak, "traffic": traffic,
+        "traffic_source": os.path.relpath(tpath, ROOT) if traffic is not None else None,
         "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)",
         "algorithmic_bytes_per_launch": l_by / l_n if l_n else None,
         "avg_launch_ms": l_ms / l_n if l_n else None,

@@ -19,27 +19,30 @@ namespace {
 
 // Tile 128 x 128 of C per step of a persistent CTA; K consumed in stages of 128 bytes per
 // operand row (64 bf16 or 32 tf32 elements), four 16 KB parts per stage (A.hi, A.lo,
-// B.hi, B.lo) loaded by TMA with the 128-byte swizzle into a 3-deep ring.  Warp roles:
+// B.hi, B.lo) loaded by TMA with the 128-byte swizzle into a 2-deep ring.  Warp roles:
 //   warp 0    TMA producer (one thread)
 //   warp 1    TMEM owner (allocates 256 columns = two 128 x 128 FP32 accumulators) and
 //             MMA issuer (one thread): per 32-byte K step three tcgen05.mma -- hi*hi,
 //             hi*lo, lo*hi -- into the same accumulator; tcgen05.commit frees the smem
 //             stage, and after the tile's last stage signals the epilogue
-//   warps 2-5 epilogue: tcgen05.ld of their 32-lane quarter of the accumulator (TMEM lane
-//             = tile row), C = alpha * acc + beta * C, coalesced along the column
+//   warps 2-9 epilogue: tcgen05.ld of their 32-lane quarter of the accumulator (TMEM lane
+//             = tile row, quarter = warp % 4), C = alpha * acc + beta * C, coalesced along
+//             the column; warps 2-5 take the tile's columns 0-63, warps 6-9 columns 64-127
 // The accumulator is double-buffered, so the MMAs of tile t + 1 overlap the epilogue of
 // tile t.  C (FP32, column-major) moves through shared memory in two 64-column halves,
-// each with its own 32 KB buffer: the producer loads a half by TMA after the tile's
-// operand stages, the epilogue combines it with the accumulator in place and one thread
-// stores it back by TMA, so one half's transfer overlaps the other half's epilogue (when
-// C's base and leading dimension allow TMA; otherwise the epilogue reads and writes C
-// directly).  Every wait is bounded (MO_SPIN_LIMIT) and reports MO_EDEVTIMEOUT.
+// each with its own 32 KB buffer and its own four epilogue warps: the producer loads a
+// half by TMA after the tile's operand stages, that half's warps combine it with the
+// accumulator in place and one of their threads stores it back by TMA, so the two halves
+// and their transfers proceed side by side (when C's base and leading dimension allow
+// TMA; otherwise the epilogue reads and writes C directly).  Every wait is bounded
+// (MO_SPIN_LIMIT) and reports MO_EDEVTIMEOUT.
 constexpr int TB = 128;                  // tile rows = tile columns
 constexpr int TSTAGES = 2;
 constexpr int TPART = TB * 128;          // one operand part of a stage: 128 rows x 128 B
 constexpr int TSTAGE = 4 * TPART;        // 64 KB
 constexpr int TCTILE = TB * TB * 4;      // the C tile in shared memory (column-major FP32)
-constexpr int TTHREADS = 192;
+constexpr int TTHREADS = 320;
+constexpr int TEPI_WARPS = 8;            // epilogue warps (2-9), four per 64-column half
 constexpr int TSMEM = TSTAGES * TSTAGE + TCTILE + 1024 + 256;  // + alignment slack + barriers
 constexpr int TMEM_COLS = 256;
 
@@ -174,7 +177,7 @@ __global__ void __launch_bounds__(TTHREADS, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&tfull[b], 1);
-      mbar_init(&tempty[b], 4);
+      mbar_init(&tempty[b], TEPI_WARPS);
     }
     for (int h = 0; h < 2; ++h) {
       mbar_init(&cfull[h], 1);
@@ -266,10 +269,14 @@ __global__ void __launch_bounds__(TTHREADS, 1)
       if (ok) umma_commit(&tfull[buf]);
     }
   } else if (warp >= 2) {
-    // epilogue: warp w reads TMEM lanes 32 * (w % 4) .. + 31 (= tile rows)
+    // epilogue: warp w reads TMEM lanes 32 * (w % 4) .. + 31 (= tile rows) of the 64
+    // columns of half h = (w - 2) / 4
     const int q = warp & 3;
     const int rl = q * 32 + lane;
-    int tc = 0, cu[2] = {0, 0};  // cu: uses of each C half buffer
+    const int h = (warp - 2) >> 2;
+    const bool storer = (warp - 2) % 4 == 0;  // warps 2 and 6: one thread stores the half
+    float *const cb = ctile + h * TB * (TB / 2);  // this half: column-major 128 x 64
+    int tc = 0, cu = 0;  // cu: uses of this half's buffer
     for (int t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++tc) {
       int tm, tn;
       tile_coords(p, t, tm, tn);
@@ -277,15 +284,13 @@ __global__ void __launch_bounds__(TTHREADS, 1)
       if (!mbar_wait(&tfull[buf], (tc >> 1) & 1, p.status)) break;
       tc_fence_after();
       const int row = tm * TB + rl;
+      // the second half exists only if the tile has columns there (the producer decides
+      // the same way)
+      const bool live = h == 0 || tn * TB + TB / 2 < p.N;
       if (p.c_tma) {
-        const int nh = tn * TB + TB / 2 < p.N ? 2 : 1;
         bool fail = false;
-        for (int h = 0; h < nh && !fail; ++h) {
-          float *cb = ctile + h * TB * (TB / 2);  // this half: column-major 128 x 64
-          if (!mbar_wait(&cfull[h], cu[h] & 1, p.status)) {
-            fail = true;
-            break;
-          }
+        if (live) {
+          if (!mbar_wait(&cfull[h], cu & 1, p.status)) break;
 #pragma unroll 1
           for (int c0 = h * (TB / 2); c0 < (h + 1) * (TB / 2); c0 += 16) {
             uint32_t v[16];
@@ -299,66 +304,67 @@ __global__ void __launch_bounds__(TTHREADS, 1)
               if (p.mode != kGemmLower || row >= col) *cs = nv;
             }
           }
-          // split copy of this thread's row (it wrote that row of the half itself)
-          if (p.shi != nullptr && row < p.M && row >= p.srow0) {
-            constexpr int ES = PREC == kLpBf16x3 ? 2 : 4;
-            const int64_t obase = ((int64_t)(row - p.srow0) * p.sldk + tn * TB) * ES;
-#pragma unroll 1
-            for (int c0 = h * (TB / 2); c0 < (h + 1) * (TB / 2) && tn * TB + c0 < p.N; c0 += 8) {
-              float x[8];
-#pragma unroll
-              for (int u = 0; u < 8; ++u)
-                x[u] = tn * TB + c0 + u < p.N ? cb[(c0 - h * (TB / 2) + u) * TB + rl] : 0.f;
-              if (PREC == kLpBf16x3) {
-                __align__(16) __nv_bfloat16 hh[8], ll[8];
-#pragma unroll
-                for (int u = 0; u < 8; ++u) split_bf16(x[u], hh[u], ll[u]);
-                *reinterpret_cast<uint4 *>(p.shi + obase + c0 * ES) = *reinterpret_cast<const uint4 *>(hh);
-                *reinterpret_cast<uint4 *>(p.slo + obase + c0 * ES) = *reinterpret_cast<const uint4 *>(ll);
-              } else {
-                __align__(16) uint32_t hh[8], ll[8];
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                  hh[u] = to_tf32(x[u]);
-                  ll[u] = to_tf32(x[u] - __uint_as_float(hh[u]));
-                }
-#pragma unroll
-                for (int v = 0; v < 2; ++v) {
-                  *reinterpret_cast<uint4 *>(p.shi + obase + (c0 + 4 * v) * ES) =
-                      *reinterpret_cast<const uint4 *>(hh + 4 * v);
-                  *reinterpret_cast<uint4 *>(p.slo + obase + (c0 + 4 * v) * ES) =
-                      *reinterpret_cast<const uint4 *>(ll + 4 * v);
-                }
-              }
-            }
-          }
-          if (h == nh - 1) {  // the accumulator has been read out
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&tempty[buf]);
-          }
-          // the four epilogue warps' shared-memory writes, then one TMA store of the half
-          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&cready[h]);
-          if (warp == 2) {
-            int ok = 1;
-            if (lane == 0) {
-              ok = mbar_wait(&cready[h], cu[h] & 1, p.status) ? 1 : 0;
-              if (ok) {
-                tma_store_2d(&tC, cb, tm * TB, tn * TB + h * (TB / 2));
-                mbar_arrive(&cempty[h]);
-              }
-            }
-            if (!__shfl_sync(0xffffffffu, ok, 0)) fail = true;  // warp-uniform exit
-          }
-          ++cu[h];
         }
+        // the accumulator has been read out (every epilogue warp arrives, live or not)
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&tempty[buf]);
+        if (!live) continue;
+        // split copy of this thread's row (it wrote that row of the half itself)
+        if (p.shi != nullptr && row < p.M && row >= p.srow0) {
+          constexpr int ES = PREC == kLpBf16x3 ? 2 : 4;
+          const int64_t obase = ((int64_t)(row - p.srow0) * p.sldk + tn * TB) * ES;
+#pragma unroll 1
+          for (int c0 = h * (TB / 2); c0 < (h + 1) * (TB / 2) && tn * TB + c0 < p.N; c0 += 8) {
+            float x[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+              x[u] = tn * TB + c0 + u < p.N ? cb[(c0 - h * (TB / 2) + u) * TB + rl] : 0.f;
+            if (PREC == kLpBf16x3) {
+              __align__(16) __nv_bfloat16 hh[8], ll[8];
+#pragma unroll
+              for (int u = 0; u < 8; ++u) split_bf16(x[u], hh[u], ll[u]);
+              *reinterpret_cast<uint4 *>(p.shi + obase + c0 * ES) = *reinterpret_cast<const uint4 *>(hh);
+              *reinterpret_cast<uint4 *>(p.slo + obase + c0 * ES) = *reinterpret_cast<const uint4 *>(ll);
+            } else {
+              __align__(16) uint32_t hh[8], ll[8];
+#pragma unroll
+              for (int u = 0; u < 8; ++u) {
+                hh[u] = to_tf32(x[u]);
+                ll[u] = to_tf32(x[u] - __uint_as_float(hh[u]));
+              }
+#pragma unroll
+              for (int v = 0; v < 2; ++v) {
+                *reinterpret_cast<uint4 *>(p.shi + obase + (c0 + 4 * v) * ES) =
+                    *reinterpret_cast<const uint4 *>(hh + 4 * v);
+                *reinterpret_cast<uint4 *>(p.slo + obase + (c0 + 4 * v) * ES) =
+                    *reinterpret_cast<const uint4 *>(ll + 4 * v);
+              }
+            }
+          }
+        }
+        // this half's four warps' shared-memory writes, then one TMA store of the half
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&cready[h]);
+        if (storer) {
+          int ok = 1;
+          if (lane == 0) {
+            ok = mbar_wait(&cready[h], cu & 1, p.status) ? 1 : 0;
+            if (ok) {
+              tma_store_2d(&tC, cb, tm * TB, tn * TB + h * (TB / 2));
+              mbar_arrive(&cempty[h]);
+            }
+          }
+          if (!__shfl_sync(0xffffffffu, ok, 0)) fail = true;  // warp-uniform exit
+        }
+        ++cu;
         if (fail) break;
       } else {
+        // C read and written in place: this warp's 64 columns
         const bool rok = row < p.M;
 #pragma unroll 1
-        for (int c0 = 0; c0 < TB; c0 += 16) {
+        for (int c0 = h * (TB / 2); c0 < (h + 1) * (TB / 2); c0 += 16) {
           float cv[16];
 #pragma unroll
           for (int r = 0; r < 16; ++r) {
@@ -379,8 +385,9 @@ __global__ void __launch_bounds__(TTHREADS, 1)
         if (lane == 0) mbar_arrive(&tempty[buf]);
       }
     }
-    // the last tile's store has been read out of shared memory; let it reach global memory
-    if (warp == 2 && lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    // the last store of this half has been read out of shared memory; let it reach
+    // global memory
+    if (storer && lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
   }
   tc_fence_before();
   __syncthreads();
