@@ -803,7 +803,7 @@ def main():
         e2e = {"value": e_ms * 1e-3, "unit": "s", "h2d_bytes_per_step": 8 * (tri_elems + n * nrhs),
                "d2h_bytes_per_step": 8 * n * nrhs, "steps": ke,
                "what": "pinned host A, B -> upload (A: its lower triangle, the part the solver "
-                       "reads), SolveCHOLMixed (TF32x3 + FP64 refinement), download X"}
+                       f"reads), SolveCHOLMixed ({args.prec.upper()} + FP64 refinement), download X"}
         del Ah, Bh, Ad, Bd, Xd, Xh
 
     # ---- extras: DGEMM 2048^3 and LU at n ----
