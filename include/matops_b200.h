@@ -118,8 +118,10 @@ MO_API int mo_malloc(mo_ctx *ctx, void **ptr, size_t bytes);
 MO_API int mo_free(mo_ctx *ctx, void *ptr);
 /* copy a host column-major matrix (leading dim ld_src) into the device view dst */
 MO_API int mo_upload(mo_ctx *ctx, mo_matrix dst, const double *src, int64_t ld_src);
-/* copy only the triangle that flags selects (MO_LOWER default, MO_UPPER) of a square host
- * matrix into the square device view dst, in 128-column blocks that also carry the rest
+/* No counterpart in the reference (a host -> device helper for shims that hold host
+ * matrices, like mo_upload): copy only the triangle that flags selects (MO_LOWER
+ * default, MO_UPPER) of a square host matrix into the square device view dst, in
+ * 128-column blocks that also carry the rest
  * of each 128 x 128 diagonal block: about n (n + 128) / 2 elements instead of n^2, for
  * the symmetric entry points that read one triangle.  The other triangle of dst is left
  * as it was.  Asynchronous on the context's stream. */
