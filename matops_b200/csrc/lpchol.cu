@@ -240,7 +240,9 @@ int lp_chol_factor(mo_ctx *ctx, LpChol &f, int *d_info, double *d_bad) {
   cudaStream_t s0 = ctx->stream, s1 = nullptr;
   if ((rc = aux_stream(ctx, &s1))) return rc;
   if ((rc = stream_wait(ctx, s1, s0, ctx->ev_fork))) return rc;
-  const int free_sms = 8;
+  // SMs the trailing update leaves to the look-ahead stream (diagonal block + panel);
+  // measured at n = 16384: 2 -> 34.26 ms, 8 -> 34.4 ms, 16 -> 34.82 ms per solve
+  const int free_sms = 2;
   {
     StreamSwap sw(ctx, s1);
     if ((rc = lp_panel(ctx, f, 0, d_info, d_bad, f.P[0]))) return rc;
