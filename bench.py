@@ -481,28 +481,82 @@ def scaled_cpu_seconds(n, n_s, tf, ts):
     return tf * (n / n_s) ** 3 + ts * (n / n_s) ** 2
 
 
+def reference_inputs(n, nrhs):
+    """The headline system for the CPU arm, column-major float64 host arrays: A = G G^T/n +
+    0.5 I (G iid N(0,1), seed 2) and B iid U[-1,1] (seed 3).  G G^T is formed on the GPU
+    when one is present (torch, input preparation only: nothing of this repository's engine
+    runs on the reference arm), else by numpy."""
+    import numpy as np
+    g = np.random.default_rng(2).standard_normal((n, n))
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError
+        gt = torch.from_numpy(g).cuda()
+        a = (gt @ gt.T / n).cpu().numpy()
+        del gt
+        torch.cuda.empty_cache()
+    except Exception:
+        a = g @ g.T / n
+    del g
+    a[np.diag_indices(n)] += 0.5
+    A = np.asfortranarray(a)
+    del a
+    B = np.asfortranarray(np.random.default_rng(3).uniform(-1, 1, (nrhs, n)).T)
+    return A, B
+
+
 def run_reference(args, rank):
+    """The reference's own CPU path (oracle/_ref: its calgo C kernels under the Go driver
+    bodies restated in C; NumWorkers = host cores, nb = 64): ONE full DecomposeCHOL +
+    SolveCHOL at the configured n, timed in K slices.  Step k runs the block steps of
+    blockedCHOL (chol.go:58-94) whose first column lies in slice k of [0, n); the last step
+    also runs SolveCHOL (chol.go:147-158).  The K slices run in order on the same matrix, so
+    together they are exactly one factor + solve; value = their summed wall time.  Warm-up
+    steps factor a separate n = 1024 system."""
     if rank != 0:
         return 0
-    n_s = min(args.n, 3072)
+    import numpy as np
+
+    from oracle.oracle import Oracle, ref_available
+    kind = "reference" if ref_available() else "port"
+    orc = Oracle("ref" if kind == "reference" else "port")
+    cores = os.cpu_count() or 1
+    orc.NumWorkers(cores)  # the reference parallelizes only Mult (mmult.go:241-255)
+    n, nrhs, nb, K = args.n, args.nrhs, 64, args.steps
+    for _ in range(args.warmup):
+        Aw, Bw = reference_inputs(1024, nrhs)
+        assert orc.DecomposeCHOL(Aw, LOWER, nb) == 0
+        orc.SolveCHOL(Bw, Aw, LOWER)
+    A, B = reference_inputs(n, nrhs)
+    nblk = (n + nb - 1) // nb
+    bounds = [nb * ((nblk * k) // K) for k in range(K)] + [n]
     times = []
-    for i in range(args.warmup + args.steps):
-        tf, ts, kind, cores = cpu_sample(n_s, args.nrhs, 1)
-        if i >= args.warmup:
-            times.append(scaled_cpu_seconds(args.n, n_s, tf, ts))
-    v = sum(times) / len(times)
-    sample = (f"DecomposeCHOL+SolveCHOL at n={n_s}, {args.nrhs} RHS per step; factor time "
-              f"scaled by (n/{n_s})^3, solve by (n/{n_s})^2 to n={args.n}")
+    for k in range(K):
+        t0 = time.perf_counter()
+        if bounds[k] < bounds[k + 1]:
+            assert orc.DecomposeCHOLSteps(A, LOWER, nb, bounds[k], bounds[k + 1]) == 0
+        if k == K - 1:
+            orc.SolveCHOL(B, A, LOWER)
+        times.append(time.perf_counter() - t0)
+    v = sum(times)
+    X = B
+    del A
+    sample = (f"one full DecomposeCHOL+SolveCHOL at n={n}, nb={nb}, {nrhs} RHS, timed in "
+              f"{K} consecutive slices of blockedCHOL's block steps (the last one with the "
+              f"solve); value = the sum")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
+        "steps": K, "warmup": args.warmup, "ms_per_step": v * 1e3 / K,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": workload(args.n, args.nrhs), "n": args.n, "nrhs": args.nrhs,
-                   "nb": 64, "parallelism": "host cores"},
-        "cpu_baseline": {"value": v, "unit": "s", "cores": cores, "kind": kind, "sample": sample,
-                         "num_workers": os.cpu_count()},
+        "config": {"workload": workload(n, nrhs), "n": n, "nrhs": nrhs, "nb": nb,
+                   "parallelism": "host cores (only Mult is threaded in the reference)"},
+        "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "kind": kind, "sample": sample,
+                         "num_workers": cores},
         "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "step_s": times,
+        "x_norm": float(np.linalg.norm(X)),
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -667,6 +721,12 @@ def main():
     barrier()
     fp64_ms = max_over_ranks(e0.elapsed_time(e1) / K)
     X = Bs[nsteps - 1]
+    # parity at the configured order: ||A - L L^T||_F / ||A||_F of the FP64 factor (torch
+    # matmul as the checker)
+    Lf = torch.tril(As[nsteps - 1] if fresh else As[0])
+    parity = {"chol_residual": float(torch.linalg.norm(A0 - Lf @ Lf.T) / torch.linalg.norm(A0)),
+              "bound_10n_eps": 10 * n * 2.0 ** -52}
+    del Lf
     R = B0.clone()
     assert mo.Mult(R, A0, X, -1.0, 1.0, 0) is None
     fp64_berr = float(R.norm() / (A0.norm() * X.norm() + B0.norm()))
@@ -833,15 +893,16 @@ def main():
         extras["dgemm_2048"] = {"ms": gm, "tflops": gtf, "frac_fp64_peak": gtf / fp64_peak,
                                 "alpha": 1.5, "beta": -0.5, "l2": "flushed (256 MiB write) between calls"}
         del Ag, Bg, Cg, flush
-        # LU + SolveLU at n (N(0,1) seed 4; 64 RHS U[-1,1] seed 5)
-        L0 = mo.matrix(n, n)
-        L0.normal_(generator=torch.Generator(device=dev).manual_seed(4))
-        Lb0 = mo.matrix(n, nrhs)
-        Lb0.uniform_(-1.0, 1.0, generator=torch.Generator(device=dev).manual_seed(5))
+        # LU + SolveLU at n on the reference's golden input (numpy PCG64 seed 4, column by
+        # column; 64 RHS U[-1,1] seed 5): the pivot vector is compared with the reference's
+        # own run (tests/golden/n16384.npz) and ||PA - LU|| is checked with torch matmul
+        import numpy as np
+        L0 = mo.to_device(np.random.default_rng(4).standard_normal((n, n)).T)
+        Lb0 = mo.to_device(np.random.default_rng(5).uniform(-1, 1, (nrhs, n)).T)
         LA, LB = mo.matrix(n, n), mo.matrix(n, nrhs)
         piv = torch.zeros(n, dtype=torch.int64, device=dev)
         lts = []
-        for it in range(2):
+        for it in range(3):
             LA.copy_(L0)
             LB.copy_(Lb0)
             torch.cuda.synchronize()
@@ -856,13 +917,37 @@ def main():
         R = Lb0.clone()
         mo.Mult(R, L0, LB, -1.0, 1.0, 0)
         lberr = float(R.norm() / (L0.norm() * LB.norm() + Lb0.norm()))
-        lms = min(lts)
+        lms = min(lts[1:])
         extras["lu_16384"] = {"s": lms * 1e-3, "factor_tflops": 2 * n ** 3 / 3 / (lms * 1e-3) / 1e12,
                               "berr": lberr}
-        del L0, Lb0, LA, LB, R
+        pv = piv.cpu().numpy()
+        perm = np.arange(n)
+        for k in range(n):  # row interchanges in order (pivot.go:55-61)
+            j = int(pv[k])
+            perm[k], perm[j] = perm[j], perm[k]
+        del R
+        Lu = torch.tril(LA, -1)
+        Lu.diagonal().fill_(1.0)
+        parity["lu_residual"] = float(torch.linalg.norm(L0[torch.from_numpy(perm).to(dev)] - Lu @ torch.triu(LA))
+                                      / torch.linalg.norm(L0))
+        del Lu
+        gpath = os.path.join(ROOT, "tests", "golden", "n16384.npz")
+        if os.path.exists(gpath):
+            gold = np.load(gpath)
+            if int(gold["n"]) == n:
+                d = np.flatnonzero(pv != gold["lu_piv"])
+                parity["lu_pivots_vs_reference"] = {
+                    "identical": bool(d.size == 0), "differing": int(d.size),
+                    "reference": "tests/golden/n16384.npz (oracle/_ref DecomposeLU, nb=64)"}
+        del L0, Lb0, LA, LB
         torch.cuda.empty_cache()
-        extras["mixed_ir"] = mixed_leg(mo, n, 16, [1e2, 1e6, 1e10],
-                                       [mo.PREC_TF32X3, mo.PREC_BF16X3], dev)
+        # the mixed-precision configuration: n in {8192, 16384}, 16 RHS, kappa sweep, both
+        # split formats (A = Q diag(s) Q^T, Q from Householder QR, s log-spaced 1..kappa)
+        extras["mixed_ir"] = {}
+        for nm in sorted({min(8192, n), n}):
+            extras["mixed_ir"][f"n={nm}"] = mixed_leg(mo, nm, 16, [1e2, 1e6, 1e10],
+                                                      [mo.PREC_TF32X3, mo.PREC_BF16X3], dev)
+            torch.cuda.empty_cache()
         torch.cuda.empty_cache()
         extras["batched_chol_4096"], _ = batched_leg(mo, mo.BATCH_CHOL, 4096, 8, dev, reps=3)
         extras["batched_lu_4096"], _ = batched_leg(mo, mo.BATCH_LU, 4096, 9, dev, reps=3)
@@ -877,7 +962,8 @@ def main():
         cpu = {"value": scaled_cpu_seconds(n, n_s, tf, ts_), "unit": "s", "cores": cores,
                "kind": kind, "num_workers": os.cpu_count(),
                "sample": f"DecomposeCHOL+SolveCHOL at n={n_s}, {nrhs} RHS, best of 2; factor "
-                         f"scaled by (n/{n_s})^3 and solve by (n/{n_s})^2 to n={n}",
+                         f"scaled by (n/{n_s})^3 and solve by (n/{n_s})^2 to n={n} (a bounded "
+                         f"sample; `bench.py --impl reference` times one full n={n} solve)",
                "sample_s": tf + ts_}
 
     if rank == 0:
@@ -893,7 +979,7 @@ def main():
             "berr": berr, "berr_inf": max(i.berr for i in infos),
             "ir_iters": [i.iters for i in infos], "gmres_iters": [i.gmres_iters for i in infos],
             "ir_berr_history": infos[0].history,
-            "fp64_path": fp64_path, "speedup_vs_fp64": fp64_ms / ms,
+            "fp64_path": fp64_path, "speedup_vs_fp64": fp64_ms / ms, "parity": parity,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(sum(timed_launches.values())),
             "gpu_launches_by_class": timed_launches,

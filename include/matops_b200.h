@@ -47,7 +47,7 @@ extern "C" {
 #define MO_OK 0
 #define MO_ESIZE (-1)        /* "Mult: size mismatch"                    mmult.go:224 */
 #define MO_ENOTSQUARE (-2)   /* "A not a square matrix"                  chol.go:119 */
-#define MO_EPIVLEN (-3)      /* "pivot array < min(A.Rows(),A.Cols())"    lu.go:424 */
+#define MO_EPIVLEN (-3)      /* "pivot array < min(A.Rows(),A.Cols())"    lu.go:260-262 */
 #define MO_ECNOTSQUARE (-4)  /* "C not a square matrix"                  mmult.go:428 */
 #define MO_EABSIZE (-5)      /* "A, B size mismatch"                     mmult.go:406 */
 #define MO_EINVAL (-10)      /* NULL context/pointer, negative size, ld < rows        */
@@ -87,6 +87,15 @@ MO_API int mo_num_workers(mo_ctx *ctx, int n);
  * reference's behaviour, beta only inside the nb x nb diagonal blocks (calgo/dmmat_rank.c:
  * 28-56 vs 96-121).  Returns the old value. */
 MO_API int mo_set_syrk_blas_beta(mo_ctx *ctx, int on);
+/* No counterpart in the reference (its calls cannot wait on another thread of work): the
+ * number of polls a device-side wait on another CTA's step flag makes before it gives up
+ * and records MO_EDEVTIMEOUT (the triangular solves with at most 64 right-hand sides, i.e.
+ * SolveCHOL / SolveTrm with few columns and the refinement of mo_dsposv_ir).  Default
+ * MO_SPIN_LIMIT_DEFAULT; a failing wait ends its kernel early, leaves no copy in flight and
+ * the context stays usable (mo_sync returns MO_EDEVTIMEOUT once, the next call runs
+ * normally).  *old (optional) receives the previous value. */
+#define MO_SPIN_LIMIT_DEFAULT (1u << 26)
+MO_API int mo_set_spin_limit(mo_ctx *ctx, uint32_t polls, uint32_t *old);
 
 /* ---- tracing: per-kernel-class device time (CUDA events on the context's stream) ---- */
 #define MO_PROF_GEMM 0     /* DMMA GEMM / SYRK engine (trailing updates, TRSM sweeps)  */
@@ -169,14 +178,14 @@ MO_API int mo_decompose_chol(mo_ctx *ctx, mo_matrix A, int flags, int nb, double
  * mo_decompose_chol (MO_UPPER checked first, then MO_LOWER; neither -> no-op). */
 MO_API int mo_solve_chol(mo_ctx *ctx, mo_matrix B, mo_matrix A, int flags);
 
-/* DecomposeLU(A, pivots, nb), lu.go:420-436: P*A = L*U with partial pivoting, L unit lower
+/* DecomposeLU(A, pivots, nb), lu.go:257-272: P*A = L*U with partial pivoting, L unit lower
  * (diagonal not stored), in place.  pivots: device int64 array of npiv entries; on return
  * pivots[k] is the 0-based absolute row swapped with row k (pivots[k] == k: no swap),
  * entries >= min(rows,cols) are set to 0.  npiv < min(rows,cols) -> MO_EPIVLEN.  The pivot
  * at each column is the first row holding the largest |value| (pivot.go:98-107). */
 MO_API int mo_decompose_lu(mo_ctx *ctx, mo_matrix A, int64_t *pivots, int64_t npiv, int nb);
 
-/* SolveLU(B, A, pivots, flags), lu.go:483-497: apply the row swaps to B in forward order
+/* SolveLU(B, A, pivots, flags), lu.go:320-334: apply the row swaps to B in forward order
  * (pivot.go:55-61), then B = U^-1 L^-1 B; with MO_TRANSA the same swaps followed by
  * L^-T then U^-T, exactly the reference's sequence. */
 MO_API int mo_solve_lu(mo_ctx *ctx, mo_matrix B, mo_matrix A, const int64_t *pivots, int64_t npiv,
@@ -249,7 +258,7 @@ MO_API int mo_solve_chol_adjoint(mo_ctx *ctx, mo_matrix L, mo_matrix X, mo_matri
 
 /* ---- batched factor + solve of many small systems (no counterpart in the reference,
  * which factors one matrix per call: DecomposeCHOL chol.go:116 / SolveCHOL chol.go:147,
- * DecomposeLU lu.go:420 / SolveLU lu.go:483; each matrix gets the same results those
+ * DecomposeLU lu.go:257 / SolveLU lu.go:320; each matrix gets the same results those
  * calls give, to rounding, and the same pivots) ---- */
 #define MO_BATCH_CHOL 1     /* A_i = L_i L_i^T (lower; the strict upper part is not read) */
 #define MO_BATCH_LU 2       /* P_i A_i = L_i U_i with partial pivoting                    */
@@ -300,8 +309,9 @@ MO_API int mo_batch_schedule(mo_batch *plan, int *cfg, int set);
  *     and waits for it; returns 0, a size error, or a device-side failure code.
  *   - every call on a device uses the same block, which keeps the previous call's data:
  *     calls that overlap on the GPU race; serialize them.
- *   - the first call on each device looks the block up with that device current; make it
- *     before any stream capture begins. */
+ *   - every call looks the block's device address up with the caller's device current
+ *     (allocating nothing); the first call on a device also loads this library's kernels
+ *     there, so make it before any stream capture begins. */
 MO_API int mo_solve_trm_static(mo_matrix B, mo_matrix A, double alpha, int flags, void *stream);
 
 #ifdef __cplusplus

@@ -54,6 +54,7 @@ def lib() -> ctypes.CDLL:
         "mo_blocking_params": [p, i, i, i],
         "mo_num_workers": [p, i],
         "mo_set_syrk_blas_beta": [p, i],
+        "mo_set_spin_limit": [p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)],
         "mo_malloc": [p, ctypes.POINTER(p), sz],
         "mo_free": [p, p],
         "mo_upload": [p, M, p, i64],

@@ -151,7 +151,7 @@ def SolveCHOL(B, A, flags: int) -> None:
 
 
 def DecomposeLU(A, pivots: torch.Tensor, nb: int):
-    """lu.go:420 -- returns (A, err); pivots is a CUDA int64 tensor (0-based rows)."""
+    """lu.go:257 -- returns (A, err); pivots is a CUDA int64 tensor (0-based rows)."""
     if pivots.dtype != torch.int64 or not pivots.is_cuda or not pivots.is_contiguous():
         raise TypeError("pivots must be a contiguous CUDA int64 tensor")
     rc = _lib.lib().mo_decompose_lu(context(), view(A), ctypes.c_void_p(pivots.data_ptr()),
@@ -160,7 +160,7 @@ def DecomposeLU(A, pivots: torch.Tensor, nb: int):
 
 
 def SolveLU(B, A, pivots: torch.Tensor, flags: int):
-    """lu.go:483 -- apply the interchanges, then the two triangular solves."""
+    """lu.go:320 -- apply the interchanges, then the two triangular solves."""
     if pivots.dtype != torch.int64 or not pivots.is_cuda or not pivots.is_contiguous():
         raise TypeError("pivots must be a contiguous CUDA int64 tensor")
     rc = _lib.lib().mo_solve_lu(context(), view(B), view(A), ctypes.c_void_p(pivots.data_ptr()),
@@ -227,6 +227,16 @@ def LPGemm(C, A, B, alpha: float, beta: float, flags: int = NOTRANS, prec: int =
     (pa, lda), (pb, ldb), (pc, ldc) = _fview(A), _fview(B), _fview(C)
     return _err(_lib.lib().mo_lp_gemm(context(), prec, m, n, k, alpha, pa, lda, pb, ldb, beta, pc,
                                       ldc, flags))
+
+
+def SetSpinLimit(polls: int) -> int:
+    """Polls a device-side wait on another CTA's step flag makes before it gives up with
+    MO_EDEVTIMEOUT (see mo_set_spin_limit); returns the previous value."""
+    old = ctypes.c_uint32(0)
+    rc = _lib.lib().mo_set_spin_limit(context(), polls, ctypes.byref(old))
+    if rc:
+        raise RuntimeError(_lib.lib().mo_strerror(rc).decode())
+    return old.value
 
 
 def Sync() -> int:

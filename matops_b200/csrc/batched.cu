@@ -1,7 +1,7 @@
 // Batched Cholesky / LU factor + solve of many small FP64 systems of uneven order
 // (n <= MO_BATCH_MAX_N) in one persistent launch per schedule group, replayed from a CUDA
 // graph.  The reference factors one matrix per call (DecomposeCHOL chol.go:116,
-// DecomposeLU lu.go:420, SolveCHOL chol.go:147, SolveLU lu.go:483); here each CTA takes
+// DecomposeLU lu.go:257, SolveCHOL chol.go:147, SolveLU lu.go:320); here each CTA takes
 // whole matrices from a work queue ordered by decreasing n^3 (longest job first) and
 // runs, for each one:
 //
@@ -459,7 +459,7 @@ __device__ int lu_matrix(Smem<NB> &s, double *A, int64_t ld, int n, int64_t *piv
 
 // Solve with the factor of one matrix, right-hand side by right-hand side, in 32-row
 // blocks.  CHOL: L L^T x = b (SolveCHOL LOWER, chol.go:147-158).  LU: P A = L U, x = U^-1
-// L^-1 P b (SolveLU, lu.go:483-497; P b gathered through the row map s.perm).
+// L^-1 P b (SolveLU, lu.go:320-334; P b gathered through the row map s.perm).
 template <bool LU, int NB>
 __device__ void solve_matrix(Smem<NB> &s, const double *A, int64_t ld, int n, double *B,
                              int64_t ldb, int nrhs) {

@@ -233,6 +233,13 @@ int mo_set_syrk_blas_beta(mo_ctx *ctx, int on) {
   return old;
 }
 
+int mo_set_spin_limit(mo_ctx *ctx, uint32_t polls, uint32_t *old) {
+  if (!ctx) return MO_EINVAL;
+  if (old) *old = ctx->spin_limit;
+  ctx->spin_limit = polls;
+  return MO_OK;
+}
+
 int mo_malloc(mo_ctx *ctx, void **ptr, size_t bytes) {
   int rc = mo::enter(ctx);
   if (rc) return rc;
@@ -442,7 +449,7 @@ int mo_solve_chol(mo_ctx *ctx, mo_matrix Bm, mo_matrix Am, int flags) {
   return MO_OK;
 }
 
-// lu.go:420-436
+// lu.go:257-272
 int mo_decompose_lu(mo_ctx *ctx, mo_matrix Am, int64_t *piv, int64_t npiv, int nb) {
   int rc = mo::enter(ctx);
   if (rc) return rc;
@@ -456,7 +463,7 @@ int mo_decompose_lu(mo_ctx *ctx, mo_matrix Am, int64_t *piv, int64_t npiv, int n
   return mo::getrf(ctx, A, piv, npiv, nb);
 }
 
-// lu.go:483-497
+// lu.go:320-334
 int mo_solve_lu(mo_ctx *ctx, mo_matrix Bm, mo_matrix Am, const int64_t *piv, int64_t npiv,
                 int flags) {
   int rc = mo::enter(ctx);

@@ -10,7 +10,7 @@
 // Bounded spin: every wait in these kernels gives up after this many polls, records
 // MO_EDEVTIMEOUT in the context's device status word and returns.
 #ifndef MO_SPIN_LIMIT
-#define MO_SPIN_LIMIT (1u << 26)
+#define MO_SPIN_LIMIT MO_SPIN_LIMIT_DEFAULT
 #endif
 
 namespace mo {
@@ -112,6 +112,15 @@ __device__ __forceinline__ void dmma_16x8x4(double (&d)[4], double a0, double a1
     cudaError_t _e = (expr);                               \
     if (_e != cudaSuccess) return mo_from_cuda_error(_e);  \
   } while (0)
+
+// Sets the dynamic shared-memory limit of a kernel before its launch.  Called on every
+// launch (a cheap host call) rather than cached per device, so that it holds after a
+// context reset and needs no shared state between host threads.
+static inline int mo_smem_attr(const void *fn, int bytes) {
+  const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaErrorMemoryAllocation) return MO_ENOMEM;
+  return e == cudaSuccess ? MO_OK : MO_ECUDA;
+}
 
 static inline int mo_from_cuda_error(cudaError_t e) {
   if (e == cudaErrorMemoryAllocation) return MO_ENOMEM;

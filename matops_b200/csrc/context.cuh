@@ -14,6 +14,9 @@ struct mo_ctx {
   int mb = 68, nb = 68, kb = 196;  // BlockingParams (mmult.go:33-35)
   int workers = 1;                 // NumWorkers (mmult.go:38)
   int syrk_blas_beta = 0;
+  // polls of a flag that the few-right-hand-side triangular solve makes before it gives up
+  // (mo_set_spin_limit); the mbarrier waits of the TMA pipelines keep MO_SPIN_LIMIT
+  uint32_t spin_limit = MO_SPIN_LIMIT;
   // scratch owned by the context (grown on demand, freed in mo_ctx_destroy)
   void *ws = nullptr;
   size_t ws_bytes = 0;

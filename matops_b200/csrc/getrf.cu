@@ -249,7 +249,7 @@ int laswp(mo_ctx *ctx, View A, int c0, int c1, const int64_t *piv, int ns, int64
   return MO_OK;
 }
 
-// SolveLU's applyPivots(B, pivots) (lu.go:485, pivot.go:55-61)
+// SolveLU's applyPivots(B, pivots) (lu.go:322, pivot.go:55-61)
 int laswp_forward(mo_ctx *ctx, View B, const int64_t *piv, int64_t npiv) {
   if (B.rows == 0 || B.cols == 0 || npiv <= 0) return MO_OK;
   if (npiv > INT_MAX) return MO_EINVAL;
@@ -345,7 +345,7 @@ int getrf(mo_ctx *ctx, View A, int64_t *piv, int64_t npiv, int ref_nb) {
     }
   }
   // The reference's blocked path (mlen > nb, nb != 0) leaves the pivot entries past
-  // min(rows, cols) inside the last block equal to that block's start row (lu.go:381-383).
+  // min(rows, cols) inside the last block equal to that block's start row (lu.go:216-219).
   if (ref_nb > 0 && mn > ref_nb && npiv > mn) {
     int64_t k_last = 0;
     for (int64_t k = 0; k < m && k < n;) {

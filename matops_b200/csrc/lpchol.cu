@@ -132,15 +132,7 @@ __global__ void __launch_bounds__(256) lp_convert_kernel(const double *A, int64_
 
 template <int PREC>
 int set_lp_diag_smem() {
-  static int attr_mask = 0;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (!(attr_mask & (1 << (dev & 31)))) {
-    MO_CUDA_TRY(cudaFuncSetAttribute(lp_diag_kernel<PREC>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, TRI_SMEM_BYTES));
-    attr_mask |= 1 << (dev & 31);
-  }
-  return MO_OK;
+  return mo_smem_attr((const void *)lp_diag_kernel<PREC>, TRI_SMEM_BYTES);
 }
 
 // diagonal block + panel of step k on ctx->stream; P receives the split L21.  The split

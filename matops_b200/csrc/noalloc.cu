@@ -12,55 +12,40 @@
 //   * order of A <= MO_SOLVE_TRM_STATIC_MAX_N (1024): the scratch holds the inverses of
 //     at most 8 diagonal blocks of 128 x 128 doubles (1 MiB).  Larger A -> MO_ESTATICLIMIT.
 //   * the block is part of the library image: every GPU that loads the library keeps these
-//     1 MiB (+ 16 bytes of status) until the process exits.
+//     1 MiB (+ 32 bytes of status) until the process exits.
 //   * all calls on a device share the block and it keeps the last call's contents; calls
 //     that overlap on the GPU (other threads, other streams) race and must be serialized
 //     by the caller.
-//   * the first call on a device looks the block up (cudaGetSymbolAddress) with that
-//     device current; make that first call before any stream capture begins.
-#include <mutex>
-
+//   * every call looks the block's device address up (cudaGetSymbolAddress) with the
+//     caller's device current: the first call on a device loads this library's kernels
+//     there, so make it before any stream capture begins.  Looking the address up on each
+//     call (it allocates nothing once the module is loaded) keeps the address right after
+//     a context reset, when the module and its block are loaded again elsewhere.
 #include "context.cuh"
 
 namespace {
 
 constexpr int kMaxOrder = MO_SOLVE_TRM_STATIC_MAX_N;
 constexpr int kBlock = 128;  // diagonal block order used by the triangular sweep
-constexpr size_t kScratchDoubles = (size_t)(kMaxOrder / kBlock) * kBlock * kBlock;
+static_assert(kMaxOrder % kBlock == 0, "the scratch holds whole 128 x 128 blocks");
+constexpr size_t kScratchDoubles = (size_t)((kMaxOrder + kBlock - 1) / kBlock) * kBlock * kBlock;
 
-// Fixed device scratch: inverted diagonal blocks of the last call, and a status word
-// (first int; the bounded device waits of the GEMM engine write into it).
+// Fixed device scratch: inverted diagonal blocks of the last call, and the context's
+// control words (status first; the bounded device waits write into it).
 static __device__ __align__(256) double g_static_trsm_scratch[kScratchDoubles];
-static __device__ __align__(256) int g_static_trsm_status[4];
+static __device__ __align__(256) int g_static_trsm_status[8];
 
-struct DeviceSlot {
-  bool ready = false;
-  double *scratch = nullptr;  // device address of g_static_trsm_scratch on this device
-  int *status = nullptr;      // device address of g_static_trsm_status on this device
-  int sms = 0;
-};
-DeviceSlot g_slots[64];
-std::mutex g_slots_mu;
-
-// Once per device, with that device current: the symbols' device addresses (the names
-// themselves are host-side stand-ins and must not be passed to a kernel).
-int device_slot(int dev, DeviceSlot **out) {
-  if (dev < 0 || dev >= 64) return MO_EINVAL;
-  std::lock_guard<std::mutex> lock(g_slots_mu);
-  DeviceSlot &s = g_slots[dev];
-  if (!s.ready) {
-    void *p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_static_trsm_scratch);
-    if (e != cudaSuccess) return mo_from_cuda_error(e);
-    s.scratch = static_cast<double *>(p);
-    e = cudaGetSymbolAddress(&p, g_static_trsm_status);
-    if (e != cudaSuccess) return mo_from_cuda_error(e);
-    s.status = static_cast<int *>(p);
-    e = cudaDeviceGetAttribute(&s.sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e != cudaSuccess) return mo_from_cuda_error(e);
-    s.ready = true;
-  }
-  *out = &s;
+// The device addresses of the two blocks for the current device (the names themselves
+// are host-side stand-ins and must not be passed to a kernel) and its SM count.
+int device_slot(double **scratch, int **status, int *sms) {
+  int dev = 0;
+  MO_CUDA_TRY(cudaGetDevice(&dev));
+  void *p = nullptr;
+  MO_CUDA_TRY(cudaGetSymbolAddress(&p, g_static_trsm_scratch));
+  *scratch = static_cast<double *>(p);
+  MO_CUDA_TRY(cudaGetSymbolAddress(&p, g_static_trsm_status));
+  *status = static_cast<int *>(p);
+  MO_CUDA_TRY(cudaDeviceGetAttribute(sms, cudaDevAttrMultiProcessorCount, dev));
   return MO_OK;
 }
 
@@ -68,11 +53,7 @@ int device_slot(int dev, DeviceSlot **out) {
 
 extern "C" int mo_solve_trm_static(mo_matrix Bm, mo_matrix Am, double alpha, int flags,
                                    void *stream) {
-  int dev = 0;
-  MO_CUDA_TRY(cudaGetDevice(&dev));
-  DeviceSlot *slot = nullptr;
-  int rc = device_slot(dev, &slot);
-  if (rc) return rc;
+  int rc;
   mo::View B, A;
   if ((rc = mo::to_view(Bm, B)) || (rc = mo::to_view(Am, A))) return rc;
   // the size rules of SolveTrm (mmult.go:388-422), as in mo_solve_trm
@@ -96,20 +77,25 @@ extern "C" int mo_solve_trm_static(mo_matrix Bm, mo_matrix Am, double alpha, int
   if (N == 0 || (right ? B.rows : B.cols) == 0) return MO_OK;
   if (A.rows < N || (right ? B.cols : B.rows) < N) return MO_EABSIZE;
   if (N > kMaxOrder) return MO_ESTATICLIMIT;
+  double *scratch = nullptr;
+  int *status = nullptr, sms = 0, dev = 0;
+  MO_CUDA_TRY(cudaGetDevice(&dev));
+  if ((rc = device_slot(&scratch, &status, &sms))) return rc;
 
   // a context on the host stack: no scratch of its own, no stream-K (data-parallel GEMM
   // schedule only), status word in the fixed block
   mo_ctx ctx;
   ctx.device = dev;
   ctx.stream = static_cast<cudaStream_t>(stream);
-  ctx.d_status = slot->status;
-  ctx.sms = slot->sms;
-  MO_CUDA_TRY(cudaMemsetAsync(slot->status, 0, sizeof(int), ctx.stream));
+  ctx.d_status = status;
+  ctx.sms = sms;
+  MO_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), ctx.stream));
   mo::View Bn = right ? B.sub(0, 0, B.rows, N) : B.sub(0, 0, N, B.cols);
-  rc = mo::trsm_with_scratch(&ctx, Bn, A.sub(0, 0, N, N), flags, alpha, slot->scratch);
+  rc = mo::trsm_with_scratch(&ctx, Bn, A.sub(0, 0, N, N), flags, alpha, scratch);
   if (rc) return rc;
-  MO_CUDA_TRY(cudaStreamSynchronize(ctx.stream));
+  // read the status word on the caller's stream (no device-wide synchronization)
   int st = 0;
-  MO_CUDA_TRY(cudaMemcpy(&st, slot->status, sizeof(int), cudaMemcpyDeviceToHost));
+  MO_CUDA_TRY(cudaMemcpyAsync(&st, status, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+  MO_CUDA_TRY(cudaStreamSynchronize(ctx.stream));
   return st;
 }

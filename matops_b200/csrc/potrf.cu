@@ -48,15 +48,7 @@ __global__ void __launch_bounds__(TRI_THREADS)
 namespace {
 
 int set_diag_smem() {
-  static int attr_mask = 0;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (!(attr_mask & (1 << (dev & 31)))) {
-    MO_CUDA_TRY(cudaFuncSetAttribute(potrf_diag_kernel,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, TRI_SMEM_BYTES));
-    attr_mask |= 1 << (dev & 31);
-  }
-  return MO_OK;
+  return mo_smem_attr((const void *)potrf_diag_kernel, TRI_SMEM_BYTES);
 }
 
 // Panel step at column k (block order b) on ctx->stream: factor + invert the diagonal

@@ -34,15 +34,7 @@ __global__ void __launch_bounds__(TRI_THREADS)
 }
 
 int set_tri_smem(const void *fn) {
-  static int done_mask = 0;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (!(done_mask & (1 << (dev & 31)))) {
-    MO_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     TRI_SMEM_BYTES));
-    done_mask |= 1 << (dev & 31);
-  }
-  return MO_OK;
+  return mo_smem_attr(fn, TRI_SMEM_BYTES);
 }
 
 }  // namespace

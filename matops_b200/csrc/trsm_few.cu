@@ -57,6 +57,7 @@ struct FewArgs {
   int *flags;         // [groups * nblk]
   int epoch;
   int *status;
+  uint32_t spin_limit;  // polls of a step flag before the wait gives up (MO_EDEVTIMEOUT)
 };
 
 // step flags sit one per 128-byte line, and pollers read them with acquire loads (not
@@ -257,7 +258,7 @@ __global__ void __launch_bounds__(FEW_THREADS, 1) trsm_few_kernel(FewArgs p) {
           if (threadIdx.x == 0) {
             uint32_t it = 0;
             while (flag_load(&flags[s2 * FLAG_STRIDE]) != p.epoch) {
-              if (++it > MO_SPIN_LIMIT) {
+              if (++it > p.spin_limit) {
                 set_status(p.status, MO_EDEVTIMEOUT);
                 s_abort = 1;
                 break;
@@ -328,15 +329,9 @@ __global__ void __launch_bounds__(FEW_THREADS, 1) trsm_few_kernel(FewArgs p) {
 
 template <typename TA, int NT>
 int launch_few(mo_ctx *ctx, FewArgs &p) {
-  static int attr_mask = 0;
-  int dev = 0;
-  cudaGetDevice(&dev);
   const void *kern = (const void *)trsm_few_kernel<TA, NT>;
   constexpr int smem = few_smem<TA, NT>();
-  if (!(attr_mask & (1 << (dev & 31)))) {
-    MO_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    attr_mask |= 1 << (dev & 31);
-  }
+  if (int rc = mo_smem_attr(kern, smem)) return rc;
   int occ = 0;
   MO_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, FEW_THREADS, smem));
   if (occ < 1) return MO_EINVAL;
@@ -451,7 +446,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, 1) trsm_pair_kernel(FewArgs p) {
           if (threadIdx.x == 0) {
             uint32_t it = 0;
             while (flag_load(&flags[s2 * FLAG_STRIDE]) != p.epoch) {
-              if (++it > MO_SPIN_LIMIT) {
+              if (++it > p.spin_limit) {
                 set_status(p.status, MO_EDEVTIMEOUT);
                 s_abort = 1;
                 break;
@@ -553,15 +548,9 @@ __global__ void __launch_bounds__(PAIR_THREADS, 1) trsm_pair_kernel(FewArgs p) {
 
 template <int NT>
 int launch_pair(mo_ctx *ctx, FewArgs &p) {
-  static int attr_mask = 0;
-  int dev = 0;
-  cudaGetDevice(&dev);
   const void *kern = (const void *)trsm_pair_kernel<NT>;
   constexpr int smem = pair_smem<NT>();
-  if (!(attr_mask & (1 << (dev & 31)))) {
-    MO_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    attr_mask |= 1 << (dev & 31);
-  }
+  if (int rc = mo_smem_attr(kern, smem)) return rc;
   int occ = 0;
   MO_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, PAIR_THREADS, smem));
   if (occ < 1) return MO_EINVAL;
@@ -609,6 +598,7 @@ int few_run(mo_ctx *ctx, View B, const void *A, bool a32, int64_t lda, int N, in
   p.flags = flag_buf;
   p.epoch = ++ctx->sk_epoch;
   p.status = reinterpret_cast<int *>(ctx->d_status);
+  p.spin_limit = ctx->spin_limit;
   // more than MO_FEW_GROUP columns: groups solved side by side by separate CTA sets, so
   // the per-step work on the dependency chain is that of one group
   const bool pair = a32 && p.nblk >= 4;

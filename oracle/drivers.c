@@ -24,7 +24,7 @@ enum {
   OR_OK = 0,
   OR_ESIZE = -1,        /* "Mult: size mismatch"             mmult.go:224 */
   OR_ENOTSQUARE = -2,   /* "A not a square matrix"           chol.go:119 */
-  OR_EPIVLEN = -3,      /* "pivot array < min(A.Rows(),A.Cols())" lu.go:424 */
+  OR_EPIVLEN = -3,      /* "pivot array < min(A.Rows(),A.Cols())" lu.go:260-262 */
   OR_ECNOTSQUARE = -4,  /* "C not a square matrix"           mmult.go:428 */
   OR_EABSIZE = -5,      /* "A, B size mismatch"              mmult.go:406 */
   OR_ENOTVECTOR = -6    /* "X not a vector." / "Y not a vector."  mvec.go:34-37 */
@@ -263,9 +263,9 @@ static int unblockedCHOL(fm A, int flags, int nr) {
   return OR_OK;
 }
 
-/* chol.go:58-94 (blockedCHOL) */
-static int blockedCHOL(fm A, int flags, int nb) {
-  for (int k = 0; k < A.r && k < A.c; ) {
+/* chol.go:58-94 (blockedCHOL), block steps whose first column k lies in [k0, k1) */
+static int blockedCHOL_steps(fm A, int flags, int nb, int k0, int k1) {
+  for (int k = k0; k < A.r && k < A.c && k < k1; ) {
     int b = (k + nb > A.c) ? A.c - k : nb;
     fm A11 = sub(A, k, k, b, b);
     int err = unblockedCHOL(A11, flags, k);
@@ -283,6 +283,10 @@ static int blockedCHOL(fm A, int flags, int nb) {
     k += b;
   }
   return OR_OK;
+}
+
+static int blockedCHOL(fm A, int flags, int nb) {
+  return blockedCHOL_steps(A, flags, nb, 0, A.c);
 }
 
 /* chol.go:116-127 */
@@ -423,6 +427,15 @@ int or_decompose_chol(double *A, int ar, int ac, int lda, int flags, int nb) {
 int or_decompose_lu(double *A, int ar, int ac, int lda, int64_t *piv, int npiv, int nb) {
   pv p = {piv, npiv};
   return or_decompose_lu_fm(FM(A, ar, ac, lda), p, nb);
+}
+/* blockedCHOL's steps k0 <= k < k1 (k0 a multiple of nb): a long factorization timed in
+ * slices; running the slices [0, k1), [k1, k2), ... in order equals one DecomposeCHOL call
+ * with nb > 0 and nb <= order (chol.go:123-126) */
+int or_decompose_chol_steps(double *A, int ar, int ac, int lda, int flags, int nb, int k0, int k1) {
+  fm a = FM(A, ar, ac, lda);
+  if (a.c != a.r) return OR_ENOTSQUARE;
+  if (nb <= 0 || a.c < nb || k0 % nb) return OR_ESIZE;
+  return blockedCHOL_steps(a, flags, nb, k0, k1);
 }
 void or_solve_chol(double *B, int br, int bc, int ldb, double *A, int ar, int ac, int lda, int flags) {
   or_solve_chol_fm(FM(B, br, bc, ldb), FM(A, ar, ac, lda), flags);

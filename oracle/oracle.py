@@ -72,6 +72,7 @@ class Oracle:
         L.or_solve_trm.argtypes = M + M + [d, i]
         L.or_decompose_chol.argtypes = M + [i, i]
         L.or_decompose_lu.argtypes = M + [p, i, i]
+        L.or_decompose_chol_steps.argtypes = M + [i, i, i, i]
         L.or_solve_chol.argtypes = M + M + [i]
         L.or_solve_chol.restype = None
         L.or_solve_lu.argtypes = M + M + [p, i, i]
@@ -91,6 +92,10 @@ class Oracle:
 
     def DecomposeCHOL(self, A, flags, nb):
         return self.lib.or_decompose_chol(*view(A), flags, nb)
+
+    def DecomposeCHOLSteps(self, A, flags, nb, k0, k1):
+        """blockedCHOL's block steps with first column in [k0, k1) (chol.go:58-94)"""
+        return self.lib.or_decompose_chol_steps(*view(A), flags, nb, k0, k1)
 
     def DecomposeLU(self, A, pivots: np.ndarray, nb):
         assert pivots.dtype == np.int64 and pivots.flags.c_contiguous

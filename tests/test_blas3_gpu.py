@@ -1,4 +1,6 @@
 """GPU parity: Mult / RankUpdateSym / SolveTrm against the oracle on the same inputs."""
+import os
+
 import numpy as np
 import pytest
 
@@ -36,12 +38,19 @@ def test_mult(gpu, oracle, rng, flags, m, n, k):
     alpha, beta = 1.5, -0.5
     Cg = dev(gpu, C0)
     assert gpu.Mult(Cg, dev(gpu, A), dev(gpu, B), alpha, beta, flags) is None
+    Cr = C0.copy(order="F")
     if m * n * k > 2e8:
-        opA = A.T if flags & TA else A
-        opB = B.T if flags & TB else B
-        Cr = beta * C0 + alpha * (opA @ opB)
+        # the configured DGEMM (2048^3, alpha 1.5, beta -0.5): compared with the reference's
+        # own calgo kernels (oracle/_ref) with NumWorkers = host cores when they were built,
+        # else with the oracle port on all cores
+        from oracle.oracle import Oracle, ref_available
+        big = Oracle("ref" if ref_available() else "port")
+        old = big.NumWorkers(os.cpu_count() or 1)
+        try:
+            assert big.Mult(Cr, A, B, alpha, beta, flags) == 0
+        finally:
+            big.NumWorkers(old)
     else:
-        Cr = C0.copy(order="F")
         assert oracle.Mult(Cr, A, B, alpha, beta, flags) == 0
     err = fro(host(Cg) - Cr)
     assert err <= gemm_bound(k, alpha, beta, A, B, C0), err

@@ -50,6 +50,23 @@ def test_static_solve_matches_regular_entry_point(gpu, rng, n, nrhs):
             assert err <= 100 * n * EPS, (call, hex(flags), err)
 
 
+def test_static_solve_matches_oracle(gpu, oracle, rng):
+    """The static entry point against the oracle's SolveTrm (the reference's algorithm on the
+    CPU), not only against the regular entry point."""
+    import torch
+    n, nrhs = 700, 96
+    for flags in (LEFT | LO, RIGHT | UP | TA):
+        A = _tri(rng, n)
+        B0 = colmajor(rng.standard_normal((nrhs, n) if flags & RIGHT else (n, nrhs)))
+        Bg = gpu.to_device(B0)
+        assert _static_solve(gpu, Bg, gpu.to_device(A), -0.7, flags) == 0
+        torch.cuda.synchronize()
+        Br = B0.copy(order="F")
+        assert oracle.SolveTrm(Br, A, -0.7, flags) == 0
+        err = fro(Bg.cpu().numpy() - Br) / fro(Br)
+        assert err <= 100 * n * EPS, (hex(flags), err)
+
+
 def test_static_solve_allocates_nothing(gpu, rng):
     import torch
     n = 512
