@@ -50,6 +50,7 @@ extern "C" {
 #define MO_EPIVLEN (-3)      /* "pivot array < min(A.Rows(),A.Cols())"    lu.go:260-262 */
 #define MO_ECNOTSQUARE (-4)  /* "C not a square matrix"                  mmult.go:428 */
 #define MO_EABSIZE (-5)      /* "A, B size mismatch"                     mmult.go:406 */
+#define MO_ESYMSIZE (-7)     /* "MultSym: size mismatch"                 mmult.go:290 */
 #define MO_EINVAL (-10)      /* NULL context/pointer, negative size, ld < rows        */
 #define MO_ECUDA (-20)       /* CUDA runtime error                                    */
 #define MO_EDEVTIMEOUT (-21) /* a bounded device-side wait gave up                    */
@@ -164,6 +165,44 @@ MO_API int mo_rank_update_sym(mo_ctx *ctx, mo_matrix C, mo_matrix A, double alph
  * MO_TRANSA = op(A) = A^T.  Size checks as mmult.go:394-407. */
 MO_API int mo_solve_trm(mo_ctx *ctx, mo_matrix B, mo_matrix A, double alpha, int flags);
 
+/* MultSym(C, A, B, alpha, beta, flags), mmult.go:266-330 (SYMM, calgo/dmmat_symm.c:253):
+ *   C = beta*C + alpha*S*op(B)   with MO_LEFT
+ *   C = beta*C + alpha*op(B)*S   otherwise (the reference's kernel takes this branch
+ *                                whenever MO_LEFT is not set)
+ * S is the symmetric matrix whose upper (MO_UPPER) or lower triangle A stores; op(B) = B^T
+ * with MO_TRANSB.  Size check and empty rule as mmult.go:273-291 (MO_ESYMSIZE); shapes
+ * that pass it but do not fit the product -> MO_EABSIZE (the reference reads out of
+ * range).  Asynchronous; uses n^2 doubles of context workspace. */
+MO_API int mo_mult_sym(mo_ctx *ctx, mo_matrix C, mo_matrix A, mo_matrix B, double alpha,
+                       double beta, int flags);
+
+/* MultTrm(B, A, alpha, flags), mmult.go:338-375 (TRMM, calgo/dmmat_trid.c:780):
+ *   B = alpha*op(T)*B   (MO_LEFT, or neither side bit)
+ *   B = alpha*B*op(T)   (MO_RIGHT)
+ * T triangular: MO_UPPER selects upper, otherwise lower; MO_UNIT = unit diagonal (not
+ * read); op(T) = T^T with MO_TRANSA.  Size checks as mmult.go:343-355.  Asynchronous; uses
+ * n^2 + size(B) doubles of context workspace. */
+MO_API int mo_mult_trm(mo_ctx *ctx, mo_matrix B, mo_matrix A, double alpha, int flags);
+
+/* RankUpdate2Sym(C, A, B, alpha, beta, flags), mmult.go:453-475 (SYR2K,
+ * calgo/dmmat_rank.c:132):
+ *   triangle(C) = beta*C + alpha*(A*B^T + B*A^T)     (A^T*B + B^T*A with MO_TRANSA)
+ * MO_LOWER or MO_UPPER (exactly one) selects the triangle.  Like mo_rank_update_sym, beta
+ * is applied inside the nb x nb diagonal blocks only (and there twice without MO_TRANSA,
+ * as calgo/dmmat_rank.c:167, 228 do) unless mo_set_syrk_blas_beta(ctx, 1).  Non-square C
+ * -> MO_ECNOTSQUARE; A and B of different shapes or op(A) rows != order of C ->
+ * MO_EABSIZE (the reference does not check).  Asynchronous. */
+MO_API int mo_rank_update2_sym(mo_ctx *ctx, mo_matrix C, mo_matrix A, mo_matrix B, double alpha,
+                               double beta, int flags);
+
+/* UpdateTrm(C, A, B, alpha, beta, flags), mmult.go:501-523 (calgo/dmmat_rank.c:292):
+ *   triangle(C) = beta*C + alpha*op(A)*op(B)    (MO_UPPER selects upper, else lower)
+ * beta inside the nb x nb diagonal blocks only unless mo_set_syrk_blas_beta(ctx, 1).  Non-
+ * square C -> MO_ECNOTSQUARE; op(A) n x P and op(B) P x n not matching -> MO_EABSIZE.
+ * Asynchronous. */
+MO_API int mo_update_trm(mo_ctx *ctx, mo_matrix C, mo_matrix A, mo_matrix B, double alpha,
+                         double beta, int flags);
+
 /* ---- factorizations and solves ---- */
 
 /* DecomposeCHOL(A, flags, nb), chol.go:116-127: A = L*L^T (MO_LOWER) or U^T*U (otherwise)
@@ -211,6 +250,10 @@ typedef struct mo_ir_info {
   int fallback;     /* 1 if X came from the FP64 factorization (DecomposeCHOL path)    */
   int shifts;       /* low-precision factorizations retried with a diagonal shift      */
   int method;       /* MO_IR_CLASSIC or MO_IR_GMRES: the method of the last step       */
+  int abandoned;    /* 1 if MO_IR_AUTO stopped refining because the steps it projected
+                       from the last reduction would cost more than the FP64 path      */
+  int prec;         /* split format of the factor used: MO_PREC_BF16X3, or MO_PREC_TF32X3
+                       also when MO_IR_AUTO moved from a BF16x3 factor that broke down   */
   double berr;      /* max over columns of |b - A x|_inf / (|A|_inf |x|_inf + |b|_inf) */
   double shift;     /* relative diagonal shift of the factored matrix (0 = none)       */
   double history[MO_IR_HISTORY]; /* berr before each step (history[0]: x = 0)          */
@@ -220,7 +263,10 @@ typedef struct mo_ir_info {
  * factored as L L^T in the low precision `prec` and X is refined in FP64 until the
  * normwise backward error is <= tol, for at most maxit steps (method as above).  If the
  * low-precision factorization breaks down, it is retried on A + s*diag(A) with a growing
- * relative shift s.  Unless MO_IR_NO_FALLBACK is set, a solve that does not converge is
+ * relative shift s (with MO_IR_AUTO, a BF16x3 factor that breaks down is first redone with
+ * the TF32x3 split, unshifted).  MO_IR_AUTO also stops refining when the GMRES-IR steps it
+ * projects from the last reduction would cost more than the FP64 path, and falls back.
+ * Unless MO_IR_NO_FALLBACK is set, a solve that does not converge is
  * redone with the FP64 factorization.  B and X are n x nrhs (X may be B).  Returns 0, a
  * size/argument error, or i > 0 if the FP64 fallback found A not positive definite at
  * column i - 1.  `info` may be NULL.  Synchronous. */
@@ -291,6 +337,33 @@ MO_API int mo_batch_tune(mo_batch *plan, int reps, double *ms);
 /* Read (set = 0) or replace (set = 1) the per-bucket configuration table (MO_BATCH_BUCKETS
  * ints, each 0 or 1), e.g. to persist a tuned schedule and restore it in a later run. */
 MO_API int mo_batch_schedule(mo_batch *plan, int *cfg, int set);
+
+/* ---- device mirrors of host arrays: residency for a shim that holds FloatMatrix data
+ * in host slices (no counterpart in the reference, whose calls work in place on host
+ * views, FloatArray() + LeadingIndex(), mmult.go:228-233; views of one array overlap,
+ * partition.go:210-340) ---- */
+typedef struct mo_mirror mo_mirror;
+/* Register the host array [host, host + count) (a FloatMatrix's whole backing slice) with
+ * the context: device memory of the same size is allocated on the first device view.  A
+ * range overlapping a registered one -> MO_EINVAL. */
+MO_API int mo_mirror_create(mo_ctx *ctx, double *host, int64_t count, mo_mirror **mirror);
+/* Unregister and free the device copy (the host array is untouched). */
+MO_API int mo_mirror_destroy(mo_mirror *mirror);
+/* The registered array that contains host address p, and p's element offset in it; a
+ * view of any sub-matrix maps to its root array this way.  Not registered -> MO_EINVAL. */
+MO_API int mo_mirror_find(const double *p, mo_mirror **mirror, int64_t *offset);
+/* Device view of the host view (p, rows, cols, ld) inside the mirror: uploads the whole
+ * array first if the host copy is newer; write != 0 marks the device copy newer.  The view
+ * must lie inside the array, else MO_EINVAL. */
+MO_API int mo_mirror_view(mo_mirror *mirror, const double *p, int64_t rows, int64_t cols,
+                          int64_t ld, int write, mo_matrix *out);
+/* Bring the host array up to date (download if the device copy is newer); synchronous. */
+MO_API int mo_mirror_to_host(mo_mirror *mirror);
+/* The caller changed the host array: the next device view uploads it.  MO_EINVAL if the
+ * device copy also has changes not yet brought back (mo_mirror_to_host first). */
+MO_API int mo_mirror_host_modified(mo_mirror *mirror);
+/* 0 = copies equal, 1 = host newer, 2 = device newer */
+MO_API int mo_mirror_state(const mo_mirror *mirror);
 
 /* ---- allocation-free variant (no counterpart in the reference) ---- */
 

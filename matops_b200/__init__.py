@@ -11,5 +11,6 @@ from .api import (  # noqa: F401
     matrix, to_device, view, Upload, UploadTriangle, Download, host_matrix, Profile, ProfileEnable, ProfileRead,
     MeasureFP64Peak, PREC_BF16X3, PREC_TF32X3, IR_AUTO, IR_CLASSIC, IR_GMRES, IR_NO_FALLBACK,
     IRInfo, SolveCHOLMixed, LPGemm, BATCH_CHOL, BATCH_LU, BATCH_MAX_N, BatchPlan,
-    DecomposeCHOLAdjoint, DecomposeCHOLAdjointBatched, SolveCHOLAdjoint,
+    DecomposeCHOLAdjoint, DecomposeCHOLAdjointBatched, SolveCHOLAdjoint, SetSpinLimit, Mirror,
+    context, MultSym, MultTrm, RankUpdate2Sym, UpdateTrm,
 )

@@ -27,7 +27,8 @@ class MoIRInfo(ctypes.Structure):
     """mo_ir_info: outcome of mo_dsposv_ir."""
     _fields_ = [("iters", ctypes.c_int), ("gmres_iters", ctypes.c_int),
                 ("converged", ctypes.c_int), ("fallback", ctypes.c_int),
-                ("shifts", ctypes.c_int), ("method", ctypes.c_int),
+                ("shifts", ctypes.c_int), ("method", ctypes.c_int), ("abandoned", ctypes.c_int),
+                ("prec", ctypes.c_int),
                 ("berr", ctypes.c_double), ("shift", ctypes.c_double),
                 ("history", ctypes.c_double * 32)]
 
@@ -55,6 +56,17 @@ def lib() -> ctypes.CDLL:
         "mo_num_workers": [p, i],
         "mo_set_syrk_blas_beta": [p, i],
         "mo_set_spin_limit": [p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)],
+        "mo_mult_sym": [p, M, M, M, d, d, i],
+        "mo_mult_trm": [p, M, M, d, i],
+        "mo_rank_update2_sym": [p, M, M, M, d, d, i],
+        "mo_update_trm": [p, M, M, M, d, d, i],
+        "mo_mirror_create": [p, p, i64, ctypes.POINTER(p)],
+        "mo_mirror_destroy": [p],
+        "mo_mirror_find": [p, ctypes.POINTER(p), ctypes.POINTER(i64)],
+        "mo_mirror_view": [p, p, i64, i64, i64, i, ctypes.POINTER(M)],
+        "mo_mirror_to_host": [p],
+        "mo_mirror_host_modified": [p],
+        "mo_mirror_state": [p],
         "mo_malloc": [p, ctypes.POINTER(p), sz],
         "mo_free": [p, p],
         "mo_upload": [p, M, p, i64],

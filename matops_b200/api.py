@@ -132,6 +132,29 @@ def SolveTrm(B, A, alpha: float, flags: int):
     return _err(_lib.lib().mo_solve_trm(context(), view(B), view(A), alpha, flags), True)
 
 
+def MultSym(C, A, B, alpha: float, beta: float, flags: int):
+    """mmult.go:266: C = beta*C + alpha*S*op(B) (LEFT) or beta*C + alpha*op(B)*S, S the
+    symmetric matrix of A's UPPER (else lower) triangle"""
+    return _err(_lib.lib().mo_mult_sym(context(), view(C), view(A), view(B), alpha, beta, flags))
+
+
+def MultTrm(B, A, alpha: float, flags: int):
+    """mmult.go:338: B = alpha*op(T)*B (LEFT) or alpha*B*op(T) (RIGHT), T triangular"""
+    return _err(_lib.lib().mo_mult_trm(context(), view(B), view(A), alpha, flags), True)
+
+
+def RankUpdate2Sym(C, A, B, alpha: float, beta: float, flags: int):
+    """mmult.go:453: triangle(C) = beta*C + alpha*(A*B^T + B*A^T) (TRANSA: A^T*B + B^T*A)"""
+    return _err(_lib.lib().mo_rank_update2_sym(context(), view(C), view(A), view(B), alpha, beta,
+                                               flags), True)
+
+
+def UpdateTrm(C, A, B, alpha: float, beta: float, flags: int):
+    """mmult.go:501: triangle(C) = beta*C + alpha*op(A)*op(B)"""
+    return _err(_lib.lib().mo_update_trm(context(), view(C), view(A), view(B), alpha, beta,
+                                         flags), True)
+
+
 def DecomposeCHOL(A, flags: int, nb: int):
     """chol.go:116 -- returns (A, err); a non-positive pivot panics like the reference."""
     bad = ctypes.c_double(0.0)
@@ -184,6 +207,8 @@ class IRInfo:
         self.fallback = bool(raw.fallback)
         self.shifts = raw.shifts
         self.method = raw.method
+        self.abandoned = bool(raw.abandoned)
+        self.prec = raw.prec
         self.berr = raw.berr
         self.shift = raw.shift
         self.history = [raw.history[i] for i in range(min(32, raw.iters + 1))]
@@ -191,7 +216,8 @@ class IRInfo:
     def __repr__(self):
         return (f"IRInfo(iters={self.iters}, gmres_iters={self.gmres_iters}, "
                 f"converged={self.converged}, fallback={self.fallback}, shifts={self.shifts}, "
-                f"method={self.method}, berr={self.berr:.3e}, shift={self.shift:.3e})")
+                f"method={self.method}, abandoned={self.abandoned}, berr={self.berr:.3e}, "
+                f"shift={self.shift:.3e})")
 
 
 def SolveCHOLMixed(X, A, B, flags: int = LOWER, prec: int = PREC_TF32X3, method: int = IR_AUTO,
@@ -437,3 +463,73 @@ def SolveCHOLAdjoint(L, X, Xbar, Abar, flags: int = LOWER):
     Abar -= (Bbar X^T + X Bbar^T) / 2."""
     return _err(_lib.lib().mo_solve_chol_adjoint(context(), view(L), view(X), view(Xbar),
                                                  view(Abar), flags))
+
+
+# ---- residency: device mirrors of host arrays (what a cgo shim over FloatMatrix uses) ----
+
+class Mirror:
+    """A registered host backing array (a float64 numpy array) with a device copy.
+
+    `view(sub, write)` maps any column-major view `sub` of the array (a numpy slice, as a
+    FloatMatrix view shares its parent's storage) to a device mo_matrix over the same
+    elements, uploading first if the host copy is newer; `to_host()` downloads if a device
+    view was written; `host_modified()` marks host-side edits.  Overlapping views share one
+    device copy, so a chain of calls on views of one array needs no host round trip."""
+
+    def __init__(self, host):
+        import numpy as np
+        if not isinstance(host, np.ndarray) or host.dtype != np.float64:
+            raise TypeError("expected a float64 numpy array")
+        self.host = host
+        base = host
+        while base.base is not None and isinstance(base.base, np.ndarray):
+            base = base.base
+        self._root = base
+        self._h = ctypes.c_void_p()
+        rc = _lib.lib().mo_mirror_create(context(), ctypes.c_void_p(base.ctypes.data),
+                                         base.size, ctypes.byref(self._h))
+        if rc:
+            raise MatopsError(rc, _lib.lib().mo_strerror(rc).decode())
+
+    def view(self, sub, write: bool = False) -> _lib.MoMatrix:
+        r, c = sub.shape
+        if r > 1 and sub.strides[0] != 8:
+            raise TypeError("view must be column-major")
+        ld = sub.strides[1] // 8 if c > 1 else max(r, 1)
+        out = _lib.MoMatrix()
+        rc = _lib.lib().mo_mirror_view(self._h, ctypes.c_void_p(sub.ctypes.data), r, c, max(ld, 1),
+                                       1 if write else 0, ctypes.byref(out))
+        if rc:
+            raise MatopsError(rc, _lib.lib().mo_strerror(rc).decode())
+        return out
+
+    def to_host(self) -> None:
+        rc = _lib.lib().mo_mirror_to_host(self._h)
+        if rc:
+            raise MatopsError(rc, _lib.lib().mo_strerror(rc).decode())
+
+    def host_modified(self) -> int:
+        return _lib.lib().mo_mirror_host_modified(self._h)
+
+    @property
+    def state(self) -> int:
+        return _lib.lib().mo_mirror_state(self._h)
+
+    @staticmethod
+    def find(p):
+        """(mirror handle, element offset) of the registered array containing numpy view p"""
+        h, off = ctypes.c_void_p(), ctypes.c_int64()
+        rc = _lib.lib().mo_mirror_find(ctypes.c_void_p(p.ctypes.data), ctypes.byref(h),
+                                       ctypes.byref(off))
+        return (h.value, off.value) if rc == 0 else (None, None)
+
+    def close(self) -> None:
+        if self._h:
+            _lib.lib().mo_mirror_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -65,6 +65,7 @@ int gemm_ex(mo_ctx *ctx, View C, View A, bool ta, View B, bool tb, double alpha,
   g.mode = o.mode;
   g.beta_block = o.beta_block;
   g.status = &control(ctx)->status;
+  g.skip = o.skip;
   g.sms = ctx->sms;
   g.max_ctas = o.max_ctas;
   if (o.stream_k && o.mode == kGemm) {
@@ -162,6 +163,8 @@ int mo_ctx_destroy(mo_ctx *ctx) {
     cudaStreamDestroy(s);
   }
   for (auto e : ctx->pool_ev) cudaEventDestroy(e);
+  for (auto e : ctx->gmres_ev) cudaEventDestroy(e);
+  if (ctx->h_gmres) cudaFreeHost(ctx->h_gmres);
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->sk_partial) cudaFree(ctx->sk_partial);
   if (ctx->sk_flags) cudaFree(ctx->sk_flags);
@@ -200,6 +203,7 @@ const char *mo_strerror(int s) {
     case MO_EPIVLEN: return "pivot array < min(A.Rows(),A.Cols())";
     case MO_ECNOTSQUARE: return "C not a square matrix";
     case MO_EABSIZE: return "A, B size mismatch";
+    case MO_ESYMSIZE: return "MultSym: size mismatch";
     case MO_EINVAL: return "invalid argument";
     case MO_ECUDA: return "CUDA runtime error";
     case MO_EDEVTIMEOUT: return "device-side wait timed out";

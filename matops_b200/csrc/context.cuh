@@ -48,6 +48,10 @@ struct mo_ctx {
   size_t ws_adj_bytes = 0;
   std::vector<cudaStream_t> pool;
   std::vector<cudaEvent_t> pool_ev;
+  // GMRES convergence words read back without stopping the stream: pinned host slots and
+  // one event per inner iteration
+  int *h_gmres = nullptr;
+  std::vector<cudaEvent_t> gmres_ev;
 };
 
 namespace mo {
@@ -98,6 +102,7 @@ struct GemmOpts {
   int max_ctas = 0;
   bool stream_k = true;
   int beta_block = 0;
+  const int *skip = nullptr;  // see GemmArgs::skip
 };
 int gemm_ex(mo_ctx *ctx, View C, View A, bool ta, View B, bool tb, double alpha, double beta,
             const GemmOpts &o);

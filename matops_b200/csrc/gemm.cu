@@ -71,6 +71,7 @@ struct KParams {
   int64_t ldc;
   int mode, beta_block;
   int *status;
+  const int *skip;
   int tiles_m, tiles_n;
   int total_tiles;  // tiles of C (the triangle's tiles in SYRK modes)
   int kt;           // k-slabs per tile
@@ -196,6 +197,7 @@ __global__ void __launch_bounds__(THREADS, 1)
   __shared__ int s_abort;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (p.skip && *(volatile const int *)p.skip) return;
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&full[s], USE_TMA ? 1u : 32u);
@@ -523,6 +525,7 @@ int launch_gemm(const GemmArgs &a, cudaStream_t stream) {
   kp.mode = a.mode;
   kp.beta_block = a.beta_block;
   kp.status = a.status;
+  kp.skip = a.skip;
   // narrow C (a residual with few right-hand sides): 256 x 64 tiles
   const bool narrow = a.mode == kGemm && a.N <= 64 && a.M >= 2048;
   const int tbm = narrow ? Geo<true>::TBM : BM, tbn = narrow ? Geo<true>::TBN : BN;

@@ -28,6 +28,9 @@ struct GemmArgs {
   // > 0: beta applies only where row/beta_block == col/beta_block (elsewhere beta = 1)
   int beta_block = 0;
   int *status = nullptr;  // device status word (first error wins)
+  // optional device word: when it is non-zero at launch the whole grid returns at once
+  // (iterations enqueued ahead of a convergence test that has since ended them)
+  const int *skip = nullptr;
   bool force_fallback = false;  // use the cp.async producer even when TMA is legal
   int sms = 148;                // persistent grid size
   int max_ctas = 0;             // > 0: cap the persistent grid (leave SMs to other streams)

@@ -85,7 +85,8 @@ __global__ void __launch_bounds__(PANEL_THREADS)
   __shared__ double s_oldj[MAX_PANEL_W];
   __shared__ double red_v[PANEL_THREADS / 32];
   __shared__ int red_i[PANEL_THREADS / 32];
-  __shared__ int s_p;
+  __shared__ int red_q[PANEL_THREADS / 32];
+  __shared__ int s_p, s_wb;
 
   for (int e = threadIdx.x; e < nr * W; e += blockDim.x) {
     const int r = e % nr, c = e / nr;
@@ -146,32 +147,59 @@ __global__ void __launch_bounds__(PANEL_THREADS)
       }
     }
     if (!grid_barrier(sc.barrier, (unsigned)(j + 1) * nblk, status, abort_flag)) return;
-    // (c) every CTA selects the pivot: largest value, lowest index; NaN on the diagonal wins
-    if (threadIdx.x == 0) {
+    // (c) every CTA selects the pivot: largest value, lowest index; NaN on the diagonal wins.
+    // The candidates are read in parallel (one per thread) and reduced like the local
+    // argmax, so the selection costs one L2 round trip, not one per CTA.
+    {
       double v = -2.0;
-      int p = INT_MAX, wb = -1;
-      for (int q = 0; q < nblk; ++q) {
-        const double cv = ((volatile double *)sc.cand_val)[par * nblk + q];
-        const int ci = ((volatile int *)sc.cand_idx)[par * nblk + q];
+      int p = INT_MAX, wq = INT_MAX;
+      for (int q = threadIdx.x; q < nblk; q += blockDim.x) {
+        const double cv = __ldcg(sc.cand_val + par * nblk + q);
+        const int ci = __ldcg(sc.cand_idx + par * nblk + q);
         if (ci != INT_MAX && better(cv, ci, v, p)) {
           v = cv;
           p = ci;
-          wb = q;
+          wq = q;
         }
       }
-      if (((volatile int *)sc.diag_nan)[par]) {
-        p = j;
-        wb = -1;
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ov = __shfl_down_sync(0xffffffffu, v, off);
+        const int oi = __shfl_down_sync(0xffffffffu, p, off);
+        const int oq = __shfl_down_sync(0xffffffffu, wq, off);
+        if (better(ov, oi, v, p)) {
+          v = ov;
+          p = oi;
+          wq = oq;
+        }
       }
-      s_p = p;
-      red_i[0] = wb;
+      if ((threadIdx.x & 31) == 0) {
+        red_v[threadIdx.x >> 5] = v;
+        red_i[threadIdx.x >> 5] = p;
+        red_q[threadIdx.x >> 5] = wq;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+          if (better(red_v[w], red_i[w], v, p)) {
+            v = red_v[w];
+            p = red_i[w];
+            wq = red_q[w];
+          }
+        int wb = p == INT_MAX ? -1 : wq;
+        if (__ldcg(sc.diag_nan + par)) {
+          p = j;
+          wb = -1;
+        }
+        s_p = p;
+        s_wb = wb;
+      }
+      __syncthreads();
     }
-    __syncthreads();
-    const int p = s_p, wb = red_i[0];
+    const int p = s_p, wb = s_wb;
     for (int c = threadIdx.x; c < W; c += blockDim.x) {
-      const double oj = ((volatile double *)sc.rowj)[par * W + c];
+      const double oj = __ldcg(sc.rowj + par * W + c);
       s_oldj[c] = oj;
-      s_prow[c] = (wb >= 0) ? ((volatile double *)sc.cand_row)[((size_t)par * nblk + wb) * W + c] : oj;
+      s_prow[c] = (wb >= 0) ? __ldcg(sc.cand_row + ((size_t)par * nblk + wb) * W + c) : oj;
     }
     if (b == 0 && threadIdx.x == 0) piv[j] = row0 + p;
     __syncthreads();
@@ -183,16 +211,19 @@ __global__ void __launch_bounds__(PANEL_THREADS)
         for (int c = threadIdx.x; c < W; c += blockDim.x) S[(p - rbeg) * LDW + c] = s_oldj[c];
     }
     __syncthreads();
-    // (e) l = a_ij / u_jj (true division, mvec.go:422 InvScale), then rank-1 update
+    // (e) l = a_ij / u_jj (true division, mvec.go:422 InvScale), then the rank-1 update of
+    // the owned rows below j, spread over (row, column) pairs so that every thread works
     const double ujj = s_prow[j];
-    for (int r = threadIdx.x; r < nr; r += blockDim.x) {
-      const int gi = rbeg + r;
-      if (gi <= j) continue;
-      double *row = S + r * LDW;
-      const double l = row[j] / ujj;
-      row[j] = l;
-      for (int c = j + 1; c < W; ++c) row[c] = fma(-l, s_prow[c], row[c]);
-    }
+    const int r0 = max(0, j + 1 - rbeg);  // first owned row below j
+    for (int r = r0 + threadIdx.x; r < nr; r += blockDim.x) S[r * LDW + j] /= ujj;
+    __syncthreads();
+    const int wr = W - j - 1;
+    if (wr > 0)
+      for (int e = threadIdx.x; e < (nr - r0) * wr; e += blockDim.x) {
+        const int r = r0 + e / wr, c = j + 1 + e % wr;
+        double *row = S + r * LDW;
+        row[c] = fma(-row[j], s_prow[c], row[c]);
+      }
     __syncthreads();
   }
   for (int e = threadIdx.x; e < nr * W; e += blockDim.x) {
@@ -220,6 +251,115 @@ __global__ void laswp_kernel(double *A, int64_t ld, int rows, int ncols, const i
     col[q] = col[p];
     col[p] = t;
   }
+}
+
+// The net effect of the interchanges rows (r0 + s) <-> piv[s], s = 0 .. ns - 1 in order
+// (pivot.go:55-61, entries <= 0 skipped) on the rows they touch: rows r0 .. r0 + ns - 1 and
+// the distinct pivot rows beyond them.  One warp simulates the swaps on row labels and
+// writes the moves dst[i] <- src[i] (i < *count), so that one pass of loads and one of
+// stores applies all of them to any set of columns.  ns <= MAX_PANEL_W.
+__global__ void __launch_bounds__(32) swap_map_kernel(const int64_t *piv, int ns, int64_t r0,
+                                                      int rows, int *dst, int *src, int *count,
+                                                      int *status) {
+  __shared__ int lab[2 * MAX_PANEL_W];   // source row now held at each position
+  __shared__ int ext[MAX_PANEL_W];       // rows beyond the block, in order of first use
+  __shared__ int next;
+  const int lane = threadIdx.x;
+  for (int i = lane; i < ns; i += 32) lab[i] = (int)(r0 + i);
+  if (lane == 0) next = 0;
+  __syncwarp();
+  for (int s = 0; s < ns; ++s) {
+    const int64_t p = piv[s];
+    const int64_t q = r0 + s;
+    if (p <= 0 || p == q) continue;
+    if (p >= rows || q >= rows) {
+      if (lane == 0) set_status(status, MO_EINVAL);
+      continue;
+    }
+    int pos;
+    if (p < r0 + ns) {
+      pos = (int)(p - r0);
+    } else {
+      const int ne = next;
+      int found = -1;
+      for (int b = 0; b < ne; b += 32) {
+        const unsigned hit = __ballot_sync(0xffffffffu, b + lane < ne && ext[b + lane] == (int)p);
+        if (hit) {
+          found = b + __ffs(hit) - 1;
+          break;
+        }
+      }
+      if (found < 0) {
+        found = ne;
+        if (lane == 0) {
+          ext[ne] = (int)p;
+          lab[ns + ne] = (int)p;
+          next = ne + 1;
+        }
+      }
+      pos = ns + found;
+    }
+    __syncwarp();
+    if (lane == 0) {
+      const int t = lab[s];
+      lab[s] = lab[pos];
+      lab[pos] = t;
+    }
+    __syncwarp();
+  }
+  const int total = ns + next;
+  for (int i = lane; i < total; i += 32) {
+    dst[i] = i < ns ? (int)(r0 + i) : ext[i - ns];
+    src[i] = lab[i];
+  }
+  if (lane == 0) *count = total;
+}
+
+// A[dst[i], c] = A_old[src[i], c] for the moves of swap_map_kernel, columns [0, ncols): a
+// CTA takes 32 columns, loads every source row of them into shared memory (lanes along the
+// rows, so the contiguous block rows are read 256 bytes at a time), then stores.
+__global__ void __launch_bounds__(256) laswp_map_kernel(double *A, int64_t ld, int ncols,
+                                                        const int *dst, const int *src,
+                                                        const int *count) {
+  extern __shared__ double vals[];  // [count][32]
+  const int cnt = *count;
+  const int c0 = blockIdx.x * 32;
+  const int nc = min(32, ncols - c0);
+  for (int e = threadIdx.x; e < cnt * nc; e += blockDim.x) {
+    const int i = e % cnt, c = e / cnt;
+    vals[c * cnt + i] = A[src[i] + (int64_t)(c0 + c) * ld];
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < cnt * nc; e += blockDim.x) {
+    const int i = e % cnt, c = e / cnt;
+    A[dst[i] + (int64_t)(c0 + c) * ld] = vals[c * cnt + i];
+  }
+}
+
+// All interchanges rows s <-> piv[s] (s = 0 .. ns - 1, in order) on a few columns of B
+// (SolveLU's applyPivots): one CTA per column, the column in shared memory, one thread
+// applying the swaps in order.
+__global__ void __launch_bounds__(256) laswp_cols_kernel(double *B, int64_t ld, int rows,
+                                                         const int64_t *piv, int ns, int *status) {
+  extern __shared__ double col[];
+  double *g = B + (int64_t)blockIdx.x * ld;
+  for (int i = threadIdx.x; i < rows; i += blockDim.x) col[i] = g[i];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < ns; ++s) {
+      const int64_t p = piv[s];
+      if (p <= 0 || p == s) continue;
+      if (p >= rows || s >= rows) {
+        if (blockIdx.x == 0) set_status(status, MO_EINVAL);
+        continue;
+      }
+      const double t = col[s];
+      col[s] = col[p];
+      col[p] = t;
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < rows; i += blockDim.x) g[i] = col[i];
 }
 
 // piv[i] = v for i in [lo, hi)
@@ -253,7 +393,33 @@ int laswp(mo_ctx *ctx, View A, int c0, int c1, const int64_t *piv, int ns, int64
 int laswp_forward(mo_ctx *ctx, View B, const int64_t *piv, int64_t npiv) {
   if (B.rows == 0 || B.cols == 0 || npiv <= 0) return MO_OK;
   if (npiv > INT_MAX) return MO_EINVAL;
-  return laswp(ctx, B, 0, B.cols, piv, (int)npiv, 0);
+  const size_t smem = (size_t)B.rows * sizeof(double);
+  if (smem > 200 * 1024) return laswp(ctx, B, 0, B.cols, piv, (int)npiv, 0);
+  if (int rc = mo_smem_attr((const void *)laswp_cols_kernel, (int)smem)) return rc;
+  ProfScope ps;
+  prof_begin(ctx, ps, MO_PROF_LASWP);
+  laswp_cols_kernel<<<B.cols, 256, smem, ctx->stream>>>(
+      B.d, B.ld, B.rows, piv, (int)npiv,
+      &reinterpret_cast<CtrlView *>(ctx->d_status)->status);
+  prof_end(ctx, ps, 0.0, 16.0 * B.rows * (double)B.cols);
+  MO_CUDA_TRY(cudaGetLastError());
+  return MO_OK;
+}
+
+// the panel's interchanges on columns [c0, c1) of A through the move list of swap_map_kernel
+int laswp_moves(mo_ctx *ctx, View A, int c0, int c1, const int *dst, const int *src,
+                const int *count, int max_moves) {
+  if (c1 <= c0) return MO_OK;
+  const int nc = c1 - c0;
+  const size_t smem = (size_t)max_moves * 32 * sizeof(double);
+  if (int rc = mo_smem_attr((const void *)laswp_map_kernel, (int)smem)) return rc;
+  ProfScope ps;
+  prof_begin(ctx, ps, MO_PROF_LASWP);
+  laswp_map_kernel<<<(nc + 31) / 32, 256, smem, ctx->stream>>>(A.at(0, c0), A.ld, nc, dst, src,
+                                                               count);
+  prof_end(ctx, ps, 0.0, 16.0 * max_moves * (double)nc);
+  MO_CUDA_TRY(cudaGetLastError());
+  return MO_OK;
 }
 
 int getrf(mo_ctx *ctx, View A, int64_t *piv, int64_t npiv, int ref_nb) {
@@ -287,7 +453,8 @@ int getrf(mo_ctx *ctx, View A, int64_t *piv, int64_t npiv, int ref_nb) {
   const size_t sz_val = 2 * nblk * sizeof(double), sz_idx = 2 * nblk * sizeof(int);
   const size_t sz_row = (size_t)2 * nblk * W * sizeof(double), sz_rowj = 2 * W * sizeof(double);
   const size_t inv_bytes = 128 * 128 * sizeof(double);
-  const size_t total = inv_bytes + sz_val + sz_row + sz_rowj + sz_idx + 64 + 64;
+  const size_t sz_moves = 2 * (2 * MAX_PANEL_W) * sizeof(int) + 64;
+  const size_t total = inv_bytes + sz_val + sz_row + sz_rowj + sz_idx + 64 + 64 + sz_moves;
   char *ws = nullptr;
   int rc = workspace(ctx, total, (void **)&ws);
   if (rc) return rc;
@@ -307,6 +474,8 @@ int getrf(mo_ctx *ctx, View A, int64_t *piv, int64_t npiv, int ref_nb) {
   sc.barrier = (unsigned *)q;
   q += 16;
   int *abort_flag = (int *)q;
+  q += 32;
+  int *mv_dst = (int *)q, *mv_src = mv_dst + 2 * MAX_PANEL_W, *mv_count = mv_src + 2 * MAX_PANEL_W;
 
   for (int k = 0; k < mn; k += W) {
     const int b = min(W, mn - k);
@@ -327,9 +496,16 @@ int getrf(mo_ctx *ctx, View A, int64_t *piv, int64_t npiv, int ref_nb) {
     MO_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)lu_panel_kernel, dim3(pblk),
                                             dim3(PANEL_THREADS), args, smem, ctx->stream));
     prof_end(ctx, ps, (double)pm * b * b - (double)b * b * b / 3.0, 16.0 * pm * b);
-    // interchanges on the columns left and right of the panel
-    if ((rc = laswp(ctx, A, 0, k, piv + k, b, k))) return rc;
-    if ((rc = laswp(ctx, A, k + b, n, piv + k, b, k))) return rc;
+    // interchanges on the columns left and right of the panel, as one move list
+    if (k > 0 || k + b < n) {
+      ProfScope pm;
+      prof_begin(ctx, pm, MO_PROF_LASWP);
+      swap_map_kernel<<<1, 32, 0, ctx->stream>>>(piv + k, b, k, m, mv_dst, mv_src, mv_count, status);
+      prof_end(ctx, pm, 0.0, 8.0 * b);
+      MO_CUDA_TRY(cudaGetLastError());
+    }
+    if ((rc = laswp_moves(ctx, A, 0, k, mv_dst, mv_src, mv_count, 2 * b))) return rc;
+    if ((rc = laswp_moves(ctx, A, k + b, n, mv_dst, mv_src, mv_count, 2 * b))) return rc;
     const int rest_c = n - k - b;
     if (rest_c > 0) {
       View L11 = A.sub(k, k, b, b);

@@ -15,6 +15,7 @@
 // redone on A + s*diag(A) (the shift of Higham and Pranesh, SIAM J. Sci. Comput. 43 (2021)
 // A258-A277) with s growing 8x per retry.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -54,10 +55,12 @@ struct SymArgs {
   int64_t ldy;
   int nr;
   double sa;
+  const int *skip;  // optional: return at once when the word is set
 };
 
 template <bool UP, bool ABS>
 __global__ void __launch_bounds__(256) sym_apply_kernel(SymArgs p) {
+  if (p.skip && *(volatile const int *)p.skip) return;
   // the tile buffers and, after the last tile, the cross-q reduction share one block
   __shared__ double buf[4 * RR * (RNR + 1)];
   double(*T)[RR + 1] = reinterpret_cast<double(*)[RR + 1]>(buf);
@@ -168,7 +171,9 @@ __global__ void colmax_kernel(const double *V, int64_t ld, int n, int nr, double
 // (V_i = V + i * vstride, all n x nr with leading dimension n)
 __global__ void __launch_bounds__(256) dots_kernel(const double *V, int64_t vstride, int nv,
                                                    const double *W, int n, int nr,
-                                                   double *partial, int pstride) {
+                                                   double *partial, int pstride,
+                                                   const int *skip) {
+  if (skip && *(volatile const int *)skip) return;
   __shared__ double s[8][kGmresMax + 2];
   const int c = blockIdx.y, blk = blockIdx.x;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -198,7 +203,8 @@ __global__ void __launch_bounds__(256) dots_kernel(const double *V, int64_t vstr
 
 // h[i * nr + c] (+)= sum over chunks (fixed order); with `root`, h = sqrt of the sum
 __global__ void dots_reduce_kernel(const double *partial, int pstride, int nblk, int nv, int nr,
-                                   double *h, bool root) {
+                                   double *h, bool root, const int *skip) {
+  if (skip && *(volatile const int *)skip) return;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= nv * nr) return;
   double t = 0.0;
@@ -208,7 +214,8 @@ __global__ void dots_reduce_kernel(const double *partial, int pstride, int nblk,
 
 // W(r, c) += sign * sum_{i < nv} V_i(r, c) * h[i * nr + c]
 __global__ void vupdate_kernel(double *W, const double *V, int64_t vstride, int nv,
-                               const double *h, int n, int nr, double sign) {
+                               const double *h, int n, int nr, double sign, const int *skip) {
+  if (skip && *(volatile const int *)skip) return;
   const int r = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
   if (r >= n) return;
   double t = 0.0;
@@ -217,7 +224,9 @@ __global__ void vupdate_kernel(double *W, const double *V, int64_t vstride, int 
 }
 
 // dst(r, c) = src(r, c) / s[c]  (0 where s[c] == 0)
-__global__ void vscale_kernel(double *dst, const double *src, const double *s, int n, int nr) {
+__global__ void vscale_kernel(double *dst, const double *src, const double *s, int n, int nr,
+                              const int *skip) {
+  if (skip && *(volatile const int *)skip) return;
   const int r = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
   if (r >= n) return;
   const double d = s[c];
@@ -280,6 +289,91 @@ __global__ void __launch_bounds__(256) abs_colsum_kernel(const double *S, int n,
   }
 }
 
+
+// GMRES bookkeeping on the device, one thread per right-hand side c (column-major state,
+// LDR = kGmresMax + 1 rows per Hessenberg column):
+//   column j of the Hessenberg matrix = h1 + h2 (the two Gram-Schmidt passes) and |w|,
+//   the earlier Givens rotations applied to it, a new rotation zeroing its subdiagonal, and
+//   g (the rotated right-hand side) updated; |g[j+1]| / beta is the preconditioned residual
+//   ratio.  When the largest ratio is <= tau (or j is the last iteration), *done := 1 and
+//   *m := j + 1.  Nothing happens once *done is set.
+struct GmresState {
+  double *R;      // nr x kGmresMax x LDR
+  double *cs, *sn;  // nr x kGmresMax
+  double *g;      // nr x LDR
+  double *beta;   // nr
+  int *done;      // [0] done flag, [1] iterations used
+};
+constexpr int LDR = kGmresMax + 1;
+
+__global__ void __launch_bounds__(256) gmres_start_kernel(GmresState st, const double *beta, int nr) {
+  for (int c = threadIdx.x; c < nr; c += blockDim.x) {
+    st.beta[c] = beta[c];
+    st.g[(size_t)c * LDR] = beta[c];
+    for (int i = 1; i < LDR; ++i) st.g[(size_t)c * LDR + i] = 0.0;
+  }
+  if (threadIdx.x == 0) {
+    st.done[0] = 0;
+    st.done[1] = 0;
+  }
+}
+
+__global__ void __launch_bounds__(256) gmres_givens_kernel(GmresState st, const double *h1,
+                                                          const double *h2, const double *hn,
+                                                          int j, int nr, double tau, int last) {
+  if (*(volatile const int *)st.done) return;
+  __shared__ double red[256];
+  double worst = 0.0;
+  for (int c = threadIdx.x; c < nr; c += blockDim.x) {
+    double *Rc = st.R + ((size_t)c * kGmresMax + j) * LDR;
+    double *cs = st.cs + (size_t)c * kGmresMax, *sn = st.sn + (size_t)c * kGmresMax;
+    double *g = st.g + (size_t)c * LDR;
+    for (int i = 0; i <= j; ++i) Rc[i] = h1[(size_t)i * nr + c] + h2[(size_t)i * nr + c];
+    Rc[j + 1] = hn[c];
+    for (int i = 0; i < j; ++i) {
+      const double a = Rc[i], b = Rc[i + 1];
+      Rc[i] = cs[i] * a + sn[i] * b;
+      Rc[i + 1] = -sn[i] * a + cs[i] * b;
+    }
+    const double a = Rc[j], b = Rc[j + 1];
+    const double rr = hypot(a, b);
+    const double cc = rr > 0.0 ? a / rr : 1.0, ss = rr > 0.0 ? b / rr : 0.0;
+    cs[j] = cc;
+    sn[j] = ss;
+    Rc[j] = rr;
+    Rc[j + 1] = 0.0;
+    const double gj = g[j];
+    g[j + 1] = -ss * gj;
+    g[j] = cc * gj;
+    if (st.beta[c] > 0.0) worst = fmax(worst, fabs(g[j + 1]) / st.beta[c]);
+  }
+  red[threadIdx.x] = worst;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && (red[0] <= tau || last)) {
+    st.done[1] = j + 1;
+    st.done[0] = 1;
+  }
+}
+
+// y = R^-1 g (m x m upper triangular per column), written as h[i * nr + c]
+__global__ void __launch_bounds__(256) gmres_backsolve_kernel(GmresState st, int m, int nr,
+                                                             double *y) {
+  for (int c = threadIdx.x; c < nr; c += blockDim.x) {
+    const double *g = st.g + (size_t)c * LDR;
+    for (int i = m - 1; i >= 0; --i) {
+      double t = g[i];
+      for (int k = i + 1; k < m; ++k)
+        t -= st.R[((size_t)c * kGmresMax + k) * LDR + i] * y[(size_t)k * nr + c];
+      const double dii = st.R[((size_t)c * kGmresMax + i) * LDR + i];
+      y[(size_t)i * nr + c] = dii != 0.0 ? t / dii : 0.0;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------
@@ -290,6 +384,7 @@ struct Solver {
   bool upper;
   int n, nr;  // nr: right-hand sides (all columns)
   LpChol f;
+  LpSolve ls;             // block-inverse triangular solves with the factor
   double *b, *x, *r, *d;  // n x nr packed
   double *V;              // (kGmresMax + 1) blocks of n x nr
   double *h, *h2;         // Gram-Schmidt coefficients, (kGmresMax + 1) x nr each
@@ -297,6 +392,8 @@ struct Solver {
   double *partial;        // dot partial sums
   double *norms;          // [0, nr): |r|, [nr, 2nr): |x|, [2nr, 3nr): |b|, 3nr: |A|
   int *flags;             // trsm_few block flags
+  GmresState gs;          // device-side Hessenberg, rotations and convergence words
+  const int *skip = nullptr;  // set while GMRES iterations run: their convergence word
   int nblk_dot, pstride;
   double *S = nullptr;    // full symmetric copy of A (many right-hand sides only)
 };
@@ -342,6 +439,7 @@ int sym_apply(Solver &s, const double *X, int64_t ldx, const double *Bv, double 
     p.ldy = s.n;
     p.nr = std::min(RNR, nr - c0);
     p.sa = sa;
+    p.skip = s.skip;
     const int grid = (s.n + RR - 1) / RR;
     if (s.upper) {
       if (abs_a) sym_apply_kernel<true, true><<<grid, 256, 0, ctx->stream>>>(p);
@@ -365,15 +463,11 @@ int colmax(Solver &s, const double *V, int64_t ld, int n, int nr, double *out) {
   return MO_OK;
 }
 
-// D = M^-1 D in place (D: packed n x nr); RHS in groups of 64
+// D = M^-1 D in place (D: packed n x nr): L^-1 then L^-T, block-inverse solves
 int precond(Solver &s, double *D) {
-  for (int c0 = 0; c0 < s.nr; c0 += 64) {
-    const View B{D + (int64_t)c0 * s.n, s.n, std::min(64, s.nr - c0), s.n};
-    int rc = trsm_few_f32(s.ctx, B, s.f.W, s.f.ldw, s.n, false, s.f.inv, s.flags);
-    if (!rc) rc = trsm_few_f32(s.ctx, B, s.f.W, s.f.ldw, s.n, true, s.f.inv, s.flags);
-    if (rc) return rc;
-  }
-  return MO_OK;
+  int rc = lp_solve_apply(s.ctx, s.ls, s.n, D, s.n, s.nr, false, s.skip);
+  if (!rc) rc = lp_solve_apply(s.ctx, s.ls, s.n, D, s.n, s.nr, true, s.skip);
+  return rc;
 }
 
 // h(0..nv-1, :) = V_0..nv-1^T W per column; root: h = sqrt(W^T W) (nv = 1, V = W)
@@ -382,10 +476,10 @@ int dots(Solver &s, const double *V, int nv, const double *W, double *h, bool ro
   ProfScope ps;
   prof_begin(s.ctx, ps, MO_PROF_IR);
   dots_kernel<<<dim3(s.nblk_dot, s.nr), 256, 0, st>>>(V, (int64_t)s.n * s.nr, nv, W, s.n, s.nr,
-                                                      s.partial, s.pstride);
+                                                      s.partial, s.pstride, s.skip);
   const int m = nv * s.nr;
   dots_reduce_kernel<<<(m + 127) / 128, 128, 0, st>>>(s.partial, s.pstride, s.nblk_dot, nv, s.nr,
-                                                      h, root);
+                                                      h, root, s.skip);
   prof_end(s.ctx, ps, 2.0 * s.n * (double)s.nr * nv, 8.0 * s.n * (double)s.nr * (nv + 1));
   MO_CUDA_TRY(cudaGetLastError());
   return MO_OK;
@@ -395,36 +489,54 @@ int vupdate(Solver &s, double *W, const double *V, int nv, const double *h, doub
   ProfScope ps;
   prof_begin(s.ctx, ps, MO_PROF_IR);
   vupdate_kernel<<<vgrid(s.n, s.nr), 256, 0, s.ctx->stream>>>(W, V, (int64_t)s.n * s.nr, nv, h,
-                                                              s.n, s.nr, sign);
+                                                              s.n, s.nr, sign, s.skip);
   prof_end(s.ctx, ps, 2.0 * s.n * (double)s.nr * nv, 8.0 * s.n * (double)s.nr * (nv + 2));
   MO_CUDA_TRY(cudaGetLastError());
   return MO_OK;
 }
 
 // d = GMRES(A, r) preconditioned on the left by M^-1, at most kGmresMax iterations, until
-// every column's preconditioned residual has dropped by tau; *its receives the iterations
+// every column's preconditioned residual has dropped by tau; *its receives the iterations.
+// The Hessenberg matrix, the Givens rotations and the convergence test live on the device
+// (gmres_givens_kernel); the host enqueues iterations up to kGmresLag ahead of the last
+// test it has seen (read through pinned memory and one event per iteration, without
+// stopping the stream), and iterations enqueued past convergence return at once (their
+// kernels test the same device word).
+constexpr int kGmresLag = 2;
+
+int gmres_slots(mo_ctx *ctx) {
+  if (!ctx->h_gmres) MO_CUDA_TRY(cudaHostAlloc((void **)&ctx->h_gmres, 64 * sizeof(int) * 2, 0));
+  while ((int)ctx->gmres_ev.size() < kGmresMax) {
+    cudaEvent_t e;
+    MO_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    ctx->gmres_ev.push_back(e);
+  }
+  return MO_OK;
+}
+
 int gmres(Solver &s, double tau, int *its) {
   const int n = s.n, nr = s.nr;
   const int64_t vs = (int64_t)n * nr;
-  cudaStream_t st = s.ctx->stream;
+  mo_ctx *ctx = s.ctx;
+  cudaStream_t st = ctx->stream;
   int rc;
+  if ((rc = gmres_slots(ctx))) return rc;
   MO_CUDA_TRY(cudaMemcpyAsync(s.d, s.r, sizeof(double) * vs, cudaMemcpyDeviceToDevice, st));
   if ((rc = precond(s, s.d))) return rc;
   if ((rc = dots(s, s.d, 1, s.d, s.scal, true))) return rc;  // beta = |M^-1 r|_2
-  vscale_kernel<<<vgrid(n, nr), 256, 0, st>>>(s.V, s.d, s.scal, n, nr);
-  std::vector<double> beta(nr);
-  MO_CUDA_TRY(cudaMemcpyAsync(beta.data(), s.scal, sizeof(double) * nr, cudaMemcpyDeviceToHost, st));
-  MO_CUDA_TRY(cudaStreamSynchronize(st));
-  // per column c: R (rotated Hessenberg, column-major (kGmresMax+1) x kGmresMax), the
-  // rotations (cs, sn) and the rotated right-hand side g
-  const int LDR = kGmresMax + 1;
-  std::vector<double> R((size_t)LDR * kGmresMax * nr, 0.0), cs((size_t)kGmresMax * nr, 1.0),
-      sn((size_t)kGmresMax * nr, 0.0), g((size_t)LDR * nr, 0.0);
-  auto Rat = [&](int i, int j, int c) -> double & { return R[((size_t)c * kGmresMax + j) * LDR + i]; };
-  for (int c = 0; c < nr; ++c) g[(size_t)c * LDR] = beta[c];
-  std::vector<double> h1((size_t)(kGmresMax + 1) * nr), h2((size_t)(kGmresMax + 1) * nr), hn(nr);
+  vscale_kernel<<<vgrid(n, nr), 256, 0, st>>>(s.V, s.d, s.scal, n, nr, nullptr);
+  gmres_start_kernel<<<1, 256, 0, st>>>(s.gs, s.scal, nr);
+  MO_CUDA_TRY(cudaGetLastError());
+  int *hd = ctx->h_gmres;  // hd[2 j], hd[2 j + 1]: done word and count after iteration j
+  s.skip = s.gs.done;
   int m = 0;
   for (int j = 0; j < kGmresMax; ++j) {
+    // the convergence test of iteration j - kGmresLag, once the device has passed it
+    if (j - kGmresLag >= 0) {
+      const int q = j - kGmresLag;
+      MO_CUDA_TRY(cudaEventSynchronize(ctx->gmres_ev[q]));
+      if (hd[2 * q]) break;
+    }
     double *vj = s.V + j * vs, *w = s.V + (j + 1) * vs;
     if ((rc = sym_apply(s, vj, n, nullptr, w, 1.0, false, nr))) return rc;  // w = A v_j
     if ((rc = precond(s, w))) return rc;                                     // w = M^-1 w
@@ -434,53 +546,23 @@ int gmres(Solver &s, double tau, int *its) {
     if ((rc = dots(s, s.V, j + 1, w, s.h2, false))) return rc;
     if ((rc = vupdate(s, w, s.V, j + 1, s.h2, -1.0))) return rc;
     if ((rc = dots(s, w, 1, w, s.scal, true))) return rc;  // |w|_2
-    vscale_kernel<<<vgrid(n, nr), 256, 0, st>>>(w, w, s.scal, n, nr);
+    vscale_kernel<<<vgrid(n, nr), 256, 0, st>>>(w, w, s.scal, n, nr, s.skip);
+    gmres_givens_kernel<<<1, 256, 0, st>>>(s.gs, s.h, s.h2, s.scal, j, nr, tau,
+                                           j == kGmresMax - 1);
     MO_CUDA_TRY(cudaGetLastError());
-    MO_CUDA_TRY(cudaMemcpyAsync(h1.data(), s.h, sizeof(double) * (j + 1) * nr,
-                                cudaMemcpyDeviceToHost, st));
-    MO_CUDA_TRY(cudaMemcpyAsync(h2.data(), s.h2, sizeof(double) * (j + 1) * nr,
-                                cudaMemcpyDeviceToHost, st));
-    MO_CUDA_TRY(cudaMemcpyAsync(hn.data(), s.scal, sizeof(double) * nr, cudaMemcpyDeviceToHost, st));
-    MO_CUDA_TRY(cudaStreamSynchronize(st));
-    m = j + 1;
-    double worst = 0.0;
-    for (int c = 0; c < nr; ++c) {
-      for (int i = 0; i <= j; ++i) Rat(i, j, c) = h1[(size_t)i * nr + c] + h2[(size_t)i * nr + c];
-      Rat(j + 1, j, c) = hn[c];
-      for (int i = 0; i < j; ++i) {  // earlier rotations
-        const double a = Rat(i, j, c), b = Rat(i + 1, j, c);
-        const double cc = cs[(size_t)c * kGmresMax + i], ss = sn[(size_t)c * kGmresMax + i];
-        Rat(i, j, c) = cc * a + ss * b;
-        Rat(i + 1, j, c) = -ss * a + cc * b;
-      }
-      const double a = Rat(j, j, c), b = Rat(j + 1, j, c);
-      const double rr = std::hypot(a, b);
-      const double cc = rr > 0.0 ? a / rr : 1.0, ss = rr > 0.0 ? b / rr : 0.0;
-      cs[(size_t)c * kGmresMax + j] = cc;
-      sn[(size_t)c * kGmresMax + j] = ss;
-      Rat(j, j, c) = rr;
-      Rat(j + 1, j, c) = 0.0;
-      double &gj = g[(size_t)c * LDR + j];
-      g[(size_t)c * LDR + j + 1] = -ss * gj;
-      gj = cc * gj;
-      if (beta[c] > 0.0) worst = std::max(worst, std::fabs(g[(size_t)c * LDR + j + 1]) / beta[c]);
-    }
-    if (worst <= tau) break;
+    MO_CUDA_TRY(cudaMemcpyAsync(hd + 2 * j, s.gs.done, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    MO_CUDA_TRY(cudaEventRecord(ctx->gmres_ev[j], st));
   }
-  // y = R^-1 g (m x m upper triangular, per column), d = V y
-  std::vector<double> y((size_t)m * nr, 0.0);
-  for (int c = 0; c < nr; ++c)
-    for (int i = m - 1; i >= 0; --i) {
-      double t = g[(size_t)c * LDR + i];
-      for (int k = i + 1; k < m; ++k) t -= Rat(i, k, c) * y[(size_t)k * nr + c];
-      const double dii = Rat(i, i, c);
-      y[(size_t)i * nr + c] = dii != 0.0 ? t / dii : 0.0;
-    }
-  MO_CUDA_TRY(cudaMemcpyAsync(s.h, y.data(), sizeof(double) * m * nr, cudaMemcpyHostToDevice, st));
+  s.skip = nullptr;
+  MO_CUDA_TRY(cudaMemcpyAsync(hd, s.gs.done, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+  MO_CUDA_TRY(cudaStreamSynchronize(st));
+  m = hd[1];
+  if (m <= 0) return MO_EDEVTIMEOUT;  // the last iteration always sets the count
+  // y = R^-1 g per column (device), d = V y
+  gmres_backsolve_kernel<<<1, 256, 0, st>>>(s.gs, m, nr, s.h);
+  MO_CUDA_TRY(cudaGetLastError());
   MO_CUDA_TRY(cudaMemsetAsync(s.d, 0, sizeof(double) * vs, st));
   if ((rc = vupdate(s, s.d, s.V, m, s.h, 1.0))) return rc;
-  // y lives in host memory only until the copy above has run
-  MO_CUDA_TRY(cudaStreamSynchronize(st));
   *its = m;
   return MO_OK;
 }
@@ -491,10 +573,14 @@ size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 size_t ir_bytes(int n, int nr, int prec, bool gmres_possible) {
   const size_t vec = align256((size_t)n * nr * 8);
   const int nblk_dot = (n + DOT_ROWS - 1) / DOT_ROWS;
-  size_t b = lp_chol_bytes(n, prec) + 4 * vec;
+  const int NP = ((n + 127) / 128) * 128;
+  size_t b = align256(lp_chol_bytes(n, prec)) + align256(lp_solve_bytes(NP, nr)) + 4 * vec;
   if (nr >= kGemmResidualMinRhs) b += align256((size_t)n * n * 8);
   if (gmres_possible) b += (kGmresMax + 1) * vec;
   b += 2 * align256((size_t)(kGmresMax + 1) * nr * 8) + align256((size_t)nr * 8);
+  if (gmres_possible)
+    b += align256((size_t)nr * kGmresMax * (kGmresMax + 1) * 8) + 2 * align256((size_t)nr * kGmresMax * 8) +
+         align256((size_t)nr * (kGmresMax + 1) * 8) + align256((size_t)nr * 8) + 256;
   b += align256((size_t)nblk_dot * (kGmresMax + 2) * nr * 8);
   b += align256((size_t)(3 * nr + 1) * 8) + align256((size_t)(128 * ((n + 63) / 64) + 64) * 4) + 4096;
   return b;
@@ -572,7 +658,10 @@ int dsposv(mo_ctx *ctx, const View &X, const View &A, const View &B, bool upper,
   s.n = n;
   s.nr = nr;
   const bool gm = method != MO_IR_CLASSIC;
-  const size_t need = ir_bytes(n, nr, prec, gm);
+  // BF16x3 under MO_IR_AUTO may move to the TF32x3 factor (see below): room for either
+  const bool may_switch = prec == kLpBf16x3 && method == MO_IR_AUTO;
+  const int ws_prec = may_switch ? kLpTf32x3 : prec;
+  const size_t need = ir_bytes(n, nr, ws_prec, gm);
   if (need > ctx->ws_ir_bytes) {
     MO_CUDA_TRY(cudaStreamSynchronize(st));
     if (ctx->ws_ir) cudaFree(ctx->ws_ir);
@@ -587,7 +676,10 @@ int dsposv(mo_ctx *ctx, const View &X, const View &A, const View &B, bool upper,
     p += align256(bytes);
     return r;
   };
-  lp_chol_setup(n, prec, take(lp_chol_bytes(n, prec)), s.f);
+  void *chol_mem = take(lp_chol_bytes(n, ws_prec));
+  lp_chol_setup(n, prec, chol_mem, s.f);
+  info.prec = prec == kLpBf16x3 ? MO_PREC_BF16X3 : MO_PREC_TF32X3;
+  lp_solve_setup(s.f.NP, nr, take(lp_solve_bytes(s.f.NP, nr)), s.ls);
   const size_t vec = (size_t)n * nr * 8;
   s.b = (double *)take(vec);
   s.x = (double *)take(vec);
@@ -598,6 +690,14 @@ int dsposv(mo_ctx *ctx, const View &X, const View &A, const View &B, bool upper,
   s.h = (double *)take((size_t)(kGmresMax + 1) * nr * 8);
   s.h2 = (double *)take((size_t)(kGmresMax + 1) * nr * 8);
   s.scal = (double *)take((size_t)nr * 8);
+  if (gm) {
+    s.gs.R = (double *)take((size_t)nr * kGmresMax * (kGmresMax + 1) * 8);
+    s.gs.cs = (double *)take((size_t)nr * kGmresMax * 8);
+    s.gs.sn = (double *)take((size_t)nr * kGmresMax * 8);
+    s.gs.g = (double *)take((size_t)nr * (kGmresMax + 1) * 8);
+    s.gs.beta = (double *)take((size_t)nr * 8);
+    s.gs.done = (int *)take(256);
+  }
   s.nblk_dot = (n + DOT_ROWS - 1) / DOT_ROWS;
   s.pstride = (kGmresMax + 2) * nr;
   s.partial = (double *)take((size_t)s.nblk_dot * s.pstride * 8);
@@ -622,16 +722,19 @@ int dsposv(mo_ctx *ctx, const View &X, const View &A, const View &B, bool upper,
   if ((rc = colmax(s, s.b, n, n, nr, s.norms + 2 * nr))) return rc;
   // low-precision factorization, shifted on breakdown
   Control *cb = control(ctx);
-  const double s0 = prec == kLpBf16x3 ? 0x1p-15 : 0x1p-22;
+  auto first_shift = [](int p) { return p == kLpBf16x3 ? 0x1p-15 : 0x1p-22; };
   double shift = 0.0;
   bool factored = false;
+  double t_fact = 0.0;  // host seconds of the last factorization attempt
   for (int attempt = 0; attempt < 5; ++attempt) {
+    const auto f0 = std::chrono::steady_clock::now();
     MO_CUDA_TRY(cudaMemsetAsync(&cb->info, 0, sizeof(Control) - offsetof(Control, info), st));
     if ((rc = lp_chol_convert(ctx, s.f, A, upper, shift))) return rc;
     if ((rc = lp_chol_factor(ctx, s.f, &cb->info, &cb->bad))) return rc;
     Control h;
+    MO_CUDA_TRY(cudaMemcpyAsync(&h, cb, sizeof(h), cudaMemcpyDeviceToHost, st));
     MO_CUDA_TRY(cudaStreamSynchronize(st));
-    MO_CUDA_TRY(cudaMemcpy(&h, cb, sizeof(h), cudaMemcpyDeviceToHost));
+    t_fact = std::chrono::duration<double>(std::chrono::steady_clock::now() - f0).count();
     if (h.status) {
       cudaMemset(&cb->status, 0, sizeof(int));
       return h.status;
@@ -640,14 +743,28 @@ int dsposv(mo_ctx *ctx, const View &X, const View &A, const View &B, bool upper,
       factored = true;
       break;
     }
-    shift = shift == 0.0 ? s0 : shift * 8.0;
+    if (may_switch && s.f.prec == kLpBf16x3) {
+      // the BF16x3 factor (about 16 significant bits) broke down: kappa(A) is beyond what
+      // it can precondition well, so refactor with the TF32x3 split (FP32 accuracy), unshifted
+      lp_chol_setup(n, kLpTf32x3, chol_mem, s.f);
+      info.prec = MO_PREC_TF32X3;
+      shift = 0.0;
+    } else {
+      shift = shift == 0.0 ? first_shift(s.f.prec) : shift * 8.0;
+    }
     info.shifts += 1;
   }
   info.shift = factored ? shift : 0.0;
+  if (factored && (rc = lp_solve_prepare(ctx, s.f, s.ls))) return rc;
   std::vector<double> nh(3 * nr + 1);
   double prev = INFINITY;
   bool use_gmres = method == MO_IR_GMRES;
   int stall = 0;
+  // the FP64 path (factor + solve) costs about kFp64OverLp times the split-product factor
+  // (measured at n = 16384: 73.5 ms against about 20 ms); a refinement whose projected
+  // remaining cost exceeds that is abandoned for the fallback
+  constexpr double kFp64OverLp = 3.0;
+  auto t_step0 = std::chrono::steady_clock::now();
   if (factored) {
     MO_CUDA_TRY(cudaMemsetAsync(s.x, 0, vec, st));
     for (int it = 0;; ++it) {
@@ -665,6 +782,19 @@ int dsposv(mo_ctx *ctx, const View &X, const View &A, const View &B, bool upper,
         break;
       }
       if (it >= maxit || !std::isfinite(berr)) break;
+      const auto now = std::chrono::steady_clock::now();
+      const double t_step = std::chrono::duration<double>(now - t_step0).count();
+      t_step0 = now;
+      // GMRES-IR steps so far: project the steps still needed from the last reduction and
+      // fall back once they would cost more than the FP64 path
+      if (fallback_ok && method == MO_IR_AUTO && it > 0 && info.method == MO_IR_GMRES &&
+          berr < prev) {
+        const double need = std::ceil(std::log(tol / berr) / std::log(berr / prev));
+        if (need * t_step > kFp64OverLp * t_fact) {
+          info.abandoned = 1;
+          break;
+        }
+      }
       // a step that did not reduce berr 20x: switch to GMRES-IR (auto), else count stalls
       if (it > 0 && berr > 0.05 * prev) {
         if (method == MO_IR_AUTO && !use_gmres) use_gmres = true;

@@ -44,5 +44,15 @@ void dmvec_solve_blocked(mvec_t *X, const mdata_t *A, int flags, int N, int NB);
 double dvec_dot(const mvec_t *X, const mvec_t *Y, double alpha, int N);
 void dvec_invscal(mvec_t *X, double alpha, int N);
 void dvec_swap(mvec_t *X, mvec_t *Y, int N);
+/* the rest of the level-3 surface (calgo/cmops.h:149-152, 200-201, 218-226) */
+void dmult_symm_blocked2(mdata_t *C, const mdata_t *A, const mdata_t *B,
+                         double alpha, double beta, int flags,
+                         int P, int S, int L, int R, int E, int vlen, int NB, int MB);
+void dmmat_trmm_blk(mdata_t *B, const mdata_t *A, double alpha, int flags,
+                    int N, int S, int E, int NB);
+void dmmat_rank2_blk(mdata_t *C, const mdata_t *A, const mdata_t *B,
+                     double alpha, double beta, int flags, int P, int S, int E, int vlen, int NB);
+void dmmat_trmupd_blk(mdata_t *C, const mdata_t *A, const mdata_t *B, double alpha, double beta,
+                      int flags, int P, int S, int E, int vlen, int NB);
 
 #endif

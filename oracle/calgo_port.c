@@ -245,3 +245,125 @@ void dvec_swap(mvec_t *X, mvec_t *Y, int N) {
     Y->md[(long)i * Y->inc] = t;
   }
 }
+
+/* ---------------- the rest of the level-3 surface ---------------- */
+
+/* element (i, j) of the symmetric matrix whose UPPER (flags & MTX_UPPER) or LOWER triangle A
+ * stores (calgo/dmmat_symm.c:253-390 reads only that triangle) */
+static inline double sym_at(const mdata_t *A, int flags, int i, int j) {
+  const int up = (flags & MTX_UPPER) != 0;
+  if (up ? i <= j : i >= j) return AT(A, i, j);
+  return AT(A, j, i);
+}
+
+/* calgo/dmmat_symm.c:253-390 (dmult_symm_blocked2): C[R:E, S:L] = beta*C + alpha*A*B with
+ * MTX_LEFT, else beta*C + alpha*op(B)*A (op(B) = B^T with MTX_TRANSB); A (P x P) symmetric.
+ * The left branch reads B untransposed whatever MTX_TRANSB says (the reference's kernel
+ * never consults it there). */
+void dmult_symm_blocked2(mdata_t *C, const mdata_t *A, const mdata_t *B, double alpha,
+                         double beta, int flags, int P, int S, int L, int R, int E, int vlen,
+                         int NB, int MB) {
+  (void)vlen; (void)NB; (void)MB;
+  if (L - S <= 0 || E - R <= 0) return;
+  scale_tile(&AT(C, R, S), C->step, beta, E - R, L - S);
+  for (int j = S; j < L; j++)
+    for (int i = R; i < E; i++) {
+      double s = 0.0;
+      for (int p = 0; p < P; p++) {
+        if (flags & MTX_LEFT) s += sym_at(A, flags, i, p) * AT(B, p, j);
+        else s += ((flags & MTX_TRANSB) ? AT(B, p, i) : AT(B, i, p)) * sym_at(A, flags, p, j);
+      }
+      AT(C, i, j) += alpha * s;
+    }
+}
+
+/* element (i, k) of op(A) for the triangular A of TRMM (flags: UPPER / LOWER, TRANSA, UNIT) */
+static inline double tri_op(const mdata_t *A, int flags, int i, int k) {
+  const int r = (flags & MTX_TRANSA) ? k : i, c = (flags & MTX_TRANSA) ? i : k;
+  const int up = (flags & MTX_UPPER) != 0;
+  if (up ? r > c : r < c) return 0.0;
+  if (r == c && (flags & MTX_UNIT)) return 1.0;
+  return AT(A, r, c);
+}
+
+/* calgo/dmmat_trid.c:780-830 (dmmat_trmm_blk): B = alpha*op(A)*B (columns S..E-1 of B) or
+ * alpha*B*op(A) with MTX_RIGHT (rows S..E-1 of B); A is N x N triangular */
+void dmmat_trmm_blk(mdata_t *B, const mdata_t *A, double alpha, int flags, int N, int S, int E,
+                    int NB) {
+  (void)NB;
+  if (E - S <= 0 || N <= 0) return;
+  double *t = malloc(sizeof(double) * N);
+  for (int v = S; v < E; v++) {
+    /* v: a column of B (left) or a row of B (right) */
+    for (int i = 0; i < N; i++) {
+      double s = 0.0;
+      for (int k = 0; k < N; k++) {
+        if (flags & MTX_RIGHT) s += AT(B, v, k) * tri_op(A, flags, k, i);
+        else s += tri_op(A, flags, i, k) * AT(B, k, v);
+      }
+      t[i] = alpha * s;
+    }
+    for (int i = 0; i < N; i++) {
+      if (flags & MTX_RIGHT) AT(B, v, i) = t[i];
+      else AT(B, i, v) = t[i];
+    }
+  }
+  free(t);
+}
+
+static inline int in_tri(int flags, int i, int j) {
+  return (flags & MTX_UPPER) ? i <= j : i >= j;
+}
+
+/* calgo/dmmat_rank.c:132-235 (dmmat_rank2_blk): the triangle of C[S:E, S:E] gets
+ * alpha*(A*B^T + B*A^T) (alpha*(A^T*B + B^T*A) with MTX_TRANSA).  beta is applied inside the
+ * NB x NB diagonal blocks only (dmmat_rank.c:167, 196), and without MTX_TRANSA a second time
+ * before the second product (dmmat_rank.c:228): the diagonal blocks become
+ * beta^2 C + beta alpha A B^T + alpha B A^T there.  Off the diagonal blocks beta is not
+ * applied.  NB as in dmmat_rank.c:146-154. */
+void dmmat_rank2_blk(mdata_t *C, const mdata_t *A, const mdata_t *B, double alpha, double beta,
+                     int flags, int P, int S, int E, int vlen, int NB) {
+  (void)vlen;
+  if (E - S <= 0 || P <= 0) return;
+  if (NB > MAX_VP_COLS || NB <= 0) NB = MAX_VP_COLS;
+  if (NB > E - S) NB = E - S;
+  const int ta = (flags & MTX_TRANSA) != 0;
+  for (int j = S; j < E; j++)
+    for (int i = S; i < E; i++) {
+      if (!in_tri(flags, i, j)) continue;
+      double ab = 0.0, ba = 0.0;
+      for (int p = 0; p < P; p++) {
+        const double ai = ta ? AT(A, p, i) : AT(A, i, p), aj = ta ? AT(A, p, j) : AT(A, j, p);
+        const double bi = ta ? AT(B, p, i) : AT(B, i, p), bj = ta ? AT(B, p, j) : AT(B, j, p);
+        ab += ai * bj;
+        ba += bi * aj;
+      }
+      const int diag = (i - S) / NB == (j - S) / NB;
+      double c = AT(C, i, j);
+      if (diag) c = (beta == 0.0) ? 0.0 : (beta == 1.0 ? c : beta * c);
+      c += alpha * ab;
+      if (diag && !ta) c = (beta == 0.0) ? 0.0 : (beta == 1.0 ? c : beta * c);
+      c += alpha * ba;
+      AT(C, i, j) = c;
+    }
+}
+
+/* calgo/dmmat_rank.c:292-355 (dmmat_trmupd_blk): the triangle of C[S:E, S:E] =
+ * beta*C + alpha*op(A)*op(B), beta applied inside the NB x NB diagonal blocks only
+ * (_dmmat_trmupd_diag); NB as in dmmat_rank.c:306-314 */
+void dmmat_trmupd_blk(mdata_t *C, const mdata_t *A, const mdata_t *B, double alpha, double beta,
+                      int flags, int P, int S, int E, int vlen, int NB) {
+  (void)vlen;
+  if (E - S <= 0 || P <= 0) return;
+  if (NB > MAX_VP_COLS || NB <= 0) NB = MAX_VP_COLS;
+  if (NB > E - S) NB = E - S;
+  for (int j = S; j < E; j++)
+    for (int i = S; i < E; i++) {
+      if (!in_tri(flags, i, j)) continue;
+      double s = 0.0;
+      for (int p = 0; p < P; p++) s += opA(A, flags, i, p) * opB(B, flags, p, j);
+      double c = AT(C, i, j);
+      if ((i - S) / NB == (j - S) / NB) c = (beta == 0.0) ? 0.0 : (beta == 1.0 ? c : beta * c);
+      AT(C, i, j) = c + alpha * s;
+    }
+}

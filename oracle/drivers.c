@@ -27,7 +27,8 @@ enum {
   OR_EPIVLEN = -3,      /* "pivot array < min(A.Rows(),A.Cols())" lu.go:260-262 */
   OR_ECNOTSQUARE = -4,  /* "C not a square matrix"           mmult.go:428 */
   OR_EABSIZE = -5,      /* "A, B size mismatch"              mmult.go:406 */
-  OR_ENOTVECTOR = -6    /* "X not a vector." / "Y not a vector."  mvec.go:34-37 */
+  OR_ENOTVECTOR = -6,   /* "X not a vector." / "Y not a vector."  mvec.go:34-37 */
+  OR_ESYMSIZE = -7      /* "MultSym: size mismatch"          mmult.go:290 */
 };
 
 /* package globals, mmult.go:33-41 */
@@ -240,6 +241,79 @@ int or_rank_update_sym_fm(fm C, fm A, double alpha, double beta, int flags) {
   return OR_OK;
 }
 
+/* ---------------- the rest of mmult.go's level-3 surface ---------------- */
+
+/* mmult.go:266-330 (MultSym); errors.New("MultSym: size mismatch") -> OR_ESYMSIZE */
+int or_mult_sym_fm(fm C, fm A, fm B, double alpha, double beta, int flags) {
+  int ok, empty;
+  int ar = A.r, ac = A.c, br = B.r, bc = B.c, cr = C.r, cc = C.c;
+  switch (flags & (MTX_TRANSA | MTX_TRANSB)) {
+  case MTX_TRANSA | MTX_TRANSB:
+    empty = ac == 0 || br == 0;
+    ok = ar == ac && cr == ac && cc == br && ar == bc;
+    break;
+  case MTX_TRANSA:
+    empty = ac == 0 || bc == 0;
+    ok = ar == ac && cr == ac && cc == bc && ar == br;
+    break;
+  case MTX_TRANSB:
+    empty = ar == 0 || br == 0;
+    ok = ar == ac && cr == ar && cc == br && ac == bc;
+    break;
+  default:
+    empty = ar == 0 || bc == 0;
+    ok = ar == ac && cr == ar && cc == bc && ac == br;
+  }
+  if (empty) return OR_OK;
+  if (!ok) return OR_ESYMSIZE;
+  mdata_t c = {C.d, C.ld}, a = {A.d, A.ld}, b = {B.d, B.ld};
+  /* the worker split of mmult.go:311-321 partitions C only; one call covers it */
+  dmult_symm_blocked2(&c, &a, &b, alpha, beta, flags, A.c, 0, C.c, 0, C.r, vpLen, nB, mB);
+  return OR_OK;
+}
+
+/* mmult.go:338-375 (MultTrm) */
+int or_mult_trm_fm(fm B, fm A, double alpha, int flags) {
+  int ok = 1, empty = 0;
+  switch (flags & (MTX_LEFT | MTX_RIGHT)) {
+  case MTX_LEFT:
+    empty = B.r == 0 || B.c == 0;
+    ok = B.r == A.c && A.c == A.r;
+    break;
+  case MTX_RIGHT:
+    empty = B.c == 0 || B.r == 0;
+    ok = B.c == A.r && A.c == A.r;
+    break;
+  }
+  if (empty) return OR_OK;
+  if (!ok) return OR_EABSIZE;
+  int E = (flags & MTX_RIGHT) ? B.r : B.c;
+  if (A.c == 0 || E <= 0) return OR_OK; /* calgo/cmops.go:153-155 */
+  mdata_t b = {B.d, B.ld}, a = {A.d, A.ld};
+  dmmat_trmm_blk(&b, &a, alpha, flags, A.c, 0, E, nB);
+  return OR_OK;
+}
+
+/* mmult.go:453-475 (RankUpdate2Sym) */
+int or_rank_update2_sym_fm(fm C, fm A, fm B, double alpha, double beta, int flags) {
+  if (C.r != C.c) return OR_ECNOTSQUARE;
+  int P = (flags & MTX_TRANSA) ? A.r : A.c;
+  if (P == 0 || C.r == 0) return OR_OK; /* calgo/cmops.go:252-254 */
+  mdata_t c = {C.d, C.ld}, a = {A.d, A.ld}, b = {B.d, B.ld};
+  dmmat_rank2_blk(&c, &a, &b, alpha, beta, flags, P, 0, C.r, vpLen, nB);
+  return OR_OK;
+}
+
+/* mmult.go:501-523 (UpdateTrm) */
+int or_update_trm_fm(fm C, fm A, fm B, double alpha, double beta, int flags) {
+  if (C.r != C.c) return OR_ECNOTSQUARE;
+  int P = (flags & MTX_TRANSA) ? A.r : A.c;
+  if (P == 0 || C.r == 0) return OR_OK; /* calgo/cmops.go:281-283 */
+  mdata_t c = {C.d, C.ld}, a = {A.d, A.ld}, b = {B.d, B.ld};
+  dmmat_trmupd_blk(&c, &a, &b, alpha, beta, flags, P, 0, C.r, vpLen, nB);
+  return OR_OK;
+}
+
 /* ---------------- chol.go ---------------- */
 
 /* chol.go:17-56 (unblockedCHOL); returns k+1 for the panic at absolute column k */
@@ -444,6 +518,26 @@ int or_solve_lu(double *B, int br, int bc, int ldb, double *A, int ar, int ac, i
                 int npiv, int flags) {
   pv p = {piv, npiv};
   return or_solve_lu_fm(FM(B, br, bc, ldb), FM(A, ar, ac, lda), p, flags);
+}
+int or_mult_sym(double *C, int cr, int cc, int ldc, double *A, int ar, int ac, int lda,
+                double *B, int br, int bc, int ldb, double alpha, double beta, int flags) {
+  return or_mult_sym_fm(FM(C, cr, cc, ldc), FM(A, ar, ac, lda), FM(B, br, bc, ldb), alpha, beta,
+                        flags);
+}
+int or_mult_trm(double *B, int br, int bc, int ldb, double *A, int ar, int ac, int lda,
+                double alpha, int flags) {
+  return or_mult_trm_fm(FM(B, br, bc, ldb), FM(A, ar, ac, lda), alpha, flags);
+}
+int or_rank_update2_sym(double *C, int cr, int cc, int ldc, double *A, int ar, int ac, int lda,
+                        double *B, int br, int bc, int ldb, double alpha, double beta,
+                        int flags) {
+  return or_rank_update2_sym_fm(FM(C, cr, cc, ldc), FM(A, ar, ac, lda), FM(B, br, bc, ldb),
+                                alpha, beta, flags);
+}
+int or_update_trm(double *C, int cr, int cc, int ldc, double *A, int ar, int ac, int lda,
+                  double *B, int br, int bc, int ldb, double alpha, double beta, int flags) {
+  return or_update_trm_fm(FM(C, cr, cc, ldc), FM(A, ar, ac, lda), FM(B, br, bc, ldb), alpha, beta,
+                          flags);
 }
 /* mmult.go:69-73 */
 int or_num_workers(int n) {

@@ -32,6 +32,7 @@ ERRORS = {
     -4: "C not a square matrix",
     -5: "A, B size mismatch",
     -6: "X not a vector.",
+    -7: "MultSym: size mismatch",
 }
 
 
@@ -73,6 +74,10 @@ class Oracle:
         L.or_decompose_chol.argtypes = M + [i, i]
         L.or_decompose_lu.argtypes = M + [p, i, i]
         L.or_decompose_chol_steps.argtypes = M + [i, i, i, i]
+        L.or_mult_sym.argtypes = M + M + M + [d, d, i]
+        L.or_mult_trm.argtypes = M + M + [d, i]
+        L.or_rank_update2_sym.argtypes = M + M + M + [d, d, i]
+        L.or_update_trm.argtypes = M + M + M + [d, d, i]
         L.or_solve_chol.argtypes = M + M + [i]
         L.or_solve_chol.restype = None
         L.or_solve_lu.argtypes = M + M + [p, i, i]
@@ -92,6 +97,18 @@ class Oracle:
 
     def DecomposeCHOL(self, A, flags, nb):
         return self.lib.or_decompose_chol(*view(A), flags, nb)
+
+    def MultSym(self, C, A, B, alpha, beta, flags):
+        return self.lib.or_mult_sym(*view(C), *view(A), *view(B), alpha, beta, flags)
+
+    def MultTrm(self, B, A, alpha, flags):
+        return self.lib.or_mult_trm(*view(B), *view(A), alpha, flags)
+
+    def RankUpdate2Sym(self, C, A, B, alpha, beta, flags):
+        return self.lib.or_rank_update2_sym(*view(C), *view(A), *view(B), alpha, beta, flags)
+
+    def UpdateTrm(self, C, A, B, alpha, beta, flags):
+        return self.lib.or_update_trm(*view(C), *view(A), *view(B), alpha, beta, flags)
 
     def DecomposeCHOLSteps(self, A, flags, nb, k0, k1):
         """blockedCHOL's block steps with first column in [k0, k1) (chol.go:58-94)"""

@@ -129,6 +129,40 @@ def main():
                 case[f"B{tr}"] = B
                 case[f"X{tr}"] = X
         put(f"lu_{m}_{n}_{nb}", **case)
+    # ---- the rest of the level-3 surface (mmult.go:266, :338, :453, :501) ----
+    for fl in [LEFT | LO, LEFT | UP, LEFT | LO | TA, RIGHT | LO, RIGHT | UP]:
+        n, p = (45, 7) if fl & LEFT else (45, 45)
+        A = F(rng.uniform(-1, 1, (n, n)))
+        B = F(rng.uniform(-1, 1, (n, p) if fl & LEFT else (p, n)))
+        C = F(rng.uniform(-1, 1, (n, p) if fl & LEFT else (p, n)))
+        R = F(C)
+        assert ref.MultSym(R, A, B, 1.5, -0.5, fl) == 0
+        put(f"symm_{fl:#x}", A=A, B=B, C=C, R=R, alpha=1.5, beta=-0.5, flags=fl)
+    for fl in [LEFT | LO, LEFT | UP | TA, RIGHT | LO | UNIT, RIGHT | UP | TA, LO | TA | UNIT]:
+        n = 75
+        A = F(rng.uniform(-1, 1, (n, n)))
+        B = F(rng.uniform(-1, 1, (6, n) if fl & RIGHT else (n, 6)))
+        R = F(B)
+        assert ref.MultTrm(R, A, 0.75, fl) == 0
+        put(f"trmm_{fl:#x}", A=A, B=B, R=R, alpha=0.75, flags=fl)
+    for fl in [LO, UP, LO | TA, UP | TA]:
+        for beta in [1.0, 0.5]:
+            n, k = 75, 6
+            A = F(rng.standard_normal((k, n) if fl & TA else (n, k)))
+            B = F(rng.standard_normal(A.shape))
+            C = F(rng.standard_normal((n, n)))
+            R = F(C)
+            assert ref.RankUpdate2Sym(R, A, B, 1.5, beta, fl) == 0
+            put(f"syr2k_{fl}_{beta}", A=A, B=B, C=C, R=R, alpha=1.5, beta=beta, flags=fl)
+    for fl in [LO, UP, LO | TA, UP | TB]:
+        for beta in [1.0, 0.5]:
+            n, k = 75, 6
+            A = F(rng.standard_normal((k, n) if fl & TA else (n, k)))
+            B = F(rng.standard_normal((n, k) if fl & TB else (k, n)))
+            C = F(rng.standard_normal((n, n)))
+            R = F(C)
+            assert ref.UpdateTrm(R, A, B, 1.5, beta, fl) == 0
+            put(f"trmupd_{fl}_{beta}", A=A, B=B, C=C, R=R, alpha=1.5, beta=beta, flags=fl)
     path = os.path.join(HERE, "golden.npz")
     np.savez_compressed(path, **out)
     print(path, len(out), "arrays")

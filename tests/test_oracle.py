@@ -91,6 +91,35 @@ def test_golden_lu(oracle, golden, name):
             assert rel(X, c[f"X{tr}"]) <= 1e-11
 
 
+@pytest.mark.parametrize("name", names("symm_"))
+def test_golden_mult_sym(oracle, golden, name):
+    c = golden[name]
+    R = F(c["C"])
+    assert oracle.MultSym(R, F(c["A"]), F(c["B"]), float(c["alpha"]), float(c["beta"]), int(c["flags"])) == 0
+    assert rel(R, c["R"]) <= 1e-13
+
+
+@pytest.mark.parametrize("name", names("trmm_"))
+def test_golden_mult_trm(oracle, golden, name):
+    c = golden[name]
+    R = F(c["B"])
+    assert oracle.MultTrm(R, F(c["A"]), float(c["alpha"]), int(c["flags"])) == 0
+    assert rel(R, c["R"]) <= 1e-13
+
+
+@pytest.mark.parametrize("name", names("syr2k_") + names("trmupd_"))
+def test_golden_rank2_and_trm_update(oracle, golden, name):
+    c = golden[name]
+    R = F(c["C"])
+    fn = oracle.RankUpdate2Sym if name.startswith("syr2k") else oracle.UpdateTrm
+    assert fn(R, F(c["A"]), F(c["B"]), float(c["alpha"]), float(c["beta"]), int(c["flags"])) == 0
+    assert rel(R, c["R"]) <= 1e-13
+    # the opposite strict triangle is untouched
+    n = R.shape[0]
+    other = np.triu(np.ones((n, n), bool), 1) if int(c["flags"]) & LO else np.tril(np.ones((n, n), bool), -1)
+    assert np.array_equal(R[other], c["C"][other])
+
+
 def test_golden_lu3x3_matches_lapack(golden):
     """decomp_test.go:85-108 compares against lapack.Getrf: pivots are LAPACK's minus one."""
     import scipy.linalg as sl
