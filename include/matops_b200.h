@@ -203,6 +203,14 @@ MO_API int mo_rank_update2_sym(mo_ctx *ctx, mo_matrix C, mo_matrix A, mo_matrix 
 MO_API int mo_update_trm(mo_ctx *ctx, mo_matrix C, mo_matrix A, mo_matrix B, double alpha,
                          double beta, int flags);
 
+/* InverseTrm(A, flags, nb), trinv.go:219-243: A := the inverse of its lower (MO_LOWER) or
+ * upper (otherwise) triangle, in place; MO_UNIT: unit diagonal, not read or written.  The
+ * opposite strict triangle is not touched.  Non-square A -> MO_ENOTSQUARE (the reference
+ * does not check).  nb is accepted; the device blocks by 128 and doubles.  No singularity
+ * check (a zero diagonal gives inf, as the reference's 1/a11).  Asynchronous; uses about
+ * 1.25 n^2 doubles of context workspace. */
+MO_API int mo_inverse_trm(mo_ctx *ctx, mo_matrix A, int flags, int nb);
+
 /* ---- factorizations and solves ---- */
 
 /* DecomposeCHOL(A, flags, nb), chol.go:116-127: A = L*L^T (MO_LOWER) or U^T*U (otherwise)

@@ -12,5 +12,5 @@ from .api import (  # noqa: F401
     MeasureFP64Peak, PREC_BF16X3, PREC_TF32X3, IR_AUTO, IR_CLASSIC, IR_GMRES, IR_NO_FALLBACK,
     IRInfo, SolveCHOLMixed, LPGemm, BATCH_CHOL, BATCH_LU, BATCH_MAX_N, BatchPlan,
     DecomposeCHOLAdjoint, DecomposeCHOLAdjointBatched, SolveCHOLAdjoint, SetSpinLimit, Mirror,
-    context, MultSym, MultTrm, RankUpdate2Sym, UpdateTrm,
+    context, MultSym, MultTrm, RankUpdate2Sym, UpdateTrm, InverseTrm,
 )

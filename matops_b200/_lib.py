@@ -60,6 +60,7 @@ def lib() -> ctypes.CDLL:
         "mo_mult_trm": [p, M, M, d, i],
         "mo_rank_update2_sym": [p, M, M, M, d, d, i],
         "mo_update_trm": [p, M, M, M, d, d, i],
+        "mo_inverse_trm": [p, M, i, i],
         "mo_mirror_create": [p, p, i64, ctypes.POINTER(p)],
         "mo_mirror_destroy": [p],
         "mo_mirror_find": [p, ctypes.POINTER(p), ctypes.POINTER(i64)],

@@ -155,6 +155,12 @@ def UpdateTrm(C, A, B, alpha: float, beta: float, flags: int):
                                          flags), True)
 
 
+def InverseTrm(A, flags: int, nb: int):
+    """trinv.go:219: A := inverse of its LOWER (else upper) triangle (UNIT: unit diagonal);
+    returns (A, err)"""
+    return A, _err(_lib.lib().mo_inverse_trm(context(), view(A), flags, nb))
+
+
 def DecomposeCHOL(A, flags: int, nb: int):
     """chol.go:116 -- returns (A, err); a non-positive pivot panics like the reference."""
     bad = ctypes.c_double(0.0)

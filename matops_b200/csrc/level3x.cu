@@ -71,6 +71,31 @@ int expand(mo_ctx *ctx, View A, int n, int mode, bool unit, double *D) {
   return MO_OK;
 }
 
+// T's 128 x 128 diagonal blocks <- the block inverses (nblk x 128 x 128, ld 128)
+__global__ void __launch_bounds__(256) place_diag_kernel(const double *inv, double *T, int64_t ldt,
+                                                         int n) {
+  const int q = blockIdx.x, r0 = q * 128, h = min(128, n - r0);
+  const double *src = inv + (size_t)q * 128 * 128;
+  for (int e = threadIdx.x; e < 128 * 128; e += 256) {
+    const int i = e & 127, j = e >> 7;
+    if (i < h && j < h) T[(r0 + i) + (int64_t)(r0 + j) * ldt] = src[e];
+  }
+}
+
+// A's triangle (lower or upper; strict with unit) <- T's
+__global__ void __launch_bounds__(256) tri_back_kernel(const double *T, int64_t ldt, double *A,
+                                                       int64_t lda, int n, int lower, int unit) {
+  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  if (lower ? i0 + 31 < j0 : j0 + 31 < i0) return;
+  for (int e = threadIdx.x; e < 32 * 32; e += 256) {
+    const int i = i0 + (e & 31), j = j0 + (e >> 5);
+    if (i >= n || j >= n) continue;
+    if (lower ? i < j : i > j) continue;
+    if (unit && i == j) continue;
+    A[i + (int64_t)j * lda] = T[i + (int64_t)j * ldt];
+  }
+}
+
 // the diagonal-block size of the reference's beta (calgo/dmmat_rank.c:146-154), or 0 for
 // BLAS semantics / beta == 1
 int beta_block_of(mo_ctx *ctx, double beta, int n) {
@@ -82,6 +107,9 @@ int beta_block_of(mo_ctx *ctx, double beta, int n) {
 }
 
 }  // namespace
+
+int trtri_blocks(mo_ctx *ctx, View A, int N, bool trans, bool lower_eff, bool unit, double *inv);
+
 }  // namespace mo
 
 using mo::View;
@@ -219,6 +247,67 @@ int mo_update_trm(mo_ctx *ctx, mo_matrix Cm, mo_matrix Am, mo_matrix Bm, double 
   o.mode = (flags & MO_UPPER) ? mo::kSyrkUpper : mo::kSyrkLower;
   o.beta_block = mo::beta_block_of(ctx, beta, n);
   return mo::gemm_ex(ctx, C, A, ta, B, tb, alpha, beta, o);
+}
+
+// trinv.go:219-243 (InverseTrm).  The triangle is expanded into a dense square T (zeros
+// outside it, ones on the diagonal with MO_UNIT), its 128 x 128 diagonal blocks are
+// inverted in shared memory, and the inverse is assembled bottom-up by recursive doubling
+// on the FP64 engine:
+//   lower:  inv([A 0; B C]) = [inv(A) 0; -inv(C) B inv(A)  inv(C)]
+//   upper:  inv([A B; 0 C]) = [inv(A) -inv(A) B inv(C); 0 inv(C)]
+// before the triangle is written back into A (the other triangle and, with MO_UNIT, the
+// diagonal are not written).
+int mo_inverse_trm(mo_ctx *ctx, mo_matrix Am, int flags, int nb) {
+  (void)nb;
+  int rc = mo::enter(ctx);
+  if (rc) return rc;
+  View A;
+  if ((rc = mo::to_view(Am, A))) return rc;
+  if (A.rows != A.cols) return MO_ENOTSQUARE;
+  const int n = A.rows;
+  if (n == 0) return MO_OK;
+  const bool lower = (flags & MO_LOWER) != 0, unit = (flags & MO_UNIT) != 0;
+  const int nblk = (n + 127) / 128;
+  int mtop = 128;  // largest merge half: the biggest power-of-two multiple of 128 below n
+  while (2 * mtop < n) mtop *= 2;
+  auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t tb = al((size_t)n * n * 8), ib = al((size_t)nblk * 128 * 128 * 8),
+               wb = al((size_t)mtop * mtop * 8);
+  char *ws = nullptr;
+  if ((rc = mo::workspace(ctx, tb + ib + wb, (void **)&ws))) return rc;
+  double *T = (double *)ws, *inv = (double *)(ws + tb), *W = (double *)(ws + tb + ib);
+  const View Tv{T, n, n, n};
+  if ((rc = mo::expand(ctx, A, n, lower ? mo::kTriLower : mo::kTriUpper, unit, T))) return rc;
+  if ((rc = mo::trtri_blocks(ctx, Tv, n, false, lower, false, inv))) return rc;
+  {
+    mo::ProfScope ps;
+    mo::prof_begin(ctx, ps, MO_PROF_OTHER);
+    mo::place_diag_kernel<<<nblk, 256, 0, ctx->stream>>>(inv, T, n, n);
+    mo::prof_end(ctx, ps, 0.0, 16.0 * nblk * 128 * 128);
+    MO_CUDA_TRY(cudaGetLastError());
+  }
+  for (int m = 128; m < n; m *= 2) {
+    for (int o = 0; o + m < n; o += 2 * m) {
+      const int mc = std::min(m, n - o - m);
+      const View Ai = Tv.sub(o, o, m, m), Ci = Tv.sub(o + m, o + m, mc, mc);
+      if (lower) {
+        const View B = Tv.sub(o + m, o, mc, m), Wv{W, mc, m, mc};
+        if ((rc = mo::gemm(ctx, Wv, B, false, Ai, false, 1.0, 0.0))) return rc;
+        if ((rc = mo::gemm(ctx, B, Ci, false, Wv, false, -1.0, 0.0))) return rc;
+      } else {
+        const View B = Tv.sub(o, o + m, m, mc), Wv{W, m, mc, m};
+        if ((rc = mo::gemm(ctx, Wv, B, false, Ci, false, 1.0, 0.0))) return rc;
+        if ((rc = mo::gemm(ctx, B, Ai, false, Wv, false, -1.0, 0.0))) return rc;
+      }
+    }
+  }
+  mo::ProfScope pb;
+  mo::prof_begin(ctx, pb, MO_PROF_OTHER);
+  mo::tri_back_kernel<<<dim3((n + 31) / 32, (n + 31) / 32), 256, 0, ctx->stream>>>(
+      T, n, A.d, A.ld, n, lower ? 1 : 0, unit ? 1 : 0);
+  mo::prof_end(ctx, pb, 0.0, 8.0 * n * (double)n);
+  MO_CUDA_TRY(cudaGetLastError());
+  return MO_OK;
 }
 
 }  // extern "C"

@@ -44,6 +44,9 @@ void dmvec_solve_blocked(mvec_t *X, const mdata_t *A, int flags, int N, int NB);
 double dvec_dot(const mvec_t *X, const mvec_t *Y, double alpha, int N);
 void dvec_invscal(mvec_t *X, double alpha, int N);
 void dvec_swap(mvec_t *X, mvec_t *Y, int N);
+void dmvec_rank(mdata_t *A, const mvec_t *X, const mvec_t *Y, double alpha, int S, int L, int R,
+                int E, int NB, int MB);
+void dvec_scal(mvec_t *X, double alpha, int N);
 /* the rest of the level-3 surface (calgo/cmops.h:149-152, 200-201, 218-226) */
 void dmult_symm_blocked2(mdata_t *C, const mdata_t *A, const mdata_t *B,
                          double alpha, double beta, int flags,

@@ -367,3 +367,18 @@ void dmmat_trmupd_blk(mdata_t *C, const mdata_t *A, const mdata_t *B, double alp
       AT(C, i, j) = c + alpha * s;
     }
 }
+
+/* calgo/dmvec_rank.c:128-148 (dmvec_rank): A[R:E, S:L] += alpha * x * y^T */
+void dmvec_rank(mdata_t *A, const mvec_t *X, const mvec_t *Y, double alpha, int S, int L, int R,
+                int E, int NB, int MB) {
+  (void)NB; (void)MB;
+  for (int j = S; j < L; j++) {
+    const double yj = Y->md[(long)j * Y->inc];
+    for (int i = R; i < E; i++) AT(A, i, j) += alpha * X->md[(long)i * X->inc] * yj;
+  }
+}
+
+/* calgo/dvec_util.c:250-264 (dvec_scal): X *= alpha */
+void dvec_scal(mvec_t *X, double alpha, int N) {
+  for (int i = 0; i < N; i++) X->md[(long)i * X->inc] *= alpha;
+}

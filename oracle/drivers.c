@@ -59,6 +59,24 @@ static void InvScale(fm X, double alpha) {
   dvec_invscal(&x, alpha, n);
 }
 
+/* mvec.go:67-95 (MVRankUpdate): A += alpha * x * y^T for row or column vectors x, y */
+static int MVRankUpdate(fm A, fm X, fm Y, double alpha) {
+  if (A.r == 0 || A.c == 0) return OR_OK;
+  if (!is_vector(Y) || !is_vector(X)) return OR_ENOTVECTOR;
+  mdata_t a = {A.d, A.ld};
+  mvec_t x = {X.d, X.r == 1 ? X.ld : 1}, y = {Y.d, Y.r == 1 ? Y.ld : 1};
+  dmvec_rank(&a, &x, &y, alpha, 0, A.c, 0, A.r, 0, 0);
+  return OR_OK;
+}
+
+/* mvec.go:439-453 (Scale) */
+static void Scale(fm X, double alpha) {
+  int n = X.r * X.c;
+  if (n == 0 || !is_vector(X)) return;
+  mvec_t x = {X.d, X.c != 1 ? X.ld : 1};
+  dvec_scal(&x, alpha, n);
+}
+
 /* mvec.go:101-121 */
 static int MVRankUpdateSym(fm A, fm X, double alpha, int flags) {
   if (A.r == 0 || A.c == 0) return OR_OK;
@@ -314,6 +332,99 @@ int or_update_trm_fm(fm C, fm A, fm B, double alpha, double beta, int flags) {
   return OR_OK;
 }
 
+/* ---------------- trinv.go ---------------- */
+
+/* trinv.go:16-49 (unblockedInverseLower) */
+static void unblockedInverseLower(fm A) {
+  for (int k = 0; k < A.r; k++) {
+    fm a10t = sub(A, k, 0, 1, k), a11 = sub(A, k, k, 1, 1);
+    fm A20 = sub(A, k + 1, 0, A.r - k - 1, k), a21 = sub(A, k + 1, k, A.r - k - 1, 1);
+    double aval = a11.d[0];
+    InvScale(a21, -aval);
+    MVRankUpdate(A20, a21, a10t, 1.0);
+    InvScale(a10t, aval);
+    a11.d[0] = 1.0 / aval;
+  }
+}
+
+/* trinv.go:51-84 (unblockedInverseUpper) */
+static void unblockedInverseUpper(fm A) {
+  for (int k = 0; k < A.r; k++) {
+    fm a01 = sub(A, 0, k, k, 1), a11 = sub(A, k, k, 1, 1);
+    fm A02 = sub(A, 0, k + 1, k, A.c - k - 1), a12t = sub(A, k, k + 1, 1, A.c - k - 1);
+    double aval = a11.d[0];
+    InvScale(a12t, -aval);
+    MVRankUpdate(A02, a01, a12t, 1.0);
+    InvScale(a01, aval);
+    a11.d[0] = 1.0 / aval;
+  }
+}
+
+/* trinv.go:86-114 (unblockedInverseUnitLower) */
+static void unblockedInverseUnitLower(fm A) {
+  for (int k = 0; k < A.r; k++) {
+    fm a10t = sub(A, k, 0, 1, k);
+    fm A20 = sub(A, k + 1, 0, A.r - k - 1, k), a21 = sub(A, k + 1, k, A.r - k - 1, 1);
+    Scale(a21, -1.0);
+    MVRankUpdate(A20, a21, a10t, 1.0);
+  }
+}
+
+/* trinv.go:116-144 (unblockedInverseUnitUpper) */
+static void unblockedInverseUnitUpper(fm A) {
+  for (int k = 0; k < A.r; k++) {
+    fm a01 = sub(A, 0, k, k, 1);
+    fm A02 = sub(A, 0, k + 1, k, A.c - k - 1), a12t = sub(A, k, k + 1, 1, A.c - k - 1);
+    Scale(a12t, -1.0);
+    MVRankUpdate(A02, a01, a12t, 1.0);
+  }
+}
+
+/* trinv.go:146-181 (blockedInverseLower, libflame variant 3) */
+static void blockedInverseLower(fm A, int flags, int nb) {
+  for (int k = 0; k < A.r; ) {
+    int b = (k + nb > A.c) ? A.c - k : nb; /* partition.go:252-254 */
+    fm A10 = sub(A, k, 0, b, k), A11 = sub(A, k, k, b, b);
+    fm A20 = sub(A, k + b, 0, A.r - k - b, k), A21 = sub(A, k + b, k, A.r - k - b, b);
+    or_solve_trm_fm(A21, A11, -1.0, flags | MTX_RIGHT);
+    or_mult_fm(A20, A21, A10, 1.0, 1.0, MTX_NOTRANS);
+    or_solve_trm_fm(A10, A11, 1.0, flags);
+    if (flags & MTX_UNIT) unblockedInverseUnitLower(A11);
+    else unblockedInverseLower(A11);
+    k += b;
+  }
+}
+
+/* trinv.go:183-217 (blockedInverseUpper, libflame variant 1) */
+static void blockedInverseUpper(fm A, int flags, int nb) {
+  for (int k = 0; k < A.r; ) {
+    int b = (k + nb > A.c) ? A.c - k : nb;
+    fm A00 = sub(A, 0, 0, k, k), A01 = sub(A, 0, k, k, b), A11 = sub(A, k, k, b, b);
+    or_mult_trm_fm(A01, A00, 1.0, flags);
+    or_solve_trm_fm(A01, A11, -1.0, flags | MTX_RIGHT);
+    if (flags & MTX_UNIT) unblockedInverseUnitUpper(A11);
+    else unblockedInverseUpper(A11);
+    k += b;
+  }
+}
+
+/* trinv.go:219-243 (InverseTrm) */
+int or_inverse_trm_fm(fm A, int flags, int nb) {
+  if (nb == 0 || A.c < nb) {
+    if (flags & MTX_UNIT) {
+      if (flags & MTX_LOWER) unblockedInverseUnitLower(A);
+      else unblockedInverseUnitUpper(A);
+    } else {
+      if (flags & MTX_LOWER) unblockedInverseLower(A);
+      else unblockedInverseUpper(A);
+    }
+  } else {
+    if (flags & MTX_LOWER) blockedInverseLower(A, flags, nb);
+    else blockedInverseUpper(A, flags, nb);
+  }
+  return OR_OK;
+}
+
 /* ---------------- chol.go ---------------- */
 
 /* chol.go:17-56 (unblockedCHOL); returns k+1 for the panic at absolute column k */
@@ -538,6 +649,9 @@ int or_update_trm(double *C, int cr, int cc, int ldc, double *A, int ar, int ac,
                   double *B, int br, int bc, int ldb, double alpha, double beta, int flags) {
   return or_update_trm_fm(FM(C, cr, cc, ldc), FM(A, ar, ac, lda), FM(B, br, bc, ldb), alpha, beta,
                           flags);
+}
+int or_inverse_trm(double *A, int ar, int ac, int lda, int flags, int nb) {
+  return or_inverse_trm_fm(FM(A, ar, ac, lda), flags, nb);
 }
 /* mmult.go:69-73 */
 int or_num_workers(int n) {

@@ -78,6 +78,7 @@ class Oracle:
         L.or_mult_trm.argtypes = M + M + [d, i]
         L.or_rank_update2_sym.argtypes = M + M + M + [d, d, i]
         L.or_update_trm.argtypes = M + M + M + [d, d, i]
+        L.or_inverse_trm.argtypes = M + [i, i]
         L.or_solve_chol.argtypes = M + M + [i]
         L.or_solve_chol.restype = None
         L.or_solve_lu.argtypes = M + M + [p, i, i]
@@ -109,6 +110,10 @@ class Oracle:
 
     def UpdateTrm(self, C, A, B, alpha, beta, flags):
         return self.lib.or_update_trm(*view(C), *view(A), *view(B), alpha, beta, flags)
+
+    def InverseTrm(self, A, flags, nb):
+        """trinv.go:219: A := inverse of its LOWER (else upper) triangle, in place"""
+        return self.lib.or_inverse_trm(*view(A), flags, nb)
 
     def DecomposeCHOLSteps(self, A, flags, nb, k0, k1):
         """blockedCHOL's block steps with first column in [k0, k1) (chol.go:58-94)"""

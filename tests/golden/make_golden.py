@@ -163,6 +163,13 @@ def main():
             R = F(C)
             assert ref.UpdateTrm(R, A, B, 1.5, beta, fl) == 0
             put(f"trmupd_{fl}_{beta}", A=A, B=B, C=C, R=R, alpha=1.5, beta=beta, flags=fl)
+    for fl in [LO, UP, LO | UNIT, UP | UNIT]:
+        for n, nb in [(40, 0), (75, 16)]:
+            T = rng.uniform(-0.5, 0.5, (n, n)) / np.sqrt(n) + np.diag(rng.uniform(1.0, 2.0, n))
+            A = F(T)
+            R = F(A)
+            assert ref.InverseTrm(R, fl, nb) == 0
+            put(f"trinv_{fl}_{n}_{nb}", A=A, R=R, flags=fl, nb=nb)
     path = os.path.join(HERE, "golden.npz")
     np.savez_compressed(path, **out)
     print(path, len(out), "arrays")

@@ -147,3 +147,22 @@ def test_blas_beta_switch(gpu, rng):
     fu = 0.5 * C0 + A @ B.T
     up = np.triu(np.ones((n, n), bool))
     assert fro((Cu.cpu().numpy() - fu)[up]) <= 1e-12 * fro(fu)
+
+
+@pytest.mark.parametrize("n", [1, 31, 128, 129, 300, 700, 1500])
+@pytest.mark.parametrize("flags", [LO, UP, LO | UNIT, UP | UNIT])
+def test_inverse_trm(gpu, ref, rng, n, flags):
+    T = rng.uniform(-0.5, 0.5, (n, n)) / np.sqrt(n) + np.diag(rng.uniform(1.0, 2.0, n))
+    A = colmajor(T, ld=even_ld(n) + 2)
+    Ag = dev(gpu, A)
+    _, err = gpu.InverseTrm(Ag, flags, 64)
+    assert err is None
+    out = Ag.cpu().numpy()
+    Ar = A.copy(order="F")
+    assert ref.InverseTrm(Ar, flags, 64) == 0
+    tri = np.tril(np.ones((n, n), bool)) if flags & LO else np.triu(np.ones((n, n), bool))
+    if flags & UNIT:
+        tri &= ~np.eye(n, dtype=bool)
+    assert fro(out[tri] - Ar[tri]) <= 1e-12 * max(fro(Ar[tri]), 1.0)
+    # the other triangle (and a unit diagonal) is not written
+    assert np.array_equal(out[~tri], A[~tri])

@@ -120,6 +120,14 @@ def test_golden_rank2_and_trm_update(oracle, golden, name):
     assert np.array_equal(R[other], c["C"][other])
 
 
+@pytest.mark.parametrize("name", names("trinv_"))
+def test_golden_inverse_trm(oracle, golden, name):
+    c = golden[name]
+    R = F(c["A"])
+    assert oracle.InverseTrm(R, int(c["flags"]), int(c["nb"])) == 0
+    assert rel(R, c["R"]) <= 1e-13
+
+
 def test_golden_lu3x3_matches_lapack(golden):
     """decomp_test.go:85-108 compares against lapack.Getrf: pivots are LAPACK's minus one."""
     import scipy.linalg as sl
