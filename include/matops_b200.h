@@ -166,9 +166,10 @@ MO_API int mo_rank_update_sym(mo_ctx *ctx, mo_matrix C, mo_matrix A, double alph
 MO_API int mo_solve_trm(mo_ctx *ctx, mo_matrix B, mo_matrix A, double alpha, int flags);
 
 /* MultSym(C, A, B, alpha, beta, flags), mmult.go:266-330 (SYMM, calgo/dmmat_symm.c:253):
- *   C = beta*C + alpha*S*op(B)   with MO_LEFT
- *   C = beta*C + alpha*op(B)*S   otherwise (the reference's kernel takes this branch
- *                                whenever MO_LEFT is not set)
+ *   C = beta*C + alpha*S*op(B)   without MO_RIGHT (MO_LEFT or no side bit: mmult.go:260's
+ *                                default, which the reference's kernel computes for orders up
+ *                                to its block size 68)
+ *   C = beta*C + alpha*op(B)*S   with MO_RIGHT
  * S is the symmetric matrix whose upper (MO_UPPER) or lower triangle A stores; op(B) = B^T
  * with MO_TRANSB.  Size check and empty rule as mmult.go:273-291 (MO_ESYMSIZE); shapes
  * that pass it but do not fit the product -> MO_EABSIZE (the reference reads out of

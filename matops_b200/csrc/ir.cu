@@ -422,7 +422,9 @@ int sym_apply(Solver &s, const double *X, int64_t ldx, const double *Bv, double 
     }
     const View Yv{Y, s.n, nr, s.n}, Sv{s.S, s.n, s.n, s.n},
         Xv{const_cast<double *>(X), s.n, nr, ldx};
-    return gemm(ctx, Yv, Sv, false, Xv, false, sa, Bv ? 1.0 : 0.0);
+    GemmOpts o;
+    o.skip = s.skip;  // inside GMRES: iterations past convergence return at once
+    return gemm_ex(ctx, Yv, Sv, false, Xv, false, sa, Bv ? 1.0 : 0.0, o);
   }
   ProfScope ps;
   prof_begin(ctx, ps, MO_PROF_IR);
@@ -465,9 +467,14 @@ int colmax(Solver &s, const double *V, int64_t ld, int n, int nr, double *out) {
 
 // D = M^-1 D in place (D: packed n x nr): L^-1 then L^-T, block-inverse solves
 int precond(Solver &s, double *D) {
-  int rc = lp_solve_apply(s.ctx, s.ls, s.n, D, s.n, s.nr, false, s.skip);
-  if (!rc) rc = lp_solve_apply(s.ctx, s.ls, s.n, D, s.n, s.nr, true, s.skip);
-  return rc;
+  for (int c0 = 0; c0 < s.nr; c0 += 64) {  // up to 64 columns per cooperative launch
+    const int nc = std::min(64, s.nr - c0);
+    double *Dc = D + (int64_t)c0 * s.n;
+    int rc = lp_solve_apply(s.ctx, s.ls, s.n, Dc, s.n, nc, false, s.skip);
+    if (!rc) rc = lp_solve_apply(s.ctx, s.ls, s.n, Dc, s.n, nc, true, s.skip);
+    if (rc) return rc;
+  }
+  return MO_OK;
 }
 
 // h(0..nv-1, :) = V_0..nv-1^T W per column; root: h = sqrt(W^T W) (nv = 1, V = W)
@@ -574,7 +581,7 @@ size_t ir_bytes(int n, int nr, int prec, bool gmres_possible) {
   const size_t vec = align256((size_t)n * nr * 8);
   const int nblk_dot = (n + DOT_ROWS - 1) / DOT_ROWS;
   const int NP = ((n + 127) / 128) * 128;
-  size_t b = align256(lp_chol_bytes(n, prec)) + align256(lp_solve_bytes(NP, nr)) + 4 * vec;
+  size_t b = align256(lp_chol_bytes(n, prec)) + align256(lp_solve_bytes(NP, std::min(nr, 64))) + 4 * vec;
   if (nr >= kGemmResidualMinRhs) b += align256((size_t)n * n * 8);
   if (gmres_possible) b += (kGmresMax + 1) * vec;
   b += 2 * align256((size_t)(kGmresMax + 1) * nr * 8) + align256((size_t)nr * 8);
@@ -679,7 +686,7 @@ int dsposv(mo_ctx *ctx, const View &X, const View &A, const View &B, bool upper,
   void *chol_mem = take(lp_chol_bytes(n, ws_prec));
   lp_chol_setup(n, prec, chol_mem, s.f);
   info.prec = prec == kLpBf16x3 ? MO_PREC_BF16X3 : MO_PREC_TF32X3;
-  lp_solve_setup(s.f.NP, nr, take(lp_solve_bytes(s.f.NP, nr)), s.ls);
+  lp_solve_setup(s.f.NP, std::min(nr, 64), take(lp_solve_bytes(s.f.NP, std::min(nr, 64))), s.ls);
   const size_t vec = (size_t)n * nr * 8;
   s.b = (double *)take(vec);
   s.x = (double *)take(vec);

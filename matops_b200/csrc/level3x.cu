@@ -3,7 +3,7 @@
 //
 // Reference semantics (mmult.go:266-523 over calgo/dmmat_symm.c:253, dmmat_trid.c:780,
 // dmmat_rank.c:132 and :292):
-//   MultSym        C = beta*C + alpha*S*B (MO_LEFT) or beta*C + alpha*op(B)*S (otherwise),
+//   MultSym        C = beta*C + alpha*S*op(B) (no MO_RIGHT) or beta*C + alpha*op(B)*S (MO_RIGHT),
 //                  S symmetric stored in the triangle MO_UPPER (else lower) selects
 //   MultTrm        B = alpha*op(T)*B (MO_LEFT or no side) / alpha*B*op(T) (MO_RIGHT), T
 //                  triangular (MO_UPPER / lower, MO_UNIT)
@@ -146,7 +146,9 @@ int mo_mult_sym(mo_ctx *ctx, mo_matrix Cm, mo_matrix Am, mo_matrix Bm, double al
   if (empty) return MO_OK;
   if (!ok) return MO_ESYMSIZE;
   const int n = ar;
-  const bool left = (flags & MO_LEFT) != 0, tb = (flags & MO_TRANSB) != 0;
+  // S*op(B) unless MO_RIGHT (mmult.go:260's default; the reference's kernel gives S*B for
+  // no side bit where its diagonal-block helper decides, calgo/dmmat_symm.c:239-244)
+  const bool left = (flags & MO_RIGHT) == 0, tb = (flags & MO_TRANSB) != 0;
   // the products the shapes allow: S*op(B) (left) or op(B)*S; shapes the size check lets
   // through but that do not fit (the reference reads out of range) are refused
   const int orow = left ? n : (tb ? bc : br), ocol = left ? (tb ? br : bc) : n;

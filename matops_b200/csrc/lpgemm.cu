@@ -19,29 +19,31 @@ namespace {
 
 // Tile 128 x 128 of C per step of a persistent CTA; K consumed in stages of 128 bytes per
 // operand row (64 bf16 or 32 tf32 elements), four 16 KB parts per stage (A.hi, A.lo,
-// B.hi, B.lo) loaded by TMA with the 128-byte swizzle into a 3-deep ring.  Warp roles:
+// B.hi, B.lo) loaded by TMA with the 128-byte swizzle into a 2-deep ring.  Warp roles:
 //   warp 0    TMA producer (one thread)
 //   warp 1    TMEM owner (allocates 256 columns = two 128 x 128 FP32 accumulators) and
 //             MMA issuer (one thread): per 32-byte K step three tcgen05.mma -- hi*hi,
 //             hi*lo, lo*hi -- into the same accumulator; tcgen05.commit frees the smem
 //             stage, and after the tile's last stage signals the epilogue
-//   warps 2-9 epilogue: warp w owns TMEM lanes 32 * (w % 4) .. + 31 (= tile rows) and the
-//             64 columns of half (w - 2) / 4 of the tile; each thread holds its row's 64
-//             C values in registers
+//   warps 2-9 epilogue: tcgen05.ld of their 32-lane quarter of the accumulator (TMEM lane
+//             = tile row, quarter = warp % 4), C = alpha * acc + beta * C, coalesced along
+//             the column; warps 2-5 take the tile's columns 0-63, warps 6-9 columns 64-127
 // The accumulator is double-buffered, so the MMAs of tile t + 1 overlap the epilogue of
-// tile t.  C (FP32, column-major) never passes through shared memory: as soon as a thread
-// has stored tile t it issues the loads of its row of tile t + 1's C (a warp reads 32
-// consecutive rows of a column: 128 contiguous bytes), so that C's DRAM latency overlaps
-// the tile's MMAs instead of sitting between one tile's store and the next tile's load;
-// the update is written back with streaming stores.  Every wait is bounded
+// tile t.  C (FP32, column-major) moves through shared memory in two 64-column halves,
+// each with its own 32 KB buffer and its own four epilogue warps: the producer loads a
+// half by TMA after the tile's operand stages, that half's warps combine it with the
+// accumulator in place and one of their threads stores it back by TMA, so the two halves
+// and their transfers proceed side by side (when C's base and leading dimension allow
+// TMA; otherwise the epilogue reads and writes C directly).  Every wait is bounded
 // (MO_SPIN_LIMIT) and reports MO_EDEVTIMEOUT.
 constexpr int TB = 128;                  // tile rows = tile columns
-constexpr int TSTAGES = 3;
+constexpr int TSTAGES = 2;
 constexpr int TPART = TB * 128;          // one operand part of a stage: 128 rows x 128 B
 constexpr int TSTAGE = 4 * TPART;        // 64 KB
+constexpr int TCTILE = TB * TB * 4;      // the C tile in shared memory (column-major FP32)
 constexpr int TTHREADS = 320;
 constexpr int TEPI_WARPS = 8;            // epilogue warps (2-9), four per 64-column half
-constexpr int TSMEM = TSTAGES * TSTAGE + 1024 + 256;  // + alignment slack + barriers
+constexpr int TSMEM = TSTAGES * TSTAGE + TCTILE + 1024 + 256;  // + alignment slack + barriers
 constexpr int TMEM_COLS = 256;
 
 struct TcParams {
@@ -53,7 +55,8 @@ struct TcParams {
   int mt, nt;
   int ntiles;   // tiles in the schedule (lower mode: only those with tm >= tn)
   int kstages;  // ceil(K * esize / 128)
-  int c_load;   // the C tile is read (beta != 0)
+  int c_tma;    // C moves through shared memory by TMA (else plain loads and stores)
+  int c_load;   // the C tile is read (beta != 0, or lower mode)
   char *shi, *slo;  // optional split copy of rows >= srow0 of the result (K-major)
   int64_t sldk;
   int srow0;
@@ -138,19 +141,34 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+__device__ __forceinline__ void tma_store_2d(const void *tmap, const void *src, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];" ::"l"(tmap),
+      "r"(smem_u32(src)), "r"(x), "r"(y)
+      : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
 template <int PREC>
 __global__ void __launch_bounds__(TTHREADS, 1)
     lp_gemm_tc_kernel(const __grid_constant__ CUtensorMap tAh, const __grid_constant__ CUtensorMap tAl,
                       const __grid_constant__ CUtensorMap tBh, const __grid_constant__ CUtensorMap tBl,
-                      const TcParams p) {
+                      const __grid_constant__ CUtensorMap tC, const TcParams p) {
   extern __shared__ __align__(16) unsigned char tsm_raw[];
   // the swizzle pattern repeats every 1024 bytes: align the ring to it
   unsigned char *tsm = tsm_raw + ((1024 - (smem_u32(tsm_raw) & 1023)) & 1023);
-  uint64_t *full = reinterpret_cast<uint64_t *>(tsm + TSTAGES * TSTAGE);
+  float *ctile = reinterpret_cast<float *>(tsm + TSTAGES * TSTAGE);
+  uint64_t *full = reinterpret_cast<uint64_t *>(tsm + TSTAGES * TSTAGE + TCTILE);
   uint64_t *empty = full + TSTAGES;
   uint64_t *tfull = empty + TSTAGES;   // [2]
   uint64_t *tempty = tfull + 2;        // [2]
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tempty + 2);
+  // the C tile moves in two 64-column halves with their own buffers and barriers, so one
+  // half's load or store overlaps the other half's epilogue
+  uint64_t *cfull = tempty + 2;    // [2]
+  uint64_t *cempty = cfull + 2;    // [2]
+  uint64_t *cready = cempty + 2;   // [2] the four epilogue warps have written that half
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(cready + 2);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < TSTAGES; ++s) {
@@ -160,6 +178,11 @@ __global__ void __launch_bounds__(TTHREADS, 1)
     for (int b = 0; b < 2; ++b) {
       mbar_init(&tfull[b], 1);
       mbar_init(&tempty[b], TEPI_WARPS);
+    }
+    for (int h = 0; h < 2; ++h) {
+      mbar_init(&cfull[h], 1);
+      mbar_init(&cempty[h], 1);
+      mbar_init(&cready[h], 4);
     }
     fence_barrier_init();
   }
@@ -178,10 +201,11 @@ __global__ void __launch_bounds__(TTHREADS, 1)
   constexpr int KEL = 128 / ES;  // K elements per stage
 
   if (warp == 0 && lane == 0) {
-    // producer: the operand stages of every tile of this CTA, through the ring
-    int g = 0;
+    // producer: the operand stages of tile t, then (once the previous tile's C has been
+    // stored) its C tile
+    int g = 0, tc = 0, cu[2] = {0, 0};  // cu: uses of each C half buffer
     bool ok = true;
-    for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
+    for (int t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x, ++tc) {
       int tm, tn;
       tile_coords(p, t, tm, tn);
       for (int ks = 0; ks < p.kstages; ++ks, ++g) {
@@ -197,6 +221,21 @@ __global__ void __launch_bounds__(TTHREADS, 1)
         tma_load_2d(st + TPART, &tAl, &full[slot], ks * KEL, tm * TB);
         tma_load_2d(st + 2 * TPART, &tBh, &full[slot], ks * KEL, tn * TB);
         tma_load_2d(st + 3 * TPART, &tBl, &full[slot], ks * KEL, tn * TB);
+      }
+      if (!ok || !p.c_tma) continue;
+      const int nh = tn * TB + TB / 2 < p.N ? 2 : 1;  // the second half only if it has columns
+      for (int h = 0; h < nh; ++h) {
+        if (!mbar_wait(&cempty[h], (cu[h] & 1) ^ 1, p.status)) {
+          ok = false;
+          break;
+        }
+        if (p.c_load) {
+          mbar_arrive_expect_tx(&cfull[h], TCTILE / 2);
+          tma_load_2d(ctile + h * TB * (TB / 2), &tC, &cfull[h], tm * TB, tn * TB + h * (TB / 2));
+        } else {
+          mbar_arrive(&cfull[h]);
+        }
+        ++cu[h];
       }
     }
   } else if (warp == 1 && lane == 0) {
@@ -230,27 +269,14 @@ __global__ void __launch_bounds__(TTHREADS, 1)
       if (ok) umma_commit(&tfull[buf]);
     }
   } else if (warp >= 2) {
-    // epilogue: this thread's row of the tile and the 64 columns of half h
+    // epilogue: warp w reads TMEM lanes 32 * (w % 4) .. + 31 (= tile rows) of the 64
+    // columns of half h = (w - 2) / 4
     const int q = warp & 3;
     const int rl = q * 32 + lane;
     const int h = (warp - 2) >> 2;
-    const int cbase = h * (TB / 2);
-    float creg[TB / 2];  // C(row, tile columns cbase ..) of the current tile
-    // loads of this row's C values of tile t (nothing when beta == 0)
-    auto prefetch = [&](int t) {
-      int tm, tn;
-      tile_coords(p, t, tm, tn);
-      const int row = tm * TB + rl;
-      const float *src = p.C + row + (int64_t)(tn * TB + cbase) * p.ldc;
-#pragma unroll
-      for (int r = 0; r < TB / 2; ++r) {
-        const int col = tn * TB + cbase + r;
-        const bool use = p.c_load && row < p.M && col < p.N && (p.mode != kGemmLower || row >= col);
-        creg[r] = use ? __ldcs(src + (int64_t)r * p.ldc) : 0.f;
-      }
-    };
-    if (blockIdx.x < p.ntiles) prefetch(blockIdx.x);
-    int tc = 0;
+    const bool storer = (warp - 2) % 4 == 0;  // warps 2 and 6: one thread stores the half
+    float *const cb = ctile + h * TB * (TB / 2);  // this half: column-major 128 x 64
+    int tc = 0, cu = 0;  // cu: uses of this half's buffer
     for (int t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++tc) {
       int tm, tn;
       tile_coords(p, t, tm, tn);
@@ -258,41 +284,48 @@ __global__ void __launch_bounds__(TTHREADS, 1)
       if (!mbar_wait(&tfull[buf], (tc >> 1) & 1, p.status)) break;
       tc_fence_after();
       const int row = tm * TB + rl;
-      const bool rok = row < p.M;
-      float *dst = p.C + row + (int64_t)(tn * TB + cbase) * p.ldc;
+      // the second half exists only if the tile has columns there (the producer decides
+      // the same way)
+      const bool live = h == 0 || tn * TB + TB / 2 < p.N;
+      if (p.c_tma) {
+        bool fail = false;
+        if (live) {
+          if (!mbar_wait(&cfull[h], cu & 1, p.status)) break;
+#pragma unroll 1
+          for (int c0 = h * (TB / 2); c0 < (h + 1) * (TB / 2); c0 += 16) {
+            uint32_t v[16];
+            tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + buf * TB + c0, v);
 #pragma unroll
-      for (int c0 = 0; c0 < TB / 2; c0 += 16) {
-        uint32_t v[16];
-        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + buf * TB + cbase + c0, v);
-#pragma unroll
-        for (int r = 0; r < 16; ++r) {
-          const int col = tn * TB + cbase + c0 + r;
-          const float a = p.alpha * __uint_as_float(v[r]);
-          const float nv = p.c_load ? fmaf(p.beta, creg[c0 + r], a) : a;
-          const bool w = rok && col < p.N && (p.mode != kGemmLower || row >= col);
-          creg[c0 + r] = w ? nv : 0.f;  // what the split copy sees: only written values
-          if (w) __stcs(dst + (int64_t)(c0 + r) * p.ldc, nv);
+            for (int r = 0; r < 16; ++r) {
+              const int col = tn * TB + c0 + r;
+              float *cs = cb + (c0 - h * (TB / 2) + r) * TB + rl;
+              const float a = p.alpha * __uint_as_float(v[r]);
+              const float nv = p.beta == 0.f ? a : fmaf(p.beta, *cs, a);
+              if (p.mode != kGemmLower || row >= col) *cs = nv;
+            }
+          }
         }
-      }
-      // the accumulator has been read out
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&tempty[buf]);
-      // split copy of this thread's row of the half (K-major: 16-byte stores)
-      if (p.shi != nullptr && rok && row >= p.srow0) {
-        const int64_t obase = ((int64_t)(row - p.srow0) * p.sldk + tn * TB) * ES;
-#pragma unroll
-        for (int c0 = 0; c0 < TB / 2; c0 += 8) {
-          if (tn * TB + cbase + c0 < p.N) {
+        // the accumulator has been read out (every epilogue warp arrives, live or not)
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&tempty[buf]);
+        if (!live) continue;
+        // split copy of this thread's row (it wrote that row of the half itself)
+        if (p.shi != nullptr && row < p.M && row >= p.srow0) {
+          constexpr int ES = PREC == kLpBf16x3 ? 2 : 4;
+          const int64_t obase = ((int64_t)(row - p.srow0) * p.sldk + tn * TB) * ES;
+#pragma unroll 1
+          for (int c0 = h * (TB / 2); c0 < (h + 1) * (TB / 2) && tn * TB + c0 < p.N; c0 += 8) {
             float x[8];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) x[u] = tn * TB + cbase + c0 + u < p.N ? creg[c0 + u] : 0.f;
+            for (int u = 0; u < 8; ++u)
+              x[u] = tn * TB + c0 + u < p.N ? cb[(c0 - h * (TB / 2) + u) * TB + rl] : 0.f;
             if (PREC == kLpBf16x3) {
               __align__(16) __nv_bfloat16 hh[8], ll[8];
 #pragma unroll
               for (int u = 0; u < 8; ++u) split_bf16(x[u], hh[u], ll[u]);
-              *reinterpret_cast<uint4 *>(p.shi + obase + (cbase + c0) * ES) = *reinterpret_cast<const uint4 *>(hh);
-              *reinterpret_cast<uint4 *>(p.slo + obase + (cbase + c0) * ES) = *reinterpret_cast<const uint4 *>(ll);
+              *reinterpret_cast<uint4 *>(p.shi + obase + c0 * ES) = *reinterpret_cast<const uint4 *>(hh);
+              *reinterpret_cast<uint4 *>(p.slo + obase + c0 * ES) = *reinterpret_cast<const uint4 *>(ll);
             } else {
               __align__(16) uint32_t hh[8], ll[8];
 #pragma unroll
@@ -302,18 +335,59 @@ __global__ void __launch_bounds__(TTHREADS, 1)
               }
 #pragma unroll
               for (int v = 0; v < 2; ++v) {
-                *reinterpret_cast<uint4 *>(p.shi + obase + (cbase + c0 + 4 * v) * ES) =
+                *reinterpret_cast<uint4 *>(p.shi + obase + (c0 + 4 * v) * ES) =
                     *reinterpret_cast<const uint4 *>(hh + 4 * v);
-                *reinterpret_cast<uint4 *>(p.slo + obase + (cbase + c0 + 4 * v) * ES) =
+                *reinterpret_cast<uint4 *>(p.slo + obase + (c0 + 4 * v) * ES) =
                     *reinterpret_cast<const uint4 *>(ll + 4 * v);
               }
             }
           }
         }
+        // this half's four warps' shared-memory writes, then one TMA store of the half
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&cready[h]);
+        if (storer) {
+          int ok = 1;
+          if (lane == 0) {
+            ok = mbar_wait(&cready[h], cu & 1, p.status) ? 1 : 0;
+            if (ok) {
+              tma_store_2d(&tC, cb, tm * TB, tn * TB + h * (TB / 2));
+              mbar_arrive(&cempty[h]);
+            }
+          }
+          if (!__shfl_sync(0xffffffffu, ok, 0)) fail = true;  // warp-uniform exit
+        }
+        ++cu;
+        if (fail) break;
+      } else {
+        // C read and written in place: this warp's 64 columns
+        const bool rok = row < p.M;
+#pragma unroll 1
+        for (int c0 = h * (TB / 2); c0 < (h + 1) * (TB / 2); c0 += 16) {
+          float cv[16];
+#pragma unroll
+          for (int r = 0; r < 16; ++r) {
+            const int col = tn * TB + c0 + r;
+            cv[r] = (p.beta != 0.f && rok && col < p.N) ? p.C[row + (int64_t)col * p.ldc] : 0.f;
+          }
+          uint32_t v[16];
+          tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + buf * TB + c0, v);
+#pragma unroll
+          for (int r = 0; r < 16; ++r) {
+            const int col = tn * TB + c0 + r;
+            if (rok && col < p.N && (p.mode != kGemmLower || row >= col))
+              p.C[row + (int64_t)col * p.ldc] = fmaf(p.beta, cv[r], p.alpha * __uint_as_float(v[r]));
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&tempty[buf]);
       }
-      // the next tile's C: in flight while its MMAs run
-      if (t + (int)gridDim.x < p.ntiles) prefetch(t + gridDim.x);
     }
+    // the last store of this half has been read out of shared memory; let it reach
+    // global memory
+    if (storer && lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
   }
   tc_fence_before();
   __syncthreads();
@@ -418,8 +492,22 @@ bool split_tmap(CUtensorMap *tm, const void *ptr, int prec, int64_t K, int64_t r
             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// map over the FP32 column-major C: box 128 rows x 64 columns (half a tile), no swizzle
+bool c_tmap(CUtensorMap *tm, float *C, int64_t M, int64_t N, int64_t ldc) {
+  auto fn = tc_encode_fn();
+  if (!fn) return false;
+  if (((uintptr_t)C & 15) || (ldc * 4) % 16) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)std::max<int64_t>(M, 1), (cuuint64_t)std::max<int64_t>(N, 1)};
+  cuuint64_t strides[1] = {(cuuint64_t)(ldc * 4)};
+  cuuint32_t box[2] = {(cuuint32_t)TB, (cuuint32_t)(TB / 2)};  // one 64-column half
+  cuuint32_t estr[2] = {1, 1};
+  return fn(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, C, dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <int PREC>
-int launch_tc(mo_ctx *ctx, const CUtensorMap (&m)[4], const TcParams &p, int grid) {
+int launch_tc(mo_ctx *ctx, const CUtensorMap (&m)[5], const TcParams &p, int grid) {
   static std::atomic<uint64_t> attr_done{0};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -429,7 +517,7 @@ int launch_tc(mo_ctx *ctx, const CUtensorMap (&m)[4], const TcParams &p, int gri
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, TSMEM));
     attr_done.fetch_or(bit);
   }
-  lp_gemm_tc_kernel<PREC><<<grid, TTHREADS, TSMEM, ctx->stream>>>(m[0], m[1], m[2], m[3], p);
+  lp_gemm_tc_kernel<PREC><<<grid, TTHREADS, TSMEM, ctx->stream>>>(m[0], m[1], m[2], m[3], m[4], p);
   MO_CUDA_TRY(cudaGetLastError());
   return MO_OK;
 }
@@ -458,15 +546,15 @@ int lp_gemm(mo_ctx *ctx, int prec, const LpGemmArgs &a) {
   p.ntiles = p.mode == kGemmLower ? p.nt * p.mt - p.nt * (p.nt - 1) / 2 : p.mt * p.nt;
   p.kstages = (a.K * es + 127) / 128;
   p.status = &control(ctx)->status;
-  CUtensorMap m[4];
-  p.c_load = a.beta != 0.f ? 1 : 0;
+  CUtensorMap m[5];
+  p.c_tma = c_tmap(&m[4], a.C, a.M, a.N, a.ldc) ? 1 : 0;
+  if (!p.c_tma) m[4] = CUtensorMap{};
+  p.c_load = (a.beta != 0.f || p.mode == kGemmLower) ? 1 : 0;
   p.shi = (char *)a.out.hi;
   p.slo = (char *)a.out.lo;
   p.sldk = a.out.ldk;
   p.srow0 = a.out_row0;
-  if (p.shi && (a.out.ldk % 8 || a.N > a.out.ldk || ((uintptr_t)a.out.hi & 15) ||
-                 ((uintptr_t)a.out.lo & 15)))
-    return MO_EINVAL;
+  if (p.shi && (!p.c_tma || a.out.ldk % 8 || a.N > a.out.ldk)) return MO_EINVAL;
   if (!split_tmap(&m[0], a.A.hi, prec, a.K, a.M, a.A.ldk) ||
       !split_tmap(&m[1], a.A.lo, prec, a.K, a.M, a.A.ldk) ||
       !split_tmap(&m[2], a.B.hi, prec, a.K, a.N, a.B.ldk) ||

@@ -256,8 +256,11 @@ static inline double sym_at(const mdata_t *A, int flags, int i, int j) {
   return AT(A, j, i);
 }
 
-/* calgo/dmmat_symm.c:253-390 (dmult_symm_blocked2): C[R:E, S:L] = beta*C + alpha*A*B with
- * MTX_LEFT, else beta*C + alpha*op(B)*A (op(B) = B^T with MTX_TRANSB); A (P x P) symmetric.
+/* calgo/dmmat_symm.c:253-390 (dmult_symm_blocked2): C[R:E, S:L] = beta*C + alpha*A*B
+ * without MTX_RIGHT, else beta*C + alpha*op(B)*A (op(B) = B^T with MTX_TRANSB); A (P x P)
+ * symmetric.  With no side bit the reference's kernel mixes its two branches (the loop of
+ * the right side, calgo/dmmat_symm.c:287, and the left-side diagonal-block product,
+ * :239-244), which is A*B for orders up to its block size 68; this restatement gives A*B.
  * The left branch reads B untransposed whatever MTX_TRANSB says (the reference's kernel
  * never consults it there). */
 void dmult_symm_blocked2(mdata_t *C, const mdata_t *A, const mdata_t *B, double alpha,
@@ -270,7 +273,7 @@ void dmult_symm_blocked2(mdata_t *C, const mdata_t *A, const mdata_t *B, double 
     for (int i = R; i < E; i++) {
       double s = 0.0;
       for (int p = 0; p < P; p++) {
-        if (flags & MTX_LEFT) s += sym_at(A, flags, i, p) * AT(B, p, j);
+        if (!(flags & MTX_RIGHT)) s += sym_at(A, flags, i, p) * AT(B, p, j);
         else s += ((flags & MTX_TRANSB) ? AT(B, p, i) : AT(B, i, p)) * sym_at(A, flags, p, j);
       }
       AT(C, i, j) += alpha * s;

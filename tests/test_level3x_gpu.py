@@ -1,10 +1,10 @@
 """GPU parity: MultSym / MultTrm / RankUpdate2Sym / UpdateTrm against the oracle.
 
 The oracle is the reference's own calgo kernels (oracle/_ref) under the restated Go
-wrappers when they were built, else the oracle port.  Two inputs are avoided because the
-reference itself is wrong there (recorded, not reproduced): the right-side SYMM blocked
-path for orders above its block size 68 and MultSym's MO_TRANSB with the right side (the
-kernel reads B out of shape); those cases are checked against numpy instead.
+wrappers when they were built, else the oracle port.  Inputs where the reference itself is
+wrong (recorded, not reproduced) are checked against numpy instead: SYMM's blocked paths
+for orders above its block size 68 with the right side or no side bit, and MultSym's
+MO_TRANSB with the right side (the kernel reads B out of shape).
 """
 import numpy as np
 import pytest
@@ -38,7 +38,7 @@ def sym(S, flags):
 @pytest.mark.parametrize("n,p", [(1, 1), (37, 5), (68, 70), (200, 33), (700, 129)])
 @pytest.mark.parametrize("flags", [LEFT | LO, LEFT | UP, LEFT | LO | TA, RIGHT | LO, RIGHT | UP, LO])
 def test_mult_sym(gpu, ref, rng, n, p, flags):
-    left = bool(flags & LEFT)
+    left = not flags & RIGHT
     if not left:
         p = n  # the reference's size check admits the right side only for square C
     A = colmajor(rng.uniform(-1, 1, (n, n)), ld=even_ld(n) + 2)
@@ -47,11 +47,13 @@ def test_mult_sym(gpu, ref, rng, n, p, flags):
     Cg = dev(gpu, C0)
     assert gpu.MultSym(Cg, dev(gpu, A), dev(gpu, B), 1.5, -0.5, flags) is None
     S = sym(A, flags)
-    if left or n <= 68:
+    if flags & LEFT or n <= 68:
         Cr = C0.copy(order="F")
         assert ref.MultSym(Cr, A, B, 1.5, -0.5, flags) == 0
     else:
-        Cr = -0.5 * C0 + 1.5 * (B @ S)
+        # the reference's blocked paths above its block size: right side wrong, no side bit
+        # mixed (recorded in DESIGN); the documented product instead
+        Cr = -0.5 * C0 + 1.5 * ((S @ B) if left else (B @ S))
     err = fro(Cg.cpu().numpy() - Cr)
     assert err <= 4 * n * EPS * (1.5 * fro(S) * fro(B) + 0.5 * fro(C0)) + 1e-300, err
 
