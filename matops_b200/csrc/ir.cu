@@ -25,7 +25,7 @@
 namespace mo {
 int potrf(mo_ctx *ctx, View A, bool upper, int *d_info, double *d_bad, double *inv);
 int trsm_few_f32(mo_ctx *ctx, View B, const float *L, int64_t ldl, int N, bool trans,
-                 const double *inv_L, int *flag_buf);
+                 const double *inv_L, int *flag_buf, const int *skip);
 
 namespace {
 
@@ -384,7 +384,6 @@ struct Solver {
   bool upper;
   int n, nr;  // nr: right-hand sides (all columns)
   LpChol f;
-  LpSolve ls;             // block-inverse triangular solves with the factor
   double *b, *x, *r, *d;  // n x nr packed
   double *V;              // (kGmresMax + 1) blocks of n x nr
   double *h, *h2;         // Gram-Schmidt coefficients, (kGmresMax + 1) x nr each
@@ -465,13 +464,13 @@ int colmax(Solver &s, const double *V, int64_t ld, int n, int nr, double *out) {
   return MO_OK;
 }
 
-// D = M^-1 D in place (D: packed n x nr): L^-1 then L^-T, block-inverse solves
+// D = M^-1 D in place (D: packed n x nr): L^-1 then L^-T with the FP32 factor (FP64
+// arithmetic), right-hand sides in groups of 64
 int precond(Solver &s, double *D) {
-  for (int c0 = 0; c0 < s.nr; c0 += 64) {  // up to 64 columns per cooperative launch
-    const int nc = std::min(64, s.nr - c0);
-    double *Dc = D + (int64_t)c0 * s.n;
-    int rc = lp_solve_apply(s.ctx, s.ls, s.n, Dc, s.n, nc, false, s.skip);
-    if (!rc) rc = lp_solve_apply(s.ctx, s.ls, s.n, Dc, s.n, nc, true, s.skip);
+  for (int c0 = 0; c0 < s.nr; c0 += 64) {
+    const View B{D + (int64_t)c0 * s.n, s.n, std::min(64, s.nr - c0), s.n};
+    int rc = trsm_few_f32(s.ctx, B, s.f.W, s.f.ldw, s.n, false, s.f.inv, s.flags, s.skip);
+    if (!rc) rc = trsm_few_f32(s.ctx, B, s.f.W, s.f.ldw, s.n, true, s.f.inv, s.flags, s.skip);
     if (rc) return rc;
   }
   return MO_OK;
@@ -580,8 +579,7 @@ size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 size_t ir_bytes(int n, int nr, int prec, bool gmres_possible) {
   const size_t vec = align256((size_t)n * nr * 8);
   const int nblk_dot = (n + DOT_ROWS - 1) / DOT_ROWS;
-  const int NP = ((n + 127) / 128) * 128;
-  size_t b = align256(lp_chol_bytes(n, prec)) + align256(lp_solve_bytes(NP, std::min(nr, 64))) + 4 * vec;
+  size_t b = align256(lp_chol_bytes(n, prec)) + 4 * vec;
   if (nr >= kGemmResidualMinRhs) b += align256((size_t)n * n * 8);
   if (gmres_possible) b += (kGmresMax + 1) * vec;
   b += 2 * align256((size_t)(kGmresMax + 1) * nr * 8) + align256((size_t)nr * 8);
@@ -686,7 +684,6 @@ int dsposv(mo_ctx *ctx, const View &X, const View &A, const View &B, bool upper,
   void *chol_mem = take(lp_chol_bytes(n, ws_prec));
   lp_chol_setup(n, prec, chol_mem, s.f);
   info.prec = prec == kLpBf16x3 ? MO_PREC_BF16X3 : MO_PREC_TF32X3;
-  lp_solve_setup(s.f.NP, std::min(nr, 64), take(lp_solve_bytes(s.f.NP, std::min(nr, 64))), s.ls);
   const size_t vec = (size_t)n * nr * 8;
   s.b = (double *)take(vec);
   s.x = (double *)take(vec);
@@ -762,7 +759,6 @@ int dsposv(mo_ctx *ctx, const View &X, const View &A, const View &B, bool upper,
     info.shifts += 1;
   }
   info.shift = factored ? shift : 0.0;
-  if (factored && (rc = lp_solve_prepare(ctx, s.f, s.ls))) return rc;
   std::vector<double> nh(3 * nr + 1);
   double prev = INFINITY;
   bool use_gmres = method == MO_IR_GMRES;

@@ -56,16 +56,7 @@ __global__ void __launch_bounds__(TRI_THREADS)
   __shared__ double s_badv;
   lp_load_block(S, W, ldw);
   __syncthreads();
-  // factor and invert; each row block of L goes back to W (FP32) before the inverse
-  // overwrites it in shared memory
-  auto emit = [&](int s, int tid, int nthr) {
-    const int r0 = s * SUB, ncols = r0 + SUB;
-    for (int e = tid; e < SUB * ncols; e += nthr) {
-      const int i = r0 + e % SUB, j = e / SUB;
-      if (i >= j) W[i + (int64_t)j * ldw] = (float)S[i * LDS + j];
-    }
-  };
-  tri_potrf_inverse_lower(S, NB, Wk, &s_bad, &s_badv, emit);
+  tri_potrf_lower(S, NB, &s_bad, &s_badv);
   if (s_bad >= 0) {
     // a failure inside the identity padding cannot happen; report the true column
     if (threadIdx.x == 0 && col0 + s_bad < n_true) {
@@ -74,6 +65,13 @@ __global__ void __launch_bounds__(TRI_THREADS)
     }
     return;
   }
+  for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
+    const int i = e % NB, j = e / NB;
+    if (i >= j) W[i + (int64_t)j * ldw] = (float)S[i * LDS + j];
+  }
+  __syncthreads();
+  tri_inverse_lower(S, NB, Wk);
+  __syncthreads();
   for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
     const int i = e % NB, j = e / NB;
     inv[i + j * NB] = (i >= j) ? S[i * LDS + j] : 0.0;

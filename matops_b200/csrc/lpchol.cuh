@@ -24,26 +24,4 @@ int lp_chol_convert(mo_ctx *ctx, const LpChol &f, View A, bool upper, double shi
 // factor W in place; a failing pivot sets *d_info = column + 1 (device word)
 int lp_chol_factor(mo_ctx *ctx, LpChol &f, int *d_info, double *d_bad);
 
-// Triangular solves with the factor (lpsolve.cu): the FP64 inverses of its kLpSolveBlock x
-// kLpSolveBlock diagonal blocks, a block of X and the grid-barrier words of the solve kernel
-constexpr int kLpSolveBlock = 1024;
-struct LpSolve {
-  int NP = 0, nblk = 0, nrhs = 0;
-  const float *W = nullptr;  // the factor (the working matrix of LpChol)
-  int64_t ldw = 0;
-  double *Dinv = nullptr;  // nblk blocks, each kLpSolveBlock^2 column-major (ld kLpSolveBlock)
-  double *T = nullptr;     // scratch of the inverse merges
-  double *Xb = nullptr;    // kLpSolveBlock x nrhs
-  unsigned *bar = nullptr;
-};
-// device bytes for an order-NP factor and up to nrhs right-hand sides per apply
-size_t lp_solve_bytes(int NP, int nrhs);
-int lp_solve_setup(int NP, int nrhs, void *mem, LpSolve &s);
-// after lp_chol_factor: the block inverses
-int lp_solve_prepare(mo_ctx *ctx, const LpChol &f, LpSolve &s);
-// D (n x nr, ld ldd, nr <= 64) <- L^-1 D, or L^-T D with trans; skip: optional device word
-// that turns the launch into a no-op when set
-int lp_solve_apply(mo_ctx *ctx, const LpSolve &s, int n, double *D, int64_t ldd, int nr,
-                   bool trans, const int *skip = nullptr);
-
 }  // namespace mo

@@ -28,21 +28,7 @@ __global__ void __launch_bounds__(TRI_THREADS)
   // upper storage: A = U^T U with U^T lower, so load/store the transpose
   tri_load_lower(S, A, lda, n, upper, false);
   __syncthreads();
-  // factor and invert; each row block of L goes back to A (transposed for upper storage)
-  // before the inverse overwrites it in shared memory
-  auto emit = [&](int s, int tid, int nthr) {
-    const int r0 = s * SUB, ncols = r0 + SUB;
-    for (int e = tid; e < SUB * ncols; e += nthr) {
-      // lower: rows fastest (contiguous in A); upper: A(j, i) = L(i, j), columns fastest
-      const int i = upper ? r0 + e / ncols : r0 + e % SUB;
-      const int j = upper ? e % ncols : e / SUB;
-      if (i < n && j <= i) {
-        if (upper) A[j + (int64_t)i * lda] = S[i * LDS + j];
-        else A[i + (int64_t)j * lda] = S[i * LDS + j];
-      }
-    }
-  };
-  tri_potrf_inverse_lower(S, NP, W, &s_bad, &s_badv, emit);
+  tri_potrf_lower(S, NP, &s_bad, &s_badv);
   if (s_bad >= 0) {
     if (threadIdx.x == 0) {
       *info = col0 + s_bad + 1;
@@ -50,6 +36,10 @@ __global__ void __launch_bounds__(TRI_THREADS)
     }
     return;
   }
+  tri_store_lower(S, A, lda, n, upper, false);
+  __syncthreads();
+  tri_inverse_lower(S, NP, W);
+  __syncthreads();
   tri_store_lower(S, inv, NB, n, false, true);
 }
 

@@ -304,209 +304,4 @@ __device__ inline void tri_inverse_lower(double *S, int NP, double *W) {
   }
 }
 
-
-// ---------------------------------------------------------------------------------------
-// Pipelined Cholesky + inverse of a diagonal block (order NP <= 128, a multiple of 32).
-// The 32-column leaves are factored one after another by warp 0; the other warps work
-// beside it on what the next leaf does not need:
-//   iteration s (leaf s = rows/columns 32 s .. 32 s + 31):
-//     F  warp 0      : factor leaf s
-//        warps 2..7  : rank-32 update with sub-panel s - 1 of the bands right of band s
-//        warp 1      : hand row block s - 1 of L to emit(), then invert leaf s - 1 in place
-//        warps 1..7  : row block s - 1 of the inverse, X(s-1, j) = -X(s-1,s-1) sum_k
-//                      L(s-1, k) X(k, j), over L's row block in place
-//     R  all warps   : rows below leaf s (times the leaf's inverse transposed, by
-//                      substitution)
-//     U  all warps   : rank-32 update of band s + 1 with sub-panel s (what leaf s + 1 needs)
-// and after the last leaf its row block is emitted and inverted the same way.  Row block s
-// of L is final once leaf s and the rows below the earlier leaves are done; nothing later
-// reads it, so the inverse may overwrite it after emit(s) has stored it.  On a NaN pivot
-// (sqrt of a non-positive value) *bad_col / *bad_val receive the first failing column and
-// the routine stops with S partly processed.  emit(s, tid, nthreads) is called by the
-// threads [32, 64) (warp 1) for s < nsub - 1 and by all threads for the last row block; it
-// must only read row block s of S (rows 32 s .. 32 s + 31, columns 0 .. 32 s + 31).
-// ---------------------------------------------------------------------------------------
-
-// Named barrier among the warps 1..7 (224 threads); id 1 (0 is __syncthreads).
-__device__ __forceinline__ void tri_bar_helpers() {
-  asm volatile("bar.sync 1, 224;" ::: "memory");
-}
-
-// S(i, j) -= sum_{k<32} S(i, kb + k) * S(j, kb + k), i >= j, for rows and columns in
-// [r0, NP) restricted to columns [c0, c1): 32 x 32 blocks, 64 threads per block, run by the
-// threads tid in [0, nthr) of a group (nthr a multiple of 64).
-__device__ __forceinline__ void tri_syrk_part(double *S, int NP, int r0, int c0, int c1, int kb,
-                                              int tid, int nthr) {
-  const int cb0 = c0 / SUB, cb1 = c1 / SUB, nb = NP / SUB, rb0 = r0 / SUB;
-  // tasks: (bj in [cb0, cb1), bi in [max(bj, rb0), nb)) enumerated column by column
-  int ntask = 0;
-  for (int bj = cb0; bj < cb1; ++bj) ntask += nb - max(bj, rb0);
-  const int t = tid & 63, tx = t & 7, ty = t >> 3;
-  for (int task = tid >> 6; task < ntask; task += nthr >> 6) {
-    int rem = task, bj = cb0;
-    while (rem >= nb - max(bj, rb0)) {
-      rem -= nb - max(bj, rb0);
-      ++bj;
-    }
-    const int bi = max(bj, rb0) + rem;
-    const int i0 = bi * SUB + tx, j0 = bj * SUB + ty;
-    double acc[4][4];
-#pragma unroll
-    for (int x = 0; x < 4; ++x)
-#pragma unroll
-      for (int y = 0; y < 4; ++y) acc[x][y] = 0.0;
-#pragma unroll 8
-    for (int k = 0; k < SUB; ++k) {
-      double a[4], b[4];
-#pragma unroll
-      for (int x = 0; x < 4; ++x) {
-        a[x] = S[(i0 + 8 * x) * LDS + kb + k];
-        b[x] = S[(j0 + 8 * x) * LDS + kb + k];
-      }
-#pragma unroll
-      for (int x = 0; x < 4; ++x)
-#pragma unroll
-        for (int y = 0; y < 4; ++y) acc[x][y] = fma(a[x], b[y], acc[x][y]);
-    }
-#pragma unroll
-    for (int x = 0; x < 4; ++x)
-#pragma unroll
-      for (int y = 0; y < 4; ++y)
-        if (i0 + 8 * x >= j0 + 8 * y) S[(i0 + 8 * x) * LDS + j0 + 8 * y] -= acc[x][y];
-  }
-}
-
-// In-place inverse of the 32 x 32 lower leaf at (b, b) by one warp: lane c solves
-// L x = e_c (the step (1) of tri_inverse_lower)
-__device__ __forceinline__ void tri_leaf_inverse(double *S, int b, int lane) {
-  const double rdi = 1.0 / S[(b + lane) * LDS + b + lane];
-  double x[SUB];
-#pragma unroll
-  for (int i = 0; i < SUB; ++i) {
-    const double *lrow = S + (b + i) * LDS + b;
-    double s0 = (i == lane) ? 1.0 : 0.0, s1 = 0.0;
-#pragma unroll
-    for (int m = 0; m + 1 < i; m += 2) {
-      s0 = fma(-lrow[m], x[m], s0);
-      s1 = fma(-lrow[m + 1], x[m + 1], s1);
-    }
-    if (i & 1) s0 = fma(-lrow[i - 1], x[i - 1], s0);
-    const double rd = __shfl_sync(0xffffffffu, rdi, i);
-    x[i] = (i < lane) ? 0.0 : (s0 + s1) * rd;
-  }
-  __syncwarp();
-#pragma unroll
-  for (int i = 0; i < SUB; ++i) S[(b + i) * LDS + b + lane] = x[i];
-}
-
-// Off-diagonal blocks of row block bi of the inverse (X(bi, bi) already in place): by the
-// threads tid in [0, nthr) of a group whose members meet at `bar` between the two halves.
-template <class Bar>
-__device__ __forceinline__ void tri_inverse_row(double *S, double *W, int bi, int tid, int nthr,
-                                                Bar bar) {
-  constexpr int LW = SUB + 1;
-  if (bi == 0) return;
-  for (int e = tid; e < bi * 64; e += nthr) {
-    const int bj = e / 64, tile = e % 64;
-    tri_small_gemm(W + bj * SUB * LW, LW, S + (bi * SUB) * LDS + bj * SUB, LDS,
-                   S + (bj * SUB) * LDS + bj * SUB, LDS, (bi - bj) * SUB, 1.0, tile, 64);
-  }
-  bar();
-  for (int e = tid; e < bi * 64; e += nthr) {
-    const int bj = e / 64, tile = e % 64;
-    tri_small_gemm(S + (bi * SUB) * LDS + bj * SUB, LDS, S + (bi * SUB) * LDS + bi * SUB, LDS,
-                   W + bj * SUB * LW, LW, SUB, -1.0, tile, 64);
-  }
-}
-
-template <class Emit>
-__device__ inline void tri_potrf_inverse_lower(double *S, int NP, double *W, int *bad_col,
-                                               double *bad_val, Emit emit) {
-  __shared__ int s_bad;
-  __shared__ double s_rd[SUB];
-  __shared__ double s_col[2 * SUB];
-  if (threadIdx.x == 0) s_bad = -1;
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nsub = NP / SUB;
-  for (int s = 0; s <= nsub; ++s) {
-    const int jb = s * SUB;
-    // ---- F ----
-    if (warp == 0) {
-      if (s < nsub) {
-        double r[SUB];
-#pragma unroll
-        for (int j = 0; j < SUB; ++j) r[j] = (j <= lane) ? S[(jb + lane) * LDS + jb + j] : 0.0;
-        double unused;
-        warp_potrf32<false>(r, lane, &unused, s_col);
-        double dg = r[0];
-#pragma unroll
-        for (int j = 1; j < SUB; ++j) dg = (j == lane) ? r[j] : dg;
-        if (__ballot_sync(0xffffffffu, isnan(dg)) != 0u) {
-#pragma unroll
-          for (int j = 0; j < SUB; ++j) r[j] = (j <= lane) ? S[(jb + lane) * LDS + jb + j] : 0.0;
-          double badv = 0.0;
-          const int bad = warp_potrf32<true>(r, lane, &badv, s_col);
-          if (lane == 0) {
-            s_bad = jb + bad;
-            *bad_val = badv;
-          }
-        }
-        s_rd[lane] = 1.0 / dg;
-#pragma unroll
-        for (int j = 0; j < SUB; ++j)
-          if (j <= lane) S[(jb + lane) * LDS + jb + j] = r[j];
-      }
-    } else if (s >= 1) {
-      const int tid = threadIdx.x - 32;  // 0 .. 223 among warps 1..7
-      if (warp >= 2 && s < nsub) {
-        // sub-panel s - 1 into the bands right of band s (band s got it in U of s - 1)
-        if (jb + SUB < NP) tri_syrk_part(S, NP, jb + SUB, jb + SUB, NP, jb - SUB, threadIdx.x - 64, 192);
-      } else if (warp == 1 && s < nsub) {
-        emit(s - 1, lane, 32);
-        __syncwarp();
-        tri_leaf_inverse(S, jb - SUB, lane);
-      }
-      if (s < nsub) {
-        tri_bar_helpers();
-        tri_inverse_row(S, W, s - 1, tid, 224, tri_bar_helpers);
-      }
-    }
-    __syncthreads();
-    if (s_bad >= 0) break;
-    if (s == nsub) {
-      // the last row block: emitted and inverted by all threads
-      const int b = jb - SUB;
-      emit(nsub - 1, threadIdx.x, blockDim.x);
-      __syncthreads();
-      if (warp == 0) tri_leaf_inverse(S, b, lane);
-      __syncthreads();
-      tri_inverse_row(S, W, nsub - 1, threadIdx.x, blockDim.x, [] { __syncthreads(); });
-      __syncthreads();
-      break;
-    }
-    // ---- R: rows below leaf s, L(i, jb:jb+32) = A(i, jb:jb+32) * L_ss^-T ----
-    for (int i = jb + SUB + threadIdx.x; i < NP; i += blockDim.x) {
-      double v[SUB];
-      double *row = S + i * LDS + jb;
-#pragma unroll
-      for (int k = 0; k < SUB; ++k) v[k] = row[k];
-#pragma unroll
-      for (int k = 0; k < SUB; ++k) {
-        v[k] = v[k] * s_rd[k];
-#pragma unroll
-        for (int m = k + 1; m < SUB; ++m) v[m] = fma(-v[k], S[(jb + m) * LDS + jb + k], v[m]);
-      }
-#pragma unroll
-      for (int k = 0; k < SUB; ++k) row[k] = v[k];
-    }
-    __syncthreads();
-    // ---- U: band s + 1 gets sub-panel s ----
-    if (jb + SUB < NP) tri_syrk_part(S, NP, jb + SUB, jb + SUB, jb + 2 * SUB, jb, threadIdx.x, blockDim.x);
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) *bad_col = s_bad;
-  __syncthreads();
-}
-
 }  // namespace mo

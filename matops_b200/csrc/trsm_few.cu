@@ -58,6 +58,7 @@ struct FewArgs {
   int epoch;
   int *status;
   uint32_t spin_limit;  // polls of a step flag before the wait gives up (MO_EDEVTIMEOUT)
+  const int *skip;      // optional: when the word is set at launch the grid returns at once
 };
 
 // step flags sit one per 128-byte line, and pollers read them with acquire loads (not
@@ -186,6 +187,7 @@ constexpr int few_smem() { return few_smem_ch<TA, NT>(few_ch<TA, NT>()); }
 
 template <typename TA, int NT>
 __global__ void __launch_bounds__(FEW_THREADS, 1) trsm_few_kernel(FewArgs p) {
+  if (p.skip && *(volatile const int *)p.skip) return;
   constexpr int CH = few_ch<TA, NT>(), LDXK = CH * TB + 4;  // X chunk: column-major, ld LDXK
   constexpr int CBLK = TB * few_block_ld<TA>(false);        // chunk buffer elements per block
   constexpr int XPT = CH * TB * 8 * NT / FEW_THREADS;  // X values per thread per chunk
@@ -369,6 +371,7 @@ static_assert(pair_smem<8>() <= 227 * 1024 - 64, "pair kernel shared memory");
 
 template <int NT>
 __global__ void __launch_bounds__(PAIR_THREADS, 1) trsm_pair_kernel(FewArgs p) {
+  if (p.skip && *(volatile const int *)p.skip) return;
   constexpr int LDXK = TB + 4;                        // X buffers: column-major 64 x 8NT
   constexpr int XPT = TB * 8 * NT / PAIR_THREADS;    // X values per thread per block
   extern __shared__ double sm[];
@@ -565,7 +568,8 @@ int launch_pair(mo_ctx *ctx, FewArgs &p) {
 
 // flags -> (B strides, effective transposition and sweep direction) and the launch
 int few_run(mo_ctx *ctx, View B, const void *A, bool a32, int64_t lda, int N, int flags,
-            double alpha, const double *inv, bool inv_t, int *flag_buf) {
+            double alpha, const double *inv, bool inv_t, int *flag_buf,
+            const int *skip = nullptr) {
   const bool right = (flags & MO_RIGHT) != 0;
   const bool upper = (flags & MO_UPPER) != 0;
   bool tr = (flags & MO_TRANSA) != 0;
@@ -599,6 +603,7 @@ int few_run(mo_ctx *ctx, View B, const void *A, bool a32, int64_t lda, int N, in
   p.epoch = ++ctx->sk_epoch;
   p.status = reinterpret_cast<int *>(ctx->d_status);
   p.spin_limit = ctx->spin_limit;
+  p.skip = skip;
   // more than MO_FEW_GROUP columns: groups solved side by side by separate CTA sets, so
   // the per-step work on the dependency chain is that of one group
   const bool pair = a32 && p.nblk >= 4;
@@ -659,9 +664,9 @@ int trsm_few(mo_ctx *ctx, View B, View A, int flags, double alpha, double *inv, 
 // FP64 inverses of L's 128 x 128 diagonal blocks (ld 128): op(L) X = B in place, op = L
 // (trans == false) or L^T.
 int trsm_few_f32(mo_ctx *ctx, View B, const float *L, int64_t ldl, int N, bool trans,
-                 const double *inv_L, int *flag_buf) {
+                 const double *inv_L, int *flag_buf, const int *skip) {
   const int flags = MO_LOWER | (trans ? MO_TRANSA : 0);
-  return few_run(ctx, B, L, true, ldl, N, flags, 1.0, inv_L, trans, flag_buf);
+  return few_run(ctx, B, L, true, ldl, N, flags, 1.0, inv_L, trans, flag_buf, skip);
 }
 
 }  // namespace mo

@@ -47,12 +47,12 @@ def test_mult_sym(gpu, ref, rng, n, p, flags):
     Cg = dev(gpu, C0)
     assert gpu.MultSym(Cg, dev(gpu, A), dev(gpu, B), 1.5, -0.5, flags) is None
     S = sym(A, flags)
-    if flags & LEFT or n <= 68:
+    if flags & LEFT or (flags & RIGHT and n <= 68):
         Cr = C0.copy(order="F")
         assert ref.MultSym(Cr, A, B, 1.5, -0.5, flags) == 0
     else:
-        # the reference's blocked paths above its block size: right side wrong, no side bit
-        # mixed (recorded in DESIGN); the documented product instead
+        # the reference's right-side blocked path above its block size and its no-side-bit
+        # mixture of the two branches are wrong (recorded in DESIGN): the documented product
         Cr = -0.5 * C0 + 1.5 * ((S @ B) if left else (B @ S))
     err = fro(Cg.cpu().numpy() - Cr)
     assert err <= 4 * n * EPS * (1.5 * fro(S) * fro(B) + 0.5 * fro(C0)) + 1e-300, err
