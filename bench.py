@@ -972,7 +972,7 @@ def main():
             "warmup": W, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": f"{args.prec}+f64", "data": "synthetic",
             "config": {"workload": workload(n, nrhs), "n": n, "nrhs": nrhs,
-                       "factor": f"{args.prec.upper()} split products, FP32 storage, FP64 128x128 diagonal blocks",
+                       "factor": f"{args.prec.upper()} split products, FP32 storage, FP32 128x128 diagonal blocks",
                        "refinement": "FP64 residual and update, classic IR / GMRES-IR (auto), tol 1e-14",
                        "l2": "A (2 GiB FP64) is re-read from HBM by every step (inputs > L2)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},

@@ -11,7 +11,8 @@
 //              with info = column + 1 (the reference panics, chol.go:33-36)
 //     panel  : rows below, one thread per row: x = a * L11^-T by forward substitution
 //     update : A22 -= L21 L21^T on 64 x 64 lower tiles, K = NB, operands staged in
-//              shared memory by cp.async (double-buffered), 4 x 4 FP64 FMA register tile
+//              shared memory by cp.async (double-buffered), products on the FP64 tensor
+//              pipe (mma.sync m16n8k4, 32 x 16 per warp)
 //   LU (partial pivoting, right-looking, panel width NB):
 //     panel  : the (n - j) x NB panel in registers (thread t owns logical rows j + t and
 //              j + t + 256); per column a block argmax of |a| with ties to the lowest row
@@ -27,9 +28,9 @@
 //     32-row blocks: a warp solves the diagonal block by shuffles, the other rows are
 //     updated in axpy form (columns of the factor are read contiguously)
 //
-// FP64 FMA and the FP64 tensor pipe have the same peak on B200, so the small products run
-// as register-tiled FMAs; the triangular and pivoting steps are latency-bound and use
-// warp shuffles to avoid block-wide barriers.
+// FP64 FMA and the FP64 tensor pipe have the same peak on B200, but one m16n8k4 MMA does
+// the work of sixteen warp FMAs, which leaves the issue slots to the loads; the triangular
+// and pivoting steps are latency-bound and use warp shuffles to avoid block-wide barriers.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -42,6 +43,8 @@ namespace {
 
 constexpr int BT = 256;   // threads per CTA
 constexpr int TM = 64;    // update tile (TM x TM)
+constexpr int TMP = TM + 4;  // staged row stride: fragment loads (lane 4g + t reads row t,
+                             // element g) fall in distinct banks
 constexpr int MAXN = MO_BATCH_MAX_N;
 constexpr int RPT = MAXN / BT;  // panel rows per thread (LU)
 
@@ -62,8 +65,8 @@ struct BatchParams {
 
 template <int NB>
 struct Smem {
-  double As[2][NB][TM];  // update operands, double-buffered
-  double Bs[2][NB][TM];
+  double As[2][NB][TMP];  // update operands, double-buffered
+  double Bs[2][NB][TMP];
   double L11[NB][NB + 1];
   double vec[MAXN];      // solve vector
   double ubuf[NB];       // LU: pivot row
@@ -155,15 +158,18 @@ __device__ __forceinline__ int block_argmax(Smem<NB> &s, double v, int i) {
 //               : A[(j0 + c) + (kc + k) * ld]                   (L21^T, Cholesky)
 // row() is the LU row map (identity for Cholesky).  Cholesky updates only tiles on or
 // below the diagonal and, inside diagonal tiles, only elements with row >= column.
-// Tile t + 1's operands are staged while tile t is computed.  Ends with a barrier.
+// Tile t + 1's operands are staged while tile t is computed.  The products run on the
+// FP64 tensor pipe: warp w owns the 32 x 16 block at rows 32 (w & 1), columns 16 (w >> 1)
+// of the 64 x 64 tile, as 2 x 2 fragments of mma.sync m16n8k4 (k padded to a multiple of
+// 4 with the zeros the staging writes past kb).  Ends with a barrier.
 template <bool LU, int NB>
 __device__ void trailing_update(Smem<NB> &s, double *A, int64_t ld, int j0, int m2, int kc,
                                 int kb, const double *ut) {
   const int nt = (m2 + TM - 1) / TM;
   const int T = LU ? nt * nt : nt * (nt + 1) / 2;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wr = warp & 1, wc = warp >> 1, lr = lane & 7, lc = lane >> 3;
-  const int rbase = 32 * wr + 2 * lr, cbase = 16 * wc + 2 * lc;
+  const int g = lane >> 2, t4 = lane & 3;
+  const int rw = 32 * (warp & 1), cw = 16 * (warp >> 1);
   auto tile_of = [&](int t, int &ti, int &tj) {
     if (LU) {
       ti = t % nt;
@@ -205,51 +211,65 @@ __device__ void trailing_update(Smem<NB> &s, double *A, int64_t ld, int j0, int 
     int ti, tj;
     tile_of(t, ti, tj);
     const int r0 = ti * TM, c0 = tj * TM;
-    // this thread's C elements: rows rbase + {0,1} + 16a, columns cbase + {0,1} + 8b
-    double cv[4][4];
-    int64_t roff[4];
+    // this thread's C elements (fragment layout): rows rw + 16 mi + g + 8 h,
+    // columns cw + 8 ni + 2 t4 + e, accumulator index d[mi][ni][2 h + e]
+    double cv[2][2][4];
+    int64_t roff[2][2];
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      const int i = r0 + rbase + (a & 1) + 16 * (a >> 1);
-      roff[a] = i < m2 ? (int64_t)row_of(j0 + i) : -1;
-    }
+    for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const int c = c0 + cbase + (b & 1) + 8 * (b >> 1);
-        cv[a][b] = (roff[a] >= 0 && c < m2) ? A[roff[a] + (int64_t)(j0 + c) * ld] : 0.0;
+      for (int h = 0; h < 2; ++h) {
+        const int i = r0 + rw + 16 * mi + g + 8 * h;
+        roff[mi][h] = i < m2 ? (int64_t)row_of(j0 + i) : -1;
       }
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int c = c0 + cw + 8 * ni + 2 * t4 + (q & 1);
+          const int64_t ro = roff[mi][q >> 1];
+          cv[mi][ni][q] = (ro >= 0 && c < m2) ? A[ro + (int64_t)(j0 + c) * ld] : 0.0;
+        }
     cp_wait1();
     __syncthreads();
-    double acc[4][4];
+    double d[2][2][4];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
-      for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-#pragma unroll 4
-    for (int k = 0; k < kb; ++k) {
-      const double2 p0 = *reinterpret_cast<const double2 *>(&s.As[buf][k][rbase]);
-      const double2 p1 = *reinterpret_cast<const double2 *>(&s.As[buf][k][rbase + 16]);
-      const double2 q0 = *reinterpret_cast<const double2 *>(&s.Bs[buf][k][cbase]);
-      const double2 q1 = *reinterpret_cast<const double2 *>(&s.Bs[buf][k][cbase + 8]);
-      const double pv[4] = {p0.x, p0.y, p1.x, p1.y};
-      const double qv[4] = {q0.x, q0.y, q1.x, q1.y};
+      for (int ni = 0; ni < 2; ++ni)
 #pragma unroll
-      for (int a = 0; a < 4; ++a)
+        for (int q = 0; q < 4; ++q) d[mi][ni][q] = 0.0;
+    const int ksteps = (kb + 3) >> 2;
+#pragma unroll 2
+    for (int k4 = 0; k4 < ksteps; ++k4) {
+      const int k = 4 * k4 + t4;
+      double a[2][2], b[2];
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = fma(pv[a], qv[b], acc[a][b]);
-    }
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      const int i = r0 + rbase + (a & 1) + 16 * (a >> 1);
-#pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const int c = c0 + cbase + (b & 1) + 8 * (b >> 1);
-        const bool ok = roff[a] >= 0 && c < m2 && (LU || i >= c);
-        if (ok) A[roff[a] + (int64_t)(j0 + c) * ld] = cv[a][b] - acc[a][b];
+      for (int mi = 0; mi < 2; ++mi) {
+        a[mi][0] = s.As[buf][k][rw + 16 * mi + g];
+        a[mi][1] = s.As[buf][k][rw + 16 * mi + g + 8];
       }
+#pragma unroll
+      for (int ni = 0; ni < 2; ++ni) b[ni] = s.Bs[buf][k][cw + 8 * ni + g];
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 2; ++ni) dmma_16x8x4(d[mi][ni], a[mi][0], a[mi][1], b[ni]);
     }
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int i = r0 + rw + 16 * mi + g + 8 * (q >> 1);
+          const int c = c0 + cw + 8 * ni + 2 * t4 + (q & 1);
+          const int64_t ro = roff[mi][q >> 1];
+          const bool ok = ro >= 0 && c < m2 && (LU || i >= c);
+          if (ok) A[ro + (int64_t)(j0 + c) * ld] = cv[mi][ni][q] - d[mi][ni][q];
+        }
     __syncthreads();
   }
   cp_wait0();

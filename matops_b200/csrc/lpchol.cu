@@ -1,20 +1,22 @@
 // Mixed-precision blocked Cholesky: the trailing updates and panel products run as
 // split-product GEMMs (lpgemm.cu) on an FP32 working copy, the 128 x 128 diagonal blocks
-// are factored and inverted in FP64.
+// are factored and inverted in FP32 (inverses kept in FP64 for the refinement).
 //
 // The working matrix W is NP x NP FP32 (NP = n rounded up to 128) holding the lower
 // triangle of A (or the transpose of its upper triangle), padded with the identity so
-// the padded factor is diag(L, I).  Step k (128 columns), right-looking as in the FP64
-// driver (potrf.cu) with the same one-step look-ahead:
-//   diag   : W11 -> FP64, Cholesky + inverse in shared memory; L11 back to W (FP32), the
-//            FP64 inverse kept for the refinement solves, the split inverse for (panel)
+// the padded factor is diag(L, I).  Block column k (128 columns), right-looking as in the
+// FP64 driver (potrf.cu):
+//   diag   : W11 Cholesky + inverse in shared memory (FP32); L11 back to W, the inverse
+//            kept in FP64 for the refinement solves and split for (panel)
 //   panel  : L21 = A21 * L11^-T   (split-product GEMM, written over A21; its epilogue also
-//            writes the K-major hi/lo panel P)
-//   update : W22 -= P P^T (lower), the next block column first on the look-ahead path; that
-//            launch's epilogue writes the next step's split A21, so no separate split pass
-//            sits on the step-to-step chain
-// A NaN pivot stops the factorization; its global column is reported like
-// DecomposeCHOL's (info = column + 1).
+//            writes the K-major hi/lo panel)
+//   update : W22 -= P P^T (lower), applied for two block columns at once (K = 256) so that
+//            the trailing matrix is read and written half as often; the next pair's two
+//            columns are updated first, and that launch's epilogue writes the split A21 of
+//            the next panel, so no separate split pass sits on the step-to-step chain
+// The diagonal blocks and panels of a pair run on a look-ahead stream while the previous
+// pair's trailing update runs on the caller's.  A NaN pivot stops the factorization; its
+// global column is reported like DecomposeCHOL's (info = column + 1).
 #include <cuda_bf16.h>
 
 #include "lp.cuh"
@@ -26,8 +28,11 @@ namespace {
 
 constexpr int NB = 128;
 
-// W block (FP32, column-major) -> S (FP64 lower, row-major, LDS)
-__device__ inline void lp_load_block(double *S, const float *G, int64_t ld) {
+// shared memory of lp_diag_kernel: the FP32 block plus the inverse's scratch sub-blocks
+constexpr int LP_DIAG_SMEM = (TRI_MAX * LDS + 4 * SUB * (SUB + 1)) * (int)sizeof(float);
+
+// W block (FP32, column-major) -> S (FP32 lower, row-major, LDS)
+__device__ inline void lp_load_block(float *S, const float *G, int64_t ld) {
   for (int base = threadIdx.x; base < NB * NB; base += 8 * blockDim.x) {
     float v[8];
 #pragma unroll
@@ -39,19 +44,25 @@ __device__ inline void lp_load_block(double *S, const float *G, int64_t ld) {
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const int e = base + u * blockDim.x;
-      if (e < NB * NB) S[(e % NB) * LDS + e / NB] = (double)v[u];
+      if (e < NB * NB) S[(e % NB) * LDS + e / NB] = v[u];
     }
   }
 }
 
+// The diagonal block is factored and inverted in FP32, the precision of the working
+// matrix it comes from and goes back to: its rounding is below that of the split-product
+// updates that formed it (BF16x3) or equal to it (TF32x3), and the FP32 column chain
+// (single-instruction reciprocal square root, 4-cycle FMA, one shuffle per value) is much
+// shorter than the FP64 one.  The inverse goes out as FP64 (for the refinement solves)
+// and split (for the panel product).
 template <int PREC>
 __global__ void __launch_bounds__(TRI_THREADS)
     lp_diag_kernel(float *W, int64_t ldw, double *inv, char *ihi, char *ilo, int *info,
                    double *bad_value, int col0, int n_true) {
   if (*(volatile int *)info != 0) return;
-  extern __shared__ double sm[];
-  double *S = sm;
-  double *Wk = sm + TRI_MAX * LDS;
+  extern __shared__ float smf[];
+  float *S = smf;
+  float *Wk = smf + TRI_MAX * LDS;
   __shared__ int s_bad;
   __shared__ double s_badv;
   lp_load_block(S, W, ldw);
@@ -67,19 +78,19 @@ __global__ void __launch_bounds__(TRI_THREADS)
   }
   for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
     const int i = e % NB, j = e / NB;
-    if (i >= j) W[i + (int64_t)j * ldw] = (float)S[i * LDS + j];
+    if (i >= j) W[i + (int64_t)j * ldw] = S[i * LDS + j];
   }
   __syncthreads();
   tri_inverse_lower(S, NB, Wk);
   __syncthreads();
   for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
     const int i = e % NB, j = e / NB;
-    inv[i + j * NB] = (i >= j) ? S[i * LDS + j] : 0.0;
+    inv[i + j * NB] = (i >= j) ? (double)S[i * LDS + j] : 0.0;
   }
   // split inverse, K-major: row r = row r of L11^-1 (the B operand of A21 * L11^-T)
   for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
     const int r = e / NB, k = e % NB;
-    const float x = (r >= k) ? (float)S[r * LDS + k] : 0.f;
+    const float x = (r >= k) ? S[r * LDS + k] : 0.f;
     if (PREC == kLpBf16x3) {
       const __nv_bfloat16 h = __float2bfloat16_rn(x);
       const __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
@@ -132,7 +143,7 @@ __global__ void __launch_bounds__(256) lp_convert_kernel(const double *A, int64_
 
 template <int PREC>
 int set_lp_diag_smem() {
-  return mo_smem_attr((const void *)lp_diag_kernel<PREC>, TRI_SMEM_BYTES);
+  return mo_smem_attr((const void *)lp_diag_kernel<PREC>, LP_DIAG_SMEM);
 }
 
 // diagonal block + panel of step k on ctx->stream; P receives the split L21.  The split
@@ -144,10 +155,10 @@ int lp_panel(mo_ctx *ctx, LpChol &f, int k, int *d_info, double *d_bad, const Lp
   ProfScope ps;
   prof_begin(ctx, ps, MO_PROF_DIAG);
   if (f.prec == kLpBf16x3)
-    lp_diag_kernel<kLpBf16x3><<<1, TRI_THREADS, TRI_SMEM_BYTES, ctx->stream>>>(
+    lp_diag_kernel<kLpBf16x3><<<1, TRI_THREADS, LP_DIAG_SMEM, ctx->stream>>>(
         Wkk, f.ldw, inv, (char *)f.Linv.hi, (char *)f.Linv.lo, d_info, d_bad, k, f.n);
   else
-    lp_diag_kernel<kLpTf32x3><<<1, TRI_THREADS, TRI_SMEM_BYTES, ctx->stream>>>(
+    lp_diag_kernel<kLpTf32x3><<<1, TRI_THREADS, LP_DIAG_SMEM, ctx->stream>>>(
         Wkk, f.ldw, inv, (char *)f.Linv.hi, (char *)f.Linv.lo, d_info, d_bad, k, f.n);
   prof_end(ctx, ps, 2.0 * NB * NB * NB / 3.0, 4.0 * 2.0 * NB * NB + 8.0 * NB * NB);
   MO_CUDA_TRY(cudaGetLastError());
@@ -180,7 +191,7 @@ size_t lp_chol_bytes(int n, int prec) {
   return NP * NP * 4                 // W
          + (NP / NB) * NB * NB * 8   // FP64 inverses
          + 2 * NB * NB * es          // split inverse
-         + 3 * 2 * NP * NB * es      // PA, P[0], P[1]
+         + 3 * 2 * NP * 2 * NB * es  // PA, P[0], P[1] (two panels wide)
          + 4096;
 }
 
@@ -203,9 +214,9 @@ int lp_chol_setup(int n, int prec, void *mem, LpChol &f) {
   f.Linv.ldk = NB;
   LpSplit *bufs[3] = {&f.PA, &f.P[0], &f.P[1]};
   for (LpSplit *b : bufs) {
-    b->hi = take(NP * NB * es);
-    b->lo = take(NP * NB * es);
-    b->ldk = NB;
+    b->hi = take(NP * 2 * NB * es);
+    b->lo = take(NP * 2 * NB * es);
+    b->ldk = 2 * NB;
   }
   return MO_OK;
 }
@@ -221,65 +232,88 @@ int lp_chol_convert(mo_ctx *ctx, const LpChol &f, View A, bool upper, double shi
   return MO_OK;
 }
 
-// Right-looking factorization of W with one step of look-ahead (the structure of potrf):
-//   S0 (caller):  [update next block column | record E0] [update the rest of the trailing
-//                  matrix, leaving free_sms SMs]
-//   S1 (aux):     wait E0 -> diag + panel + split of the next step -> record E1
+// Right-looking factorization of W, two 128-column steps per trailing update (K = 256),
+// with look-ahead.  Pair p covers block columns a = 2p and b = a + 1; Q = f.P[p & 1]
+// holds their split panels side by side (K-major, 256 wide; row 0 = row 128 (a + 1) of
+// W): L21 of a in k 0..127 from row 0, L21 of b in k 128..255 from row 128.
+//   S1 (aux):  [diag a, panel a -> Q] [column b -= L21_a (rows of b) ^T] [diag b,
+//              panel b -> Q] -> record E1
+//   S0 (main): wait E1 -> [columns a + 2, a + 3 -= Q Q^T (K = 256), split A21 of a + 2
+//              -> PA] -> record E0 -> [the rest of the trailing matrix (K = 256)]
+//   S1 waits E0 before the next pair.
 int lp_chol_factor(mo_ctx *ctx, LpChol &f, int *d_info, double *d_bad) {
   int rc = f.prec == kLpBf16x3 ? set_lp_diag_smem<kLpBf16x3>() : set_lp_diag_smem<kLpTf32x3>();
   if (rc) return rc;
   const int NP = f.NP;
+  const int es = lp_esize(f.prec);
   cudaStream_t s0 = ctx->stream, s1 = nullptr;
   if ((rc = aux_stream(ctx, &s1))) return rc;
   if ((rc = stream_wait(ctx, s1, s0, ctx->ev_fork))) return rc;
-  // SMs the trailing update leaves to the look-ahead stream (diagonal block + panel);
-  // measured at n = 16384: 2 -> 34.26 ms, 8 -> 34.4 ms, 16 -> 34.82 ms per solve
   const int free_sms = 2;
-  {
-    StreamSwap sw(ctx, s1);
-    if ((rc = lp_panel(ctx, f, 0, d_info, d_bad, f.P[0]))) return rc;
-  }
-  for (int k = 0, step = 0; k < NP; k += NB, ++step) {
-    const int rest = NP - k - NB;
-    if ((rc = stream_wait(ctx, s0, s1, ctx->ev_join))) return rc;  // panel k done
+  for (int ka = 0, pair = 0; ka < NP; ka += 2 * NB, ++pair) {
+    const int kb = ka + NB;
+    LpSplit &Q = f.P[pair & 1];
+    // Q shifted to (row 128, k 128): where panel b's split goes
+    const LpSplit Qb{(char *)Q.hi + (size_t)(NB * Q.ldk + NB) * es,
+                     (char *)Q.lo + (size_t)(NB * Q.ldk + NB) * es, Q.ldk};
+    {
+      StreamSwap sw(ctx, s1);
+      if ((rc = lp_panel(ctx, f, ka, d_info, d_bad, Q))) return rc;
+      if (kb < NP) {
+        // column b -= L21_a L21_a(rows of b)^T; its rows below b's diagonal block are
+        // panel b's A21: split into PA by the epilogue
+        LpGemmArgs g;
+        g.M = NP - kb;
+        g.N = NB;
+        g.K = NB;
+        g.alpha = -1.f;
+        g.beta = 1.f;
+        g.A = Q;
+        g.B = Q;
+        g.C = f.W + kb + (int64_t)kb * f.ldw;
+        g.ldc = f.ldw;
+        g.mode = kGemmLower;
+        g.out = f.PA;
+        g.out_row0 = NB;
+        if ((rc = lp_gemm(ctx, f.prec, g))) return rc;
+        if ((rc = lp_panel(ctx, f, kb, d_info, d_bad, Qb))) return rc;
+      }
+    }
+    if ((rc = stream_wait(ctx, s0, s1, ctx->ev_join))) return rc;  // pair's panels done
+    const int kc = ka + 2 * NB;  // first column of the next pair
+    const int rest = NP - kc;
     if (rest <= 0) break;
-    const LpSplit &P = f.P[step & 1];
-    float *W22 = f.W + (k + NB) + (int64_t)(k + NB) * f.ldw;
-    // 1. next block column (rest x 128, its top 128 x 128 block is diagonal)
+    float *W22 = f.W + kc + (int64_t)kc * f.ldw;
+    const LpSplit Qr = lp_rows(Q, f.prec, NB);  // rows from kc
+    // 1. the next pair's two columns (one if only one is left), K = 256
+    const int nn = std::min(2 * NB, rest);
     LpGemmArgs g;
     g.M = rest;
-    g.N = NB;
-    g.K = NB;
+    g.N = nn;
+    g.K = 2 * NB;
     g.alpha = -1.f;
     g.beta = 1.f;
-    g.A = P;
-    g.B = P;
+    g.A = Qr;
+    g.B = Qr;
     g.C = W22;
     g.ldc = f.ldw;
     g.mode = kGemmLower;
-    // rows below its top 128 x 128 block are the next step's A21: the epilogue splits them
-    // into f.PA for the next panel (which runs after this launch, on the look-ahead stream)
-    g.out = f.PA;
+    g.out = f.PA;  // rows below the next pair's first diagonal block: its A21, split
     g.out_row0 = NB;
     if ((rc = lp_gemm(ctx, f.prec, g))) return rc;
     if ((rc = stream_wait(ctx, s1, s0, ctx->ev_fork))) return rc;
-    // 2. the next step's diagonal block and panel on the look-ahead stream
-    {
-      StreamSwap sw(ctx, s1);
-      if ((rc = lp_panel(ctx, f, k + NB, d_info, d_bad, f.P[(step + 1) & 1]))) return rc;
-    }
-    // 3. the rest of the trailing matrix
-    const int r2 = rest - NB;
+    // 2. the rest of the trailing matrix, K = 256
+    const int r2 = rest - nn;
     if (r2 > 0) {
       LpGemmArgs t;
       t.M = r2;
       t.N = r2;
-      t.K = NB;
+      t.K = 2 * NB;
       t.alpha = -1.f;
       t.beta = 1.f;
-      t.A = lp_rows(P, f.prec, NB);
+      t.A = lp_rows(Qr, f.prec, nn);
       t.B = t.A;
-      t.C = W22 + NB + (int64_t)NB * f.ldw;
+      t.C = W22 + nn + (int64_t)nn * f.ldw;
       t.ldc = f.ldw;
       t.mode = kGemmLower;
       t.max_ctas = ctx->sms - free_sms;

@@ -10,8 +10,9 @@ struct LpChol {
   int64_t ldw = 0;
   double *inv = nullptr;  // NP/128 FP64 inverses of L's 128 x 128 diagonal blocks
   LpSplit Linv{};         // split inverse of the current diagonal block
-  LpSplit PA{};           // split A21 of the current panel
-  LpSplit P[2]{};         // split L21 panels, by step parity
+  LpSplit PA{};           // split A21 of the next panel (256 wide: two block columns)
+  LpSplit P[2]{};         // split L21 of a pair of panels side by side (K-major, 256
+                          // wide), by pair parity
 };
 
 // device bytes for the workspace of an order-n factorization

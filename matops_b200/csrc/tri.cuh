@@ -2,7 +2,9 @@
 // lower-triangular inverse.  A block lives in shared memory as S[i*LDS + j] = element
 // (i, j) (row-major, padded row length LDS = 129 so that threads walking down a column
 // touch distinct banks).  Blocks of order n are padded to NP = roundup(n, 32) with the
-// identity, so every routine works on whole 32 x 32 sub-blocks.
+// identity, so every routine works on whole 32 x 32 sub-blocks.  The factor and inverse
+// routines are templates on the element type: FP64 for the FP64 drivers, FP32 for the
+// diagonal blocks of the mixed-precision factorization (whose working matrix is FP32).
 #pragma once
 #include "common.cuh"
 
@@ -16,6 +18,11 @@ constexpr int TRI_THREADS = 256;
 constexpr int TRI_SMEM_BYTES = (TRI_MAX * LDS + 4 * SUB * (SUB + 1)) * 8;
 
 __device__ __forceinline__ int round_up32(int n) { return (n + 31) & ~31; }
+
+__device__ __forceinline__ double tri_rsqrt(double x) { return rsqrt(x); }
+__device__ __forceinline__ float tri_rsqrt(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double tri_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float tri_sqrt(float x) { return sqrtf(x); }
 
 // Load the n x n block at G (column-major, ld) into S as a LOWER triangle:
 //   transpose == false: S(i,j) = G(i,j) for i >= j
@@ -75,7 +82,8 @@ __device__ inline void tri_store_lower(const double *S, double *G, int64_t ld, i
 // rows/cols [r0, NP).  The region is cut into 32 x 32 blocks (bi >= bj); 64 threads own
 // one block as an 8 x 8 grid of 4 x 4 micro-tiles whose rows and columns are strided by
 // 8, so the 8 rows a warp reads sit in distinct banks.
-__device__ __forceinline__ void tri_syrk_update(double *S, int NP, int r0, int kb) {
+template <typename T>
+__device__ __forceinline__ void tri_syrk_update(T *S, int NP, int r0, int kb) {
   const int nbk = (NP - r0) / SUB;
   const int ntask = nbk * (nbk + 1) / 2;
   const int t = threadIdx.x & 63, tx = t & 7, ty = t >> 3;
@@ -85,14 +93,14 @@ __device__ __forceinline__ void tri_syrk_update(double *S, int NP, int r0, int k
     while ((bi + 1) * (bi + 2) / 2 <= task) ++bi;
     const int bj = task - bi * (bi + 1) / 2;
     const int i0 = r0 + bi * SUB + tx, j0 = r0 + bj * SUB + ty;
-    double acc[4][4];
+    T acc[4][4];
 #pragma unroll
     for (int x = 0; x < 4; ++x)
 #pragma unroll
-      for (int y = 0; y < 4; ++y) acc[x][y] = 0.0;
+      for (int y = 0; y < 4; ++y) acc[x][y] = T(0);
 #pragma unroll 8
     for (int k = 0; k < SUB; ++k) {
-      double a[4], b[4];
+      T a[4], b[4];
 #pragma unroll
       for (int x = 0; x < 4; ++x) {
         a[x] = S[(i0 + 8 * x) * LDS + kb + k];
@@ -118,18 +126,17 @@ __device__ __forceinline__ void tri_syrk_update(double *S, int NP, int r0, int k
 // right of its diagonal, which are never read, and this keeps the unrolled body free of
 // divergent branches (measured 4.4x faster than guarding each update with lane >= j).
 // With `checked`, the column loop stops at the first NaN pivot and returns its index.
-// `col` is 2 x 32 doubles of shared memory (two alternating multiplier columns).
-template <bool checked>
-__device__ __forceinline__ int warp_potrf32(double (&r)[SUB], int lane, double *badv,
-                                            double *col) {
+// `col` is 2 x 32 elements of shared memory (two alternating multiplier columns).
+template <bool checked, typename T>
+__device__ __forceinline__ int warp_potrf32(T (&r)[SUB], int lane, double *badv, T *col) {
   int bad = -1;
 #pragma unroll
   for (int k = 0; k < SUB; ++k) {
-    const double akk = __shfl_sync(0xffffffffu, r[k], k);
+    const T akk = __shfl_sync(0xffffffffu, r[k], k);
     // the column is scaled by rsqrt(akk) (one reciprocal square root on the dependency
     // chain instead of a square root followed by a division); the stored pivot is
     // sqrt(akk), which nothing on the chain waits for
-    const double rs = rsqrt(akk);
+    const T rs = tri_rsqrt(akk);
     if (checked) {
       if (isnan(rs)) {  // uniform: every lane sees the same akk
         bad = k;
@@ -142,13 +149,13 @@ __device__ __forceinline__ int warp_potrf32(double (&r)[SUB], int lane, double *
     // pay each shuffle's latency in turn.  Columns alternate between two buffers, so the
     // next column's store need not wait for every lane to finish reading this one (the
     // __syncwarp of column k + 1 orders column k's reads before column k + 2's stores).
-    double *c = col + (k & 1) * SUB;
-    const double lk = lane > k ? r[k] * rs : 0.0;
+    T *c = col + (k & 1) * SUB;
+    const T lk = lane > k ? r[k] * rs : T(0);
     c[lane] = lk;
     __syncwarp();
 #pragma unroll
     for (int j = k + 1; j < SUB; ++j) r[j] = fma(-lk, c[j], r[j]);
-    r[k] = lane == k ? sqrt(akk) : (lane > k ? lk : r[k]);
+    r[k] = lane == k ? tri_sqrt(akk) : (lane > k ? lk : r[k]);
   }
   return bad;
 }
@@ -156,33 +163,34 @@ __device__ __forceinline__ int warp_potrf32(double (&r)[SUB], int lane, double *
 // In-place Cholesky of the lower triangle of S (order NP, multiple of 32), right-looking
 // over 32-column sub-panels.  The pivot is sqrt(s_kk); when it is NaN (s_kk < 0 or NaN)
 // the column index is returned through *bad_col (first failure) and the routine stops.
-// Must be called by all threads of the block.
+// Must be called by all threads of the block.  *bad_val receives the failing pivot.
 //   (1) 32 x 32 diagonal sub-block: one warp, lane i holds row i in registers; the fast
 //       unchecked factor runs first and the checked one reruns only if a pivot was NaN
 //   (2) rows below: one thread per row, the 32-wide row segment in registers, scaled by
 //       the reciprocal pivots (as LAPACK dpotf2 scales by 1/ajj)
 //   (3) trailing lower triangle: register-blocked rank-32 update
-__device__ inline void tri_potrf_lower(double *S, int NP, int *bad_col, double *bad_val) {
+template <typename T>
+__device__ inline void tri_potrf_lower(T *S, int NP, int *bad_col, double *bad_val) {
   __shared__ int s_bad;
-  __shared__ double s_rd[SUB];
-  __shared__ double s_col[2 * SUB];
+  __shared__ T s_rd[SUB];
+  __shared__ T s_col[2 * SUB];
   if (threadIdx.x == 0) s_bad = -1;
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int jb = 0; jb < NP; jb += SUB) {
     if (warp == 0) {
-      double r[SUB];
+      T r[SUB];
 #pragma unroll
-      for (int j = 0; j < SUB; ++j) r[j] = (j <= lane) ? S[(jb + lane) * LDS + jb + j] : 0.0;
+      for (int j = 0; j < SUB; ++j) r[j] = (j <= lane) ? S[(jb + lane) * LDS + jb + j] : T(0);
       double unused;
       warp_potrf32<false>(r, lane, &unused, s_col);
-      double dg = r[0];
+      T dg = r[0];
 #pragma unroll
       for (int j = 1; j < SUB; ++j) dg = (j == lane) ? r[j] : dg;
       if (__ballot_sync(0xffffffffu, isnan(dg)) != 0u) {
         // a pivot failed: redo the sub-block with the stop at the first NaN pivot
 #pragma unroll
-        for (int j = 0; j < SUB; ++j) r[j] = (j <= lane) ? S[(jb + lane) * LDS + jb + j] : 0.0;
+        for (int j = 0; j < SUB; ++j) r[j] = (j <= lane) ? S[(jb + lane) * LDS + jb + j] : T(0);
         double badv = 0.0;
         const int bad = warp_potrf32<true>(r, lane, &badv, s_col);
         if (lane == 0) {
@@ -190,7 +198,7 @@ __device__ inline void tri_potrf_lower(double *S, int NP, int *bad_col, double *
           *bad_val = badv;
         }
       }
-      s_rd[lane] = 1.0 / dg;
+      s_rd[lane] = T(1) / dg;
 #pragma unroll
       for (int j = 0; j < SUB; ++j)
         if (j <= lane) S[(jb + lane) * LDS + jb + j] = r[j];
@@ -199,8 +207,8 @@ __device__ inline void tri_potrf_lower(double *S, int NP, int *bad_col, double *
     if (s_bad >= 0) break;
     // (2) L(i, jb:jb+32) = A(i, jb:jb+32) * L_dd^-T for rows i below the sub-block
     for (int i = jb + SUB + threadIdx.x; i < NP; i += blockDim.x) {
-      double v[SUB];
-      double *row = S + i * LDS + jb;
+      T v[SUB];
+      T *row = S + i * LDS + jb;
 #pragma unroll
       for (int k = 0; k < SUB; ++k) v[k] = row[k];
 #pragma unroll
@@ -224,18 +232,19 @@ __device__ inline void tri_potrf_lower(double *S, int NP, int *bad_col, double *
 // C(32x32, in W at ldc) = sum over `nk` 32-blocks of P_q(32x32) * Q_q(32x32), where P_q is
 // S[prow + r, pcol + 32q + k] and Q_q is S or W data given by pointers; all threads,
 // 4 x 4 register micro-tiles (64 per 32 x 32 product).
-__device__ __forceinline__ void tri_small_gemm(double *C, int ldc, const double *P, int ldp,
-                                               const double *Q, int ldq, int nk, double sign,
-                                               int tile, int ntile_total) {
+template <typename T>
+__device__ __forceinline__ void tri_small_gemm(T *C, int ldc, const T *P, int ldp, const T *Q,
+                                               int ldq, int nk, T sign, int tile,
+                                               int ntile_total) {
   (void)ntile_total;
   const int ti = tile / 8, tj = tile % 8;
-  double acc[4][4];
+  T acc[4][4];
 #pragma unroll
   for (int x = 0; x < 4; ++x)
 #pragma unroll
-    for (int y = 0; y < 4; ++y) acc[x][y] = 0.0;
+    for (int y = 0; y < 4; ++y) acc[x][y] = T(0);
   for (int k = 0; k < nk; ++k) {
-    double a[4], b[4];
+    T a[4], b[4];
 #pragma unroll
     for (int x = 0; x < 4; ++x) {
       a[x] = P[(4 * ti + x) * ldp + k];
@@ -253,10 +262,11 @@ __device__ __forceinline__ void tri_small_gemm(double *C, int ldc, const double 
 }
 
 // In-place inverse of the lower-triangular S (order NP, multiple of 32, non-singular
-// diagonal).  W: scratch of 4 * 32 * 33 doubles.  Must be called by all threads.
+// diagonal).  W: scratch of 4 * 32 * 33 elements.  Must be called by all threads.
 //   X_ii = L_ii^-1 (one warp per diagonal sub-block, one lane per column, registers)
 //   X_ij = -X_ii * sum_{k=j}^{i-1} L_ik X_kj   for i > j, block row by block row
-__device__ inline void tri_inverse_lower(double *S, int NP, double *W) {
+template <typename T>
+__device__ inline void tri_inverse_lower(T *S, int NP, T *W) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nsub = NP / SUB;
   constexpr int LW = SUB + 1;
@@ -265,20 +275,20 @@ __device__ inline void tri_inverse_lower(double *S, int NP, double *W) {
     const int b = warp * SUB;
     // reciprocal pivots, lane i holds 1 / L_ii; the substitution multiplies by them so
     // the serial chain per row is FMAs only
-    const double rdi = 1.0 / S[(b + lane) * LDS + b + lane];
-    double x[SUB];
+    const T rdi = T(1) / S[(b + lane) * LDS + b + lane];
+    T x[SUB];
 #pragma unroll
     for (int i = 0; i < SUB; ++i) {
-      const double *lrow = S + (b + i) * LDS + b;
-      double s0 = (i == lane) ? 1.0 : 0.0, s1 = 0.0;
+      const T *lrow = S + (b + i) * LDS + b;
+      T s0 = (i == lane) ? T(1) : T(0), s1 = T(0);
 #pragma unroll
       for (int m = 0; m + 1 < i; m += 2) {
         s0 = fma(-lrow[m], x[m], s0);
         s1 = fma(-lrow[m + 1], x[m + 1], s1);
       }
       if (i & 1) s0 = fma(-lrow[i - 1], x[i - 1], s0);
-      const double rd = __shfl_sync(0xffffffffu, rdi, i);
-      x[i] = (i < lane) ? 0.0 : (s0 + s1) * rd;
+      const T rd = __shfl_sync(0xffffffffu, rdi, i);
+      x[i] = (i < lane) ? T(0) : (s0 + s1) * rd;
     }
     __syncwarp();
 #pragma unroll
@@ -291,14 +301,14 @@ __device__ inline void tri_inverse_lower(double *S, int NP, double *W) {
     for (int e = threadIdx.x; e < bi * 64; e += blockDim.x) {
       const int bj = e / 64, tile = e % 64;
       tri_small_gemm(W + bj * SUB * LW, LW, S + (bi * SUB) * LDS + bj * SUB, LDS,
-                     S + (bj * SUB) * LDS + bj * SUB, LDS, (bi - bj) * SUB, 1.0, tile, 64);
+                     S + (bj * SUB) * LDS + bj * SUB, LDS, (bi - bj) * SUB, T(1), tile, 64);
     }
     __syncthreads();
     // X(bi,bj) = -X(bi,bi) * T_bj
     for (int e = threadIdx.x; e < bi * 64; e += blockDim.x) {
       const int bj = e / 64, tile = e % 64;
       tri_small_gemm(S + (bi * SUB) * LDS + bj * SUB, LDS, S + (bi * SUB) * LDS + bi * SUB, LDS,
-                     W + bj * SUB * LW, LW, SUB, -1.0, tile, 64);
+                     W + bj * SUB * LW, LW, SUB, T(-1), tile, 64);
     }
     __syncthreads();
   }
