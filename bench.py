@@ -258,7 +258,9 @@ def mixed_leg(mo, n, nrhs, kappas, precs, dev, reps=2):
             row[name] = {"ms": min(tm), "speedup_vs_fp64": min(tf) / min(tm),
                          "iters": info.iters, "gmres_iters": info.gmres_iters,
                          "method": "gmres" if info.method == mo.IR_GMRES else "classic",
-                         "fallback": info.fallback, "converged": info.converged,
+                         "fallback": info.fallback, "abandoned": info.abandoned,
+                         "converged": info.converged, "prec_used": info.prec,
+                         "berr_history": info.history,
                          "shift": info.shift, "berr": info.berr, "berr_check": berr(X),
                          "ferr_vs_fp64": float((X - Xf).norm() / Xf.norm()),
                          "traced_ms_by_class": by_class}

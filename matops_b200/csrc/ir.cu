@@ -1,10 +1,12 @@
 // Mixed-precision Cholesky solve with FP64 iterative refinement (mo_dsposv_ir).
 //
-// The factor L comes from lpchol.cu (split-product GEMMs on an FP32 copy of A, FP64
-// diagonal blocks).  Everything that decides the accuracy runs in FP64 on the device:
-//   residual   r = b - A x      sym_apply_kernel reads only the stored triangle of A
-//   correction d = M^-1 r       M = L L^T: two triangular solves that read the FP32 L and
-//                               compute in FP64 (trsm_few.cu)
+// The factor L comes from lpchol.cu (split-product GEMMs on an FP32 copy of A).  Everything
+// that decides the accuracy runs in FP64 on the device:
+//   residual   r = b - A x      sym_apply_kernel reads only the stored triangle of A (or the
+//                               GEMM engine on a full FP64 copy, for many right-hand sides)
+//   correction d = M^-1 r       M = L L^T: two triangular solves with the FP32 L in FP64
+//                               arithmetic, in 1024-row block steps (lpsolve.cu) from order
+//                               kBlockSolveMinN, else 64-row steps (trsm_few.cu)
 //              or d = GMRES(A, r) left-preconditioned by M^-1, restarted after
 //                               kGmresMax iterations, classical Gram-Schmidt applied twice
 //   update     x += d
@@ -395,7 +397,13 @@ struct Solver {
   const int *skip = nullptr;  // set while GMRES iterations run: their convergence word
   int nblk_dot, pstride;
   double *S = nullptr;    // full symmetric copy of A (many right-hand sides only)
+  LpSolve ls;             // block solves with the factor (orders >= kBlockSolveMinN)
+  bool blocked = false;
 };
+
+// from this order on the refinement solves take n / 1024 block steps (lpsolve.cu) instead
+// of the few-RHS kernel's n / 64 dependent steps
+constexpr int kBlockSolveMinN = 2048;
 
 // products with A through the FP64 GEMM engine on the symmetric copy pay off above this
 // many right-hand sides (one 128-column tile pass against a 16-column pass per group)
@@ -465,8 +473,10 @@ int colmax(Solver &s, const double *V, int64_t ld, int n, int nr, double *out) {
 }
 
 // D = M^-1 D in place (D: packed n x nr): L^-1 then L^-T with the FP32 factor (FP64
-// arithmetic), right-hand sides in groups of 64
+// arithmetic): block solves for large orders, else the few-RHS kernel with right-hand
+// sides in groups of 64
 int precond(Solver &s, double *D) {
+  if (s.blocked) return lp_solve_apply(s.ctx, s.ls, D, s.nr, s.skip);
   for (int c0 = 0; c0 < s.nr; c0 += 64) {
     const View B{D + (int64_t)c0 * s.n, s.n, std::min(64, s.nr - c0), s.n};
     int rc = trsm_few_f32(s.ctx, B, s.f.W, s.f.ldw, s.n, false, s.f.inv, s.flags, s.skip);
@@ -520,7 +530,10 @@ int gmres_slots(mo_ctx *ctx) {
   return MO_OK;
 }
 
-int gmres(Solver &s, double tau, int *its) {
+// budget_s > 0: once the iterations completed so far took longer than budget_s seconds
+// (host clock), the next one enqueued is the last
+int gmres(Solver &s, double tau, int *its, double budget_s) {
+  const auto t0 = std::chrono::steady_clock::now();
   const int n = s.n, nr = s.nr;
   const int64_t vs = (int64_t)n * nr;
   mo_ctx *ctx = s.ctx;
@@ -536,12 +549,15 @@ int gmres(Solver &s, double tau, int *its) {
   int *hd = ctx->h_gmres;  // hd[2 j], hd[2 j + 1]: done word and count after iteration j
   s.skip = s.gs.done;
   int m = 0;
+  bool final = false;
   for (int j = 0; j < kGmresMax; ++j) {
     // the convergence test of iteration j - kGmresLag, once the device has passed it
     if (j - kGmresLag >= 0) {
       const int q = j - kGmresLag;
       MO_CUDA_TRY(cudaEventSynchronize(ctx->gmres_ev[q]));
       if (hd[2 * q]) break;
+      final = budget_s > 0.0 &&
+              std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > budget_s;
     }
     double *vj = s.V + j * vs, *w = s.V + (j + 1) * vs;
     if ((rc = sym_apply(s, vj, n, nullptr, w, 1.0, false, nr))) return rc;  // w = A v_j
@@ -554,10 +570,11 @@ int gmres(Solver &s, double tau, int *its) {
     if ((rc = dots(s, w, 1, w, s.scal, true))) return rc;  // |w|_2
     vscale_kernel<<<vgrid(n, nr), 256, 0, st>>>(w, w, s.scal, n, nr, s.skip);
     gmres_givens_kernel<<<1, 256, 0, st>>>(s.gs, s.h, s.h2, s.scal, j, nr, tau,
-                                           j == kGmresMax - 1);
+                                           j == kGmresMax - 1 || final);
     MO_CUDA_TRY(cudaGetLastError());
     MO_CUDA_TRY(cudaMemcpyAsync(hd + 2 * j, s.gs.done, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
     MO_CUDA_TRY(cudaEventRecord(ctx->gmres_ev[j], st));
+    if (final) break;
   }
   s.skip = nullptr;
   MO_CUDA_TRY(cudaMemcpyAsync(hd, s.gs.done, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -576,11 +593,12 @@ int gmres(Solver &s, double tau, int *its) {
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 // workspace bytes for order n, nr right-hand sides
-size_t ir_bytes(int n, int nr, int prec, bool gmres_possible) {
+size_t ir_bytes(int n, int nr, int prec, bool gmres_possible, int sms) {
   const size_t vec = align256((size_t)n * nr * 8);
   const int nblk_dot = (n + DOT_ROWS - 1) / DOT_ROWS;
   size_t b = align256(lp_chol_bytes(n, prec)) + 4 * vec;
   if (nr >= kGemmResidualMinRhs) b += align256((size_t)n * n * 8);
+  if (n >= kBlockSolveMinN) b += align256(lp_solve_bytes(n, nr, sms));
   if (gmres_possible) b += (kGmresMax + 1) * vec;
   b += 2 * align256((size_t)(kGmresMax + 1) * nr * 8) + align256((size_t)nr * 8);
   if (gmres_possible)
@@ -666,7 +684,7 @@ int dsposv(mo_ctx *ctx, const View &X, const View &A, const View &B, bool upper,
   // BF16x3 under MO_IR_AUTO may move to the TF32x3 factor (see below): room for either
   const bool may_switch = prec == kLpBf16x3 && method == MO_IR_AUTO;
   const int ws_prec = may_switch ? kLpTf32x3 : prec;
-  const size_t need = ir_bytes(n, nr, ws_prec, gm);
+  const size_t need = ir_bytes(n, nr, ws_prec, gm, ctx->sms);
   if (need > ctx->ws_ir_bytes) {
     MO_CUDA_TRY(cudaStreamSynchronize(st));
     if (ctx->ws_ir) cudaFree(ctx->ws_ir);
@@ -707,6 +725,10 @@ int dsposv(mo_ctx *ctx, const View &X, const View &A, const View &B, bool upper,
   s.partial = (double *)take((size_t)s.nblk_dot * s.pstride * 8);
   s.norms = (double *)take((size_t)(3 * nr + 1) * 8);
   s.flags = (int *)take((size_t)(128 * ((n + 63) / 64) + 64) * 4);
+  if (n >= kBlockSolveMinN) {
+    lp_solve_setup(n, nr, ctx->sms, take(lp_solve_bytes(n, nr, ctx->sms)), s.ls);
+    s.blocked = true;
+  }
   int rc;
   if (nr >= kGemmResidualMinRhs) {
     s.S = (double *)take((size_t)n * n * 8);
@@ -759,6 +781,7 @@ int dsposv(mo_ctx *ctx, const View &X, const View &A, const View &B, bool upper,
     info.shifts += 1;
   }
   info.shift = factored ? shift : 0.0;
+  if (factored && s.blocked && (rc = lp_solve_prepare(ctx, s.f, s.ls))) return rc;
   std::vector<double> nh(3 * nr + 1);
   double prev = INFINITY;
   bool use_gmres = method == MO_IR_GMRES;
@@ -806,7 +829,10 @@ int dsposv(mo_ctx *ctx, const View &X, const View &A, const View &B, bool upper,
       prev = berr;
       if (use_gmres) {
         int its = 0;
-        if ((rc = gmres(s, 1e-10, &its))) return rc;
+        // a GMRES step may take as long as the FP64 path would (then the refinement has at
+        // most doubled the cost of solving in FP64 outright)
+        const double budget = fallback_ok && method == MO_IR_AUTO ? kFp64OverLp * t_fact : 0.0;
+        if ((rc = gmres(s, 1e-10, &its, budget))) return rc;
         info.gmres_iters += its;
         info.method = MO_IR_GMRES;
       } else {
