@@ -86,7 +86,6 @@ __global__ void __launch_bounds__(PANEL_THREADS)
   __shared__ double red_v[PANEL_THREADS / 32];
   __shared__ int red_i[PANEL_THREADS / 32];
   __shared__ int red_q[PANEL_THREADS / 32];
-  __shared__ int s_p, s_wb;
 
   for (int e = threadIdx.x; e < nr * W; e += blockDim.x) {
     const int r = e % nr, c = e / nr;
@@ -95,16 +94,20 @@ __global__ void __launch_bounds__(PANEL_THREADS)
   __syncthreads();
 
   const int kmax = min(m, W);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  // (row, column) work of the update: G consecutive lanes per row
+  int G = 32;
+  while (G > 1 && G * nr > (int)blockDim.x) G >>= 1;
   for (int j = 0; j < kmax; ++j) {
     const int par = j & 1;
-    // (a) local argmax of |column j| over owned positions >= j
+    // (a) local argmax of |column j| over owned positions >= j; every warp then combines
+    // the warps' partials itself (no second barrier)
     double bv = -1.0;
     int bi = INT_MAX;
     for (int r = threadIdx.x; r < nr; r += blockDim.x) {
       const int gi = rbeg + r;
       if (gi < j) continue;
-      const double a = S[r * LDW + j];
-      double v = fabs(a);
+      double v = fabs(S[r * LDW + j]);
       if (isnan(v)) v = -1.0;  // NaN never wins off the diagonal
       if (better(v, gi, bv, bi)) {
         bv = v;
@@ -112,35 +115,37 @@ __global__ void __launch_bounds__(PANEL_THREADS)
       }
     }
     for (int off = 16; off > 0; off >>= 1) {
-      const double ov = __shfl_down_sync(0xffffffffu, bv, off);
-      const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+      const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
       if (better(ov, oi, bv, bi)) {
         bv = ov;
         bi = oi;
       }
     }
-    if ((threadIdx.x & 31) == 0) {
-      red_v[threadIdx.x >> 5] = bv;
-      red_i[threadIdx.x >> 5] = bi;
+    if (lane == 0) {
+      red_v[wid] = bv;
+      red_i[wid] = bi;
     }
     __syncthreads();
+    bv = lane < nw ? red_v[lane] : -1.0;
+    bi = lane < nw ? red_i[lane] : INT_MAX;
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+      if (better(ov, oi, bv, bi)) {
+        bv = ov;
+        bi = oi;
+      }
+    }
+    // (b) publish the candidate and its row and, if owned here, row j
     if (threadIdx.x == 0) {
-      for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
-        if (better(red_v[w], red_i[w], bv, bi)) {
-          bv = red_v[w];
-          bi = red_i[w];
-        }
       sc.cand_val[par * nblk + b] = bv;
       sc.cand_idx[par * nblk + b] = bi;
-      s_p = bi;
     }
-    __syncthreads();
-    // (b) publish the candidate row and, if owned here, row j
     {
-      const int ci = s_p;
       double *crow = sc.cand_row + ((size_t)par * nblk + b) * W;
-      if (ci != INT_MAX)
-        for (int c = threadIdx.x; c < W; c += blockDim.x) crow[c] = S[(ci - rbeg) * LDW + c];
+      if (bi != INT_MAX)
+        for (int c = threadIdx.x; c < W; c += blockDim.x) crow[c] = S[(bi - rbeg) * LDW + c];
       if (j >= rbeg && j < rend) {
         for (int c = threadIdx.x; c < W; c += blockDim.x) sc.rowj[par * W + c] = S[(j - rbeg) * LDW + c];
         if (threadIdx.x == 0) sc.diag_nan[par] = isnan(S[(j - rbeg) * LDW + j]) ? 1 : 0;
@@ -150,52 +155,57 @@ __global__ void __launch_bounds__(PANEL_THREADS)
     // (c) every CTA selects the pivot: largest value, lowest index; NaN on the diagonal wins.
     // The candidates are read in parallel (one per thread) and reduced like the local
     // argmax, so the selection costs one L2 round trip, not one per CTA.
+    int p, wb;
     {
       double v = -2.0;
-      int p = INT_MAX, wq = INT_MAX;
+      int pi = INT_MAX, wq = INT_MAX;
       for (int q = threadIdx.x; q < nblk; q += blockDim.x) {
         const double cv = __ldcg(sc.cand_val + par * nblk + q);
         const int ci = __ldcg(sc.cand_idx + par * nblk + q);
-        if (ci != INT_MAX && better(cv, ci, v, p)) {
+        if (ci != INT_MAX && better(cv, ci, v, pi)) {
           v = cv;
-          p = ci;
+          pi = ci;
           wq = q;
         }
       }
       for (int off = 16; off > 0; off >>= 1) {
-        const double ov = __shfl_down_sync(0xffffffffu, v, off);
-        const int oi = __shfl_down_sync(0xffffffffu, p, off);
-        const int oq = __shfl_down_sync(0xffffffffu, wq, off);
-        if (better(ov, oi, v, p)) {
+        const double ov = __shfl_xor_sync(0xffffffffu, v, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, pi, off);
+        const int oq = __shfl_xor_sync(0xffffffffu, wq, off);
+        if (better(ov, oi, v, pi)) {
           v = ov;
-          p = oi;
+          pi = oi;
           wq = oq;
         }
       }
-      if ((threadIdx.x & 31) == 0) {
-        red_v[threadIdx.x >> 5] = v;
-        red_i[threadIdx.x >> 5] = p;
-        red_q[threadIdx.x >> 5] = wq;
+      if (lane == 0) {
+        red_v[wid] = v;
+        red_i[wid] = pi;
+        red_q[wid] = wq;
       }
       __syncthreads();
-      if (threadIdx.x == 0) {
-        for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
-          if (better(red_v[w], red_i[w], v, p)) {
-            v = red_v[w];
-            p = red_i[w];
-            wq = red_q[w];
-          }
-        int wb = p == INT_MAX ? -1 : wq;
-        if (__ldcg(sc.diag_nan + par)) {
-          p = j;
-          wb = -1;
+      v = lane < nw ? red_v[lane] : -2.0;
+      pi = lane < nw ? red_i[lane] : INT_MAX;
+      wq = lane < nw ? red_q[lane] : INT_MAX;
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, v, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, pi, off);
+        const int oq = __shfl_xor_sync(0xffffffffu, wq, off);
+        if (better(ov, oi, v, pi)) {
+          v = ov;
+          pi = oi;
+          wq = oq;
         }
-        s_p = p;
-        s_wb = wb;
       }
-      __syncthreads();
+      p = pi;
+      wb = pi == INT_MAX ? -1 : wq;
+      if (__ldcg(sc.diag_nan + par)) {
+        p = j;
+        wb = -1;
+      }
+      if (p == INT_MAX) p = j;  // no comparable candidate: keep the row
     }
-    const int p = s_p, wb = s_wb;
+    // (d) the pivot row (U row) and the old row j, into shared memory
     for (int c = threadIdx.x; c < W; c += blockDim.x) {
       const double oj = __ldcg(sc.rowj + par * W + c);
       s_oldj[c] = oj;
@@ -203,27 +213,28 @@ __global__ void __launch_bounds__(PANEL_THREADS)
     }
     if (b == 0 && threadIdx.x == 0) piv[j] = row0 + p;
     __syncthreads();
-    // (d) interchange rows j and p (pivot.go:27-35 on the panel columns)
-    if (p != j) {
-      if (j >= rbeg && j < rend)
-        for (int c = threadIdx.x; c < W; c += blockDim.x) S[(j - rbeg) * LDW + c] = s_prow[c];
-      if (p >= rbeg && p < rend)
-        for (int c = threadIdx.x; c < W; c += blockDim.x) S[(p - rbeg) * LDW + c] = s_oldj[c];
-    }
-    __syncthreads();
-    // (e) l = a_ij / u_jj (true division, mvec.go:422 InvScale), then the rank-1 update of
-    // the owned rows below j, spread over (row, column) pairs so that every thread works
+    // (e) interchange rows j and p (pivot.go:27-35 on the panel columns), l = a_ij / u_jj
+    // (true division, mvec.go:422 InvScale) and the rank-1 update of the owned rows below j,
+    // in one pass: row j takes the pivot row; the row at p is read from the old row j
+    if (p != j && j >= rbeg && j < rend)
+      for (int c = threadIdx.x; c < W; c += blockDim.x) S[(j - rbeg) * LDW + c] = s_prow[c];
     const double ujj = s_prow[j];
     const int r0 = max(0, j + 1 - rbeg);  // first owned row below j
-    for (int r = r0 + threadIdx.x; r < nr; r += blockDim.x) S[r * LDW + j] /= ujj;
-    __syncthreads();
-    const int wr = W - j - 1;
-    if (wr > 0)
-      for (int e = threadIdx.x; e < (nr - r0) * wr; e += blockDim.x) {
-        const int r = r0 + e / wr, c = j + 1 + e % wr;
-        double *row = S + r * LDW;
-        row[c] = fma(-row[j], s_prow[c], row[c]);
-      }
+    const int grp = threadIdx.x / G, gl = threadIdx.x % G;
+    // the lanes of this thread's group (G divides 32; every lane of a group runs the same
+    // iterations)
+    const unsigned gmask = G == 32 ? 0xffffffffu : ((1u << G) - 1u) << (lane & ~(G - 1));
+    for (int r = r0 + grp; r < nr; r += blockDim.x / G) {
+      double *row = S + r * LDW;
+      const bool swapped = p != j && rbeg + r == p;
+      const double *src = swapped ? s_oldj : row;
+      const double l = src[j] / ujj;
+      __syncwarp(gmask);  // the group has read src[j] before it is overwritten
+      if (swapped)
+        for (int c = gl; c < j; c += G) row[c] = src[c];
+      if (gl == 0) row[j] = l;
+      for (int c = j + 1 + gl; c < W; c += G) row[c] = fma(-l, s_prow[c], src[c]);
+    }
     __syncthreads();
   }
   for (int e = threadIdx.x; e < nr * W; e += blockDim.x) {
@@ -313,6 +324,62 @@ __global__ void __launch_bounds__(32) swap_map_kernel(const int64_t *piv, int ns
     src[i] = lab[i];
   }
   if (lane == 0) *count = total;
+}
+
+// swap_map_kernel for panels whose rows [r0, rows) fit a shared-memory table (label per
+// position, touched flag): the pivots are read in parallel, one thread applies the swaps
+// to the table in order (a few shared-memory operations each, no warp-wide search), and
+// the moves are written in the same form and order as swap_map_kernel's.
+constexpr int kSwapTableMax = 32768;
+__global__ void __launch_bounds__(256) swap_map_table_kernel(const int64_t *piv, int ns, int64_t r0,
+                                                             int rows, int *dst, int *src,
+                                                             int *count, int *status) {
+  extern __shared__ int tb[];
+  const int span = rows - (int)r0;
+  int *lab = tb;                                             // [span]
+  int *ext = lab + span;                                     // [MAX_PANEL_W]
+  int *pv = ext + MAX_PANEL_W;                               // [MAX_PANEL_W]
+  unsigned char *touched = reinterpret_cast<unsigned char *>(pv + MAX_PANEL_W);  // [span]
+  __shared__ int next;
+  for (int i = threadIdx.x; i < span; i += blockDim.x) {
+    lab[i] = (int)r0 + i;
+    touched[i] = 0;
+  }
+  for (int i = threadIdx.x; i < ns; i += blockDim.x) {
+    const int64_t p = piv[i];
+    // -1: skipped (pivot.go:57, entries <= 0, or no exchange); -2: out of range
+    pv[i] = (p <= 0 || p == r0 + i) ? -1 : ((p >= rows || p < r0 || r0 + i >= rows) ? -2 : (int)(p - r0));
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ne = 0;
+    bool bad = false;
+    for (int s2 = 0; s2 < ns; ++s2) {
+      const int pi = pv[s2];
+      if (pi == -1) continue;
+      if (pi == -2) {
+        bad = true;
+        continue;
+      }
+      const int t = lab[s2];
+      lab[s2] = lab[pi];
+      lab[pi] = t;
+      if (pi >= ns && !touched[pi]) {
+        touched[pi] = 1;
+        ext[ne++] = pi;
+      }
+    }
+    if (bad) set_status(status, MO_EINVAL);
+    next = ne;
+  }
+  __syncthreads();
+  const int total = ns + next;
+  for (int i = threadIdx.x; i < total; i += blockDim.x) {
+    const int pos = i < ns ? i : ext[i - ns];
+    dst[i] = (int)r0 + pos;
+    src[i] = lab[pos];
+  }
+  if (threadIdx.x == 0) *count = total;
 }
 
 // A[dst[i], c] = A_old[src[i], c] for the moves of swap_map_kernel, columns [0, ncols): a
@@ -500,7 +567,15 @@ int getrf(mo_ctx *ctx, View A, int64_t *piv, int64_t npiv, int ref_nb) {
     if (k > 0 || k + b < n) {
       ProfScope pm;
       prof_begin(ctx, pm, MO_PROF_LASWP);
-      swap_map_kernel<<<1, 32, 0, ctx->stream>>>(piv + k, b, k, m, mv_dst, mv_src, mv_count, status);
+      if (m - k <= kSwapTableMax) {
+        const size_t tsm = (size_t)(m - k) * 5 + 2 * MAX_PANEL_W * sizeof(int) + 16;
+        if ((rc = mo_smem_attr((const void *)swap_map_table_kernel, (int)tsm))) return rc;
+        swap_map_table_kernel<<<1, 256, tsm, ctx->stream>>>(piv + k, b, k, m, mv_dst, mv_src,
+                                                            mv_count, status);
+      } else {
+        swap_map_kernel<<<1, 32, 0, ctx->stream>>>(piv + k, b, k, m, mv_dst, mv_src, mv_count,
+                                                   status);
+      }
       prof_end(ctx, pm, 0.0, 8.0 * b);
       MO_CUDA_TRY(cudaGetLastError());
     }

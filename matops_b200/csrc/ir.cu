@@ -66,7 +66,8 @@ __global__ void __launch_bounds__(256) sym_apply_kernel(SymArgs p) {
   // the tile buffers and, after the last tile, the cross-q reduction share one block
   __shared__ double buf[4 * RR * (RNR + 1)];
   double(*T)[RR + 1] = reinterpret_cast<double(*)[RR + 1]>(buf);
-  double(*Xs)[RNR] = reinterpret_cast<double(*)[RNR]>(buf + RT * (RR + 1));
+  // X tile rows padded to RNR + 1 doubles: the stores walk down a column (one row per lane)
+  double(*Xs)[RNR + 1] = reinterpret_cast<double(*)[RNR + 1]>(buf + RT * (RR + 1));
   double(*red)[RR][RNR + 1] = reinterpret_cast<double(*)[RR][RNR + 1]>(buf);
   const int r = threadIdx.x & 63, q = threadIdx.x >> 6;
   const int r0 = blockIdx.x * RR;
