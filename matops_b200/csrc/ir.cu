@@ -31,20 +31,26 @@ int trsm_few_f32(mo_ctx *ctx, View B, const float *L, int64_t ldl, int N, bool t
 
 namespace {
 
-constexpr int RR = 64;    // rows of A per CTA in sym_apply
+constexpr int RR = 32;    // rows of A per CTA in sym_apply
 constexpr int RT = 32;    // tile depth
+constexpr int RQ = 256 / RR;  // depth groups per tile (threads per row)
+constexpr int RD = RT / RQ;   // depth indices per group and tile
+constexpr int RU = RT * RR / 256;  // tile elements per thread
 constexpr int RNR = 16;   // right-hand sides per launch
+static_assert(RR == 32 && RNR == 16 && RQ == 8, "sym_apply_kernel's thread layout");
 constexpr int kGmresMax = 60;
 constexpr int DOT_ROWS = 1024;
 
 // Y = Bv + sa * op|A| X for symmetric A stored as its lower (UP == false) or upper
-// triangle; ABS uses |A|.  CTA b owns rows r0 = 64 b .. r0 + 63.  It reads its row strip
-// L(r0.., 0..r0+63) (masked to j <= r) and its column strip L(r0.., r0..)^T (masked to
-// i > r), so every stored element is read twice over the grid and never mirrored in
+// triangle; ABS uses |A|.  CTA b owns rows r0 = RR b .. r0 + RR - 1.  It reads its row
+// strip L(r0.., 0..r0+RR) (masked to j <= r) and its column strip L(r0.., r0..)^T (masked
+// to i > r), so every stored element is read twice over the grid and never mirrored in
 // memory.  Tiles are 32 deep, staged in shared memory from loads that are coalesced in
 // either storage; the next tile is fetched into registers while the current one is used.
-// Thread (r, q) = (tid % 64, tid / 64) accumulates 8 of each tile's 32 depth indices for
-// all right-hand sides; the four partial sums per row are added at the end in fixed order.
+// Warp q accumulates RD of each tile's 32 depth indices, each thread a 4 x 4 block (4 rows,
+// 4 right-hand sides) in registers; the RQ partial sums per row are added at the end in
+// fixed order.
+// 32-row strips give n / 32 CTAs (two or more per SM at the orders that matter).
 struct SymArgs {
   const double *A;
   int64_t lda;
@@ -64,25 +70,31 @@ template <bool UP, bool ABS>
 __global__ void __launch_bounds__(256) sym_apply_kernel(SymArgs p) {
   if (p.skip && *(volatile const int *)p.skip) return;
   // the tile buffers and, after the last tile, the cross-q reduction share one block
-  __shared__ double buf[4 * RR * (RNR + 1)];
-  double(*T)[RR + 1] = reinterpret_cast<double(*)[RR + 1]>(buf);
-  // X tile rows padded to RNR + 1 doubles: the stores walk down a column (one row per lane)
-  double(*Xs)[RNR + 1] = reinterpret_cast<double(*)[RNR + 1]>(buf + RT * (RR + 1));
+  __shared__ __align__(16) double buf[RQ * RR * (RNR + 1) > RT * (RR + 2) + RT * (RNR + 2)
+                                          ? RQ * RR * (RNR + 1)
+                                          : RT * (RR + 2) + RT * (RNR + 2)];
+  // even row strides: the products read their operands as 16-byte pairs (the tile stores
+  // that walk down a column then meet 2-way bank conflicts, a few per thread and tile)
+  double(*T)[RR + 2] = reinterpret_cast<double(*)[RR + 2]>(buf);
+  double(*Xs)[RNR + 2] = reinterpret_cast<double(*)[RNR + 2]>(buf + RT * (RR + 2));
   double(*red)[RR][RNR + 1] = reinterpret_cast<double(*)[RR][RNR + 1]>(buf);
-  const int r = threadIdx.x & 63, q = threadIdx.x >> 6;
+  // thread = (depth group q = warp, 4 rows 4 rq.., 4 right-hand sides 4 cq..)
+  const int q = threadIdx.x >> 5, rq = threadIdx.x & 7, cq = (threadIdx.x >> 3) & 3;
   const int r0 = blockIdx.x * RR;
   const int n = p.n;
   const int t1 = (min(r0 + RR, n) + RT - 1) / RT;
   const int ntile = t1 + (n - r0 + RT - 1) / RT;
-  double acc[RNR];
+  double acc[4][4];
 #pragma unroll
-  for (int c = 0; c < RNR; ++c) acc[c] = 0.0;
-  double av[8], xv[2];
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[i][c] = 0.0;
+  double av[RU], xv[2];
   auto fetch = [&](int t) {
     const bool ph1 = t < t1;
     const int base = ph1 ? t * RT : r0 + (t - t1) * RT;
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
+    for (int u = 0; u < RU; ++u) {
       const int e = threadIdx.x + u * 256;
       int a, b;
       bool use;
@@ -113,7 +125,7 @@ __global__ void __launch_bounds__(256) sym_apply_kernel(SymArgs p) {
   auto stash = [&](int t) {
     const bool ph1 = t < t1;
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
+    for (int u = 0; u < RU; ++u) {
       const int e = threadIdx.x + u * 256;
       int a, b;
       if (ph1) {
@@ -136,21 +148,31 @@ __global__ void __launch_bounds__(256) sym_apply_kernel(SymArgs p) {
     __syncthreads();
     if (t + 1 < ntile) fetch(t + 1);
 #pragma unroll
-    for (int jj = 0; jj < 8; ++jj) {
-      const double a = T[8 * q + jj][r];
+    for (int jj = 0; jj < RD; ++jj) {
+      const double2 a01 = *reinterpret_cast<const double2 *>(&T[RD * q + jj][4 * rq]);
+      const double2 a23 = *reinterpret_cast<const double2 *>(&T[RD * q + jj][4 * rq + 2]);
+      const double2 x01 = *reinterpret_cast<const double2 *>(&Xs[RD * q + jj][4 * cq]);
+      const double2 x23 = *reinterpret_cast<const double2 *>(&Xs[RD * q + jj][4 * cq + 2]);
+      const double a[4] = {a01.x, a01.y, a23.x, a23.y}, x[4] = {x01.x, x01.y, x23.x, x23.y};
 #pragma unroll
-      for (int c = 0; c < RNR; ++c) acc[c] = fma(a, Xs[8 * q + jj][c], acc[c]);
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[i][c] = fma(a[i], x[c], acc[i][c]);
     }
   }
   __syncthreads();
 #pragma unroll
-  for (int c = 0; c < RNR; ++c) red[q][r][c] = acc[c];
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) red[q][4 * rq + i][4 * cq + c] = acc[i][c];
   __syncthreads();
   for (int e = threadIdx.x; e < RR * RNR; e += 256) {
     const int rr = e % RR, c = e / RR;
     const int row = r0 + rr;
     if (row < n && c < p.nr) {
-      const double s = ((red[0][rr][c] + red[1][rr][c]) + red[2][rr][c]) + red[3][rr][c];
+      double s = red[0][rr][c];
+#pragma unroll
+      for (int qq = 1; qq < RQ; ++qq) s += red[qq][rr][c];
       const double b = p.Bv ? p.Bv[row + (int64_t)c * p.ldb] : 0.0;
       p.Y[row + (int64_t)c * p.ldy] = fma(p.sa, s, b);
     }

@@ -120,42 +120,55 @@ __device__ __forceinline__ void tri_syrk_update(T *S, int NP, int r0, int kb) {
 }
 
 // Cholesky of a 32 x 32 lower block held by one warp, lane i holding row i in r[0..31]
-// (column-by-column; the reference divides by the square root, calgo/dvec_util.c:230-246,
-// here the column is multiplied by the reciprocal square root, equal to rounding).  The
-// rank-1 updates run on every lane without a lane test: a lane only modifies entries
-// right of its diagonal, which are never read, and this keeps the unrolled body free of
-// divergent branches (measured 4.4x faster than guarding each update with lane >= j).
-// With `checked`, the column loop stops at the first NaN pivot and returns its index.
-// `col` is 2 x 32 elements of shared memory (two alternating multiplier columns).
+// (the reference divides by the square root, calgo/dvec_util.c:230-246; here columns are
+// multiplied by reciprocal square roots, equal to rounding).  Two columns per step: every
+// lane factors the 2 x 2 diagonal block [a .; b c] itself (l11 = sqrt(a), l21 = b / l11,
+// l22 = sqrt(c - l21^2), from three shuffles), forms its row's two multipliers, and the
+// pair goes to the other lanes through shared memory, so the dependency chain has one
+// shuffle, store, __syncwarp and load per two columns.  The arithmetic is the
+// column-by-column algorithm's, in the same order (the second column is updated by the
+// first before it is scaled, and each trailing entry takes the first column's product
+// before the second's).  The rank-2 updates run on every lane without a lane test: a lane
+// only modifies entries right of its diagonal, which are never read, and this keeps the
+// unrolled body free of divergent branches.  With `checked`, the loop stops at the first
+// NaN pivot and returns its column.  `col` is 4 x 32 elements of shared memory (two
+// alternating pairs of multiplier columns).
 template <bool checked, typename T>
 __device__ __forceinline__ int warp_potrf32(T (&r)[SUB], int lane, double *badv, T *col) {
   int bad = -1;
 #pragma unroll
-  for (int k = 0; k < SUB; ++k) {
-    const T akk = __shfl_sync(0xffffffffu, r[k], k);
-    // the column is scaled by rsqrt(akk) (one reciprocal square root on the dependency
-    // chain instead of a square root followed by a division); the stored pivot is
-    // sqrt(akk), which nothing on the chain waits for
-    const T rs = tri_rsqrt(akk);
+  for (int k = 0; k < SUB; k += 2) {
+    const T a = __shfl_sync(0xffffffffu, r[k], k);
+    const T b = __shfl_sync(0xffffffffu, r[k], k + 1);
+    const T c = __shfl_sync(0xffffffffu, r[k + 1], k + 1);
+    const T rs1 = tri_rsqrt(a);
     if (checked) {
-      if (isnan(rs)) {  // uniform: every lane sees the same akk
+      if (isnan(rs1)) {  // uniform: every lane sees the same pivot
         bad = k;
-        *badv = akk;
+        *badv = a;
         break;
       }
     }
-    // the multipliers (zero on lanes <= k) go through shared memory: every lane reads the
-    // column with broadcast loads that issue back to back, where a chain of shuffles would
-    // pay each shuffle's latency in turn.  Columns alternate between two buffers, so the
-    // next column's store need not wait for every lane to finish reading this one (the
-    // __syncwarp of column k + 1 orders column k's reads before column k + 2's stores).
-    T *c = col + (k & 1) * SUB;
-    const T lk = lane > k ? r[k] * rs : T(0);
-    c[lane] = lk;
+    const T l21 = b * rs1;
+    const T d = fma(-l21, l21, c);
+    const T rs2 = tri_rsqrt(d);
+    if (checked) {
+      if (isnan(rs2)) {
+        bad = k + 1;
+        *badv = d;
+        break;
+      }
+    }
+    const T x1 = lane > k ? r[k] * rs1 : T(0);
+    const T x2 = lane > k + 1 ? fma(-x1, l21, r[k + 1]) * rs2 : T(0);
+    T *c1 = col + ((k >> 1) & 1) * 2 * SUB, *c2 = c1 + SUB;
+    c1[lane] = x1;
+    c2[lane] = x2;
     __syncwarp();
 #pragma unroll
-    for (int j = k + 1; j < SUB; ++j) r[j] = fma(-lk, c[j], r[j]);
-    r[k] = lane == k ? tri_sqrt(akk) : (lane > k ? lk : r[k]);
+    for (int j = k + 2; j < SUB; ++j) r[j] = fma(-x2, c2[j], fma(-x1, c1[j], r[j]));
+    r[k] = lane == k ? tri_sqrt(a) : (lane > k ? x1 : r[k]);
+    r[k + 1] = lane == k + 1 ? tri_sqrt(d) : (lane > k + 1 ? x2 : r[k + 1]);
   }
   return bad;
 }
@@ -173,7 +186,7 @@ template <typename T>
 __device__ inline void tri_potrf_lower(T *S, int NP, int *bad_col, double *bad_val) {
   __shared__ int s_bad;
   __shared__ T s_rd[SUB];
-  __shared__ T s_col[2 * SUB];
+  __shared__ T s_col[4 * SUB];
   if (threadIdx.x == 0) s_bad = -1;
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
