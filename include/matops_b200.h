@@ -260,7 +260,9 @@ typedef struct mo_ir_info {
   int shifts;       /* low-precision factorizations retried with a diagonal shift      */
   int method;       /* MO_IR_CLASSIC or MO_IR_GMRES: the method of the last step       */
   int abandoned;    /* 1 if MO_IR_AUTO stopped refining because the steps it projected
-                       from the last reduction would cost more than the FP64 path      */
+                       from the last reduction would cost more than the FP64 path, or a
+                       classic step reduced berr less than 3x (a GMRES step is also cut
+                       off once it has run as long as the FP64 path would)             */
   int prec;         /* split format of the factor used: MO_PREC_BF16X3, or MO_PREC_TF32X3
                        also when MO_IR_AUTO moved from a BF16x3 factor that broke down   */
   double berr;      /* max over columns of |b - A x|_inf / (|A|_inf |x|_inf + |b|_inf) */

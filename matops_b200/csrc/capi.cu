@@ -109,6 +109,16 @@ int aux_stream(mo_ctx *ctx, cudaStream_t *out) {
   return MO_OK;
 }
 
+int side_stream(mo_ctx *ctx, cudaStream_t *out) {
+  if (!ctx->side) {
+    MO_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+    MO_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_side_fork, cudaEventDisableTiming));
+    MO_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_side_join, cudaEventDisableTiming));
+  }
+  *out = ctx->side;
+  return MO_OK;
+}
+
 int stream_wait(mo_ctx *ctx, cudaStream_t waiter, cudaStream_t producer, cudaEvent_t ev) {
   (void)ctx;
   MO_CUDA_TRY(cudaEventRecord(ev, producer));
@@ -175,6 +185,12 @@ int mo_ctx_destroy(mo_ctx *ctx) {
   }
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+  if (ctx->side) {
+    cudaStreamSynchronize(ctx->side);
+    cudaStreamDestroy(ctx->side);
+  }
+  if (ctx->ev_side_fork) cudaEventDestroy(ctx->ev_side_fork);
+  if (ctx->ev_side_join) cudaEventDestroy(ctx->ev_side_join);
   delete ctx;
   return MO_OK;
 }

@@ -24,6 +24,9 @@ struct mo_ctx {
   // second, high-priority stream for look-ahead panels, and fork/join events
   cudaStream_t aux = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // a third stream (default priority) for memory-bound work that overlaps a factorization
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_side_fork = nullptr, ev_side_join = nullptr;
   // stream-K scratch of the GEMM engine (allocated with the context)
   double *sk_partial = nullptr;
   int *sk_flags = nullptr;
@@ -117,6 +120,7 @@ struct StreamSwap {
 
 // the context's auxiliary stream (created on first use, highest priority)
 int aux_stream(mo_ctx *ctx, cudaStream_t *out);
+int side_stream(mo_ctx *ctx, cudaStream_t *out);
 // make `waiter` wait for all work enqueued so far on `producer`
 int stream_wait(mo_ctx *ctx, cudaStream_t waiter, cudaStream_t producer, cudaEvent_t ev);
 

@@ -283,15 +283,20 @@ __device__ inline void tri_inverse_lower(T *S, int NP, T *W) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nsub = NP / SUB;
   constexpr int LW = SUB + 1;
-  // (1) diagonal sub-blocks, warps 0..nsub-1: lane c solves L_bb x = e_c
-  if (warp < nsub) {
-    const int b = warp * SUB;
+  // (1) diagonal sub-blocks, each split in 16 x 16 halves: warp w (< 4) inverts the upper
+  //     half of block w and warp w + 4 the lower half, lane c < 16 solving L x = e_c (a
+  //     16-long chain instead of 32); then both warps form the off-diagonal half,
+  //     X21 = -X22 (L21 X11), through the scratch W
+  constexpr int H = SUB / 2;
+  const int blk = warp & 3, half = warp >> 2;
+  if (blk < nsub) {
+    const int b = blk * SUB + half * H;
     // reciprocal pivots, lane i holds 1 / L_ii; the substitution multiplies by them so
     // the serial chain per row is FMAs only
-    const T rdi = T(1) / S[(b + lane) * LDS + b + lane];
-    T x[SUB];
+    const T rdi = lane < H ? T(1) / S[(b + lane) * LDS + b + lane] : T(0);
+    T x[H];
 #pragma unroll
-    for (int i = 0; i < SUB; ++i) {
+    for (int i = 0; i < H; ++i) {
       const T *lrow = S + (b + i) * LDS + b;
       T s0 = (i == lane) ? T(1) : T(0), s1 = T(0);
 #pragma unroll
@@ -304,8 +309,47 @@ __device__ inline void tri_inverse_lower(T *S, int NP, T *W) {
       x[i] = (i < lane) ? T(0) : (s0 + s1) * rd;
     }
     __syncwarp();
+    if (lane < H) {
 #pragma unroll
-    for (int i = 0; i < SUB; ++i) S[(b + i) * LDS + b + lane] = x[i];  // column lane
+      for (int i = 0; i < H; ++i) S[(b + i) * LDS + b + lane] = x[i];  // column lane
+    }
+  }
+  __syncthreads();
+  {
+    // thread t of the block's 64: row r = t / 4, columns 4 (t % 4) .. + 3 of the half block
+    const int t = (warp >> 2) * 32 + lane, r = t >> 2, c0 = (t & 3) * 4;
+    T *Tm = W + blk * H * (H + 1);
+    const int b = blk * SUB;
+    if (blk < nsub) {
+      // T = L21 X11 (X11 lower: k >= column)
+      T acc[4] = {T(0), T(0), T(0), T(0)};
+      const T *l21 = S + (b + H + r) * LDS + b;
+#pragma unroll
+      for (int k = 0; k < H; ++k) {
+        const T lv = l21[k];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (k >= c0 + j) acc[j] = fma(lv, S[(b + k) * LDS + b + c0 + j], acc[j]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) Tm[r * (H + 1) + c0 + j] = acc[j];
+    }
+    __syncthreads();
+    if (blk < nsub) {
+      // X21 = -X22 T (X22 lower: k <= row)
+      T acc[4] = {T(0), T(0), T(0), T(0)};
+      const T *x22 = S + (b + H + r) * LDS + b + H;
+#pragma unroll
+      for (int k = 0; k < H; ++k) {
+        if (k <= r) {
+          const T xv = x22[k];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[j] = fma(xv, Tm[k * (H + 1) + c0 + j], acc[j]);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) S[(b + H + r) * LDS + b + c0 + j] = -acc[j];
+    }
   }
   __syncthreads();
   // (2) off-diagonal blocks, block row by block row

@@ -55,8 +55,9 @@ def test_mixed_solve_kappa(gpu, oracle, rng, prec, kappa):
     X = Xg.cpu().numpy()
     assert info.converged, info
     if info.abandoned:
-        # MO_IR_AUTO projected that GMRES-IR would cost more than the FP64 path (at this small
-        # order the factor is cheap next to the latency of the inner iterations)
+        # MO_IR_AUTO judged that GMRES-IR would cost more than the FP64 path: a classic step
+        # reduced berr less than 3x, or the projected GMRES steps exceed the FP64 cost (at
+        # this small order the factor is cheap next to the latency of the inner iterations)
         assert info.fallback, info
     elif prec == BF16X3 and kappa > 1e9:
         # BF16x3 keeps about 16 bits (u ~ 1.5e-5): its factor breaks down, and MO_IR_AUTO
