@@ -519,13 +519,13 @@ int getrf(mo_ctx *ctx, View A, int64_t *piv, int64_t npiv, int ref_nb) {
   // workspace: panel scratch + L11 inverse
   const size_t sz_val = 2 * nblk * sizeof(double), sz_idx = 2 * nblk * sizeof(int);
   const size_t sz_row = (size_t)2 * nblk * W * sizeof(double), sz_rowj = 2 * W * sizeof(double);
-  const size_t inv_bytes = 128 * 128 * sizeof(double);
+  const size_t inv_bytes = 2 * 128 * 128 * sizeof(double);  // two panels' L11 inverses
   const size_t sz_moves = 2 * (2 * MAX_PANEL_W) * sizeof(int) + 64;
   const size_t total = inv_bytes + sz_val + sz_row + sz_rowj + sz_idx + 64 + 64 + sz_moves;
   char *ws = nullptr;
   int rc = workspace(ctx, total, (void **)&ws);
   if (rc) return rc;
-  double *inv = (double *)ws;
+  double *inv = (double *)ws, *inv_b = inv + 128 * 128;
   PanelScratch sc;
   char *q = ws + inv_bytes;
   sc.cand_val = (double *)q;
@@ -544,9 +544,8 @@ int getrf(mo_ctx *ctx, View A, int64_t *piv, int64_t npiv, int ref_nb) {
   q += 32;
   int *mv_dst = (int *)q, *mv_src = mv_dst + 2 * MAX_PANEL_W, *mv_count = mv_src + 2 * MAX_PANEL_W;
 
-  for (int k = 0; k < mn; k += W) {
-    const int b = min(W, mn - k);
-    // panel A[k:m, k:k+b]
+  // one panel: factor A[k:m, k:k+b], then apply its interchanges left and right of it
+  auto panel = [&](int k, int b) -> int {
     MO_CUDA_TRY(cudaMemsetAsync(sc.barrier, 0, 32, ctx->stream));  // barrier + abort flag
     View Pv = A.sub(k, k, m - k, b);
     const int pm = m - k;
@@ -565,35 +564,76 @@ int getrf(mo_ctx *ctx, View A, int64_t *piv, int64_t npiv, int ref_nb) {
     prof_end(ctx, ps, (double)pm * b * b - (double)b * b * b / 3.0, 16.0 * pm * b);
     // interchanges on the columns left and right of the panel, as one move list
     if (k > 0 || k + b < n) {
-      ProfScope pm;
-      prof_begin(ctx, pm, MO_PROF_LASWP);
+      ProfScope pms;
+      prof_begin(ctx, pms, MO_PROF_LASWP);
       if (m - k <= kSwapTableMax) {
         const size_t tsm = (size_t)(m - k) * 5 + 2 * MAX_PANEL_W * sizeof(int) + 16;
-        if ((rc = mo_smem_attr((const void *)swap_map_table_kernel, (int)tsm))) return rc;
+        int r2 = mo_smem_attr((const void *)swap_map_table_kernel, (int)tsm);
+        if (r2) return r2;
         swap_map_table_kernel<<<1, 256, tsm, ctx->stream>>>(piv + k, b, k, m, mv_dst, mv_src,
                                                             mv_count, status);
       } else {
         swap_map_kernel<<<1, 32, 0, ctx->stream>>>(piv + k, b, k, m, mv_dst, mv_src, mv_count,
                                                    status);
       }
-      prof_end(ctx, pm, 0.0, 8.0 * b);
+      prof_end(ctx, pms, 0.0, 8.0 * b);
       MO_CUDA_TRY(cudaGetLastError());
     }
-    if ((rc = laswp_moves(ctx, A, 0, k, mv_dst, mv_src, mv_count, 2 * b))) return rc;
-    if ((rc = laswp_moves(ctx, A, k + b, n, mv_dst, mv_src, mv_count, 2 * b))) return rc;
-    const int rest_c = n - k - b;
-    if (rest_c > 0) {
-      View L11 = A.sub(k, k, b, b);
-      if ((rc = trtri_blocks(ctx, L11, b, false, true, true, inv))) return rc;
-      View A12 = A.sub(k, k + b, b, rest_c);
-      if ((rc = gemm(ctx, A12, View{inv, b, b, 128}, false, A12, false, 1.0, 0.0))) return rc;
-      const int rest_r = m - k - b;
-      if (rest_r > 0) {
-        if ((rc = gemm(ctx, A.sub(k + b, k + b, rest_r, rest_c), A.sub(k + b, k, rest_r, b), false,
-                       A12, false, -1.0, 1.0)))
+    int r2 = laswp_moves(ctx, A, 0, k, mv_dst, mv_src, mv_count, 2 * b);
+    if (!r2) r2 = laswp_moves(ctx, A, k + b, n, mv_dst, mv_src, mv_count, 2 * b);
+    return r2;
+  };
+  // Panels in pairs: the second panel's columns are brought up to date with the first
+  // (its U12 block and a (m - k2) x b1 x b0 update), the second is factored, and then the
+  // rows of the first two block rows right of the pair become U (two small products and
+  // one b1-row update between them) and the rest of the matrix takes ONE update with
+  // K = b0 + b1: the trailing matrix is read and written once per pair, not per panel.
+  for (int k = 0; k < mn; k += 2 * W) {
+    const int b0 = min(W, mn - k);
+    if ((rc = panel(k, b0))) return rc;
+    const int k2 = k + b0;
+    const int b1 = k2 < mn ? min(W, mn - k2) : 0;
+    const int c_rest = n - k2 - b1;  // columns right of the pair
+    if (n - k2 > 0) {
+      if ((rc = trtri_blocks(ctx, A.sub(k, k, b0, b0), b0, false, true, true, inv))) return rc;
+    }
+    if (b1 == 0) {
+      // single last panel: U12 and the update of what is right of it
+      const int rest_c = n - k2;
+      if (rest_c > 0) {
+        View A12 = A.sub(k, k2, b0, rest_c);
+        if ((rc = gemm(ctx, A12, View{inv, b0, b0, 128}, false, A12, false, 1.0, 0.0))) return rc;
+        const int rest_r = m - k2;
+        if (rest_r > 0 && (rc = gemm(ctx, A.sub(k2, k2, rest_r, rest_c), A.sub(k2, k, rest_r, b0),
+                                     false, A12, false, -1.0, 1.0)))
           return rc;
       }
+      continue;
     }
+    // the second panel's columns: U01 = inv0 A01, A[k2:m, P1] -= L[k2:m, P0] U01
+    {
+      View U01 = A.sub(k, k2, b0, b1);
+      if ((rc = gemm(ctx, U01, View{inv, b0, b0, 128}, false, U01, false, 1.0, 0.0))) return rc;
+      if ((rc = gemm(ctx, A.sub(k2, k2, m - k2, b1), A.sub(k2, k, m - k2, b0), false, U01, false,
+                     -1.0, 1.0)))
+        return rc;
+    }
+    if ((rc = panel(k2, b1))) return rc;
+    if (c_rest <= 0) continue;
+    const int kc = k2 + b1;
+    if ((rc = trtri_blocks(ctx, A.sub(k2, k2, b1, b1), b1, false, true, true, inv_b))) return rc;
+    // rows k..k2 of the columns right of the pair: U0T = inv0 A0T
+    View U0T = A.sub(k, kc, b0, c_rest);
+    if ((rc = gemm(ctx, U0T, View{inv, b0, b0, 128}, false, U0T, false, 1.0, 0.0))) return rc;
+    // rows k2..kc: A1T -= L10 U0T, then U1T = inv1 A1T
+    View U1T = A.sub(k2, kc, b1, c_rest);
+    if ((rc = gemm(ctx, U1T, A.sub(k2, k, b1, b0), false, U0T, false, -1.0, 1.0))) return rc;
+    if ((rc = gemm(ctx, U1T, View{inv_b, b1, b1, 128}, false, U1T, false, 1.0, 0.0))) return rc;
+    // the rest: A[kc:m, kc:n] -= L[kc:m, k:kc] U[k:kc, kc:n]  (K = b0 + b1)
+    const int rest_r = m - kc;
+    if (rest_r > 0 && (rc = gemm(ctx, A.sub(kc, kc, rest_r, c_rest), A.sub(kc, k, rest_r, b0 + b1),
+                                 false, A.sub(k, kc, b0 + b1, c_rest), false, -1.0, 1.0)))
+      return rc;
   }
   // The reference's blocked path (mlen > nb, nb != 0) leaves the pivot entries past
   // min(rows, cols) inside the last block equal to that block's start row (lu.go:216-219).

@@ -77,11 +77,13 @@ int panel(mo_ctx *ctx, View A, bool upper, int k, int b, int *d_info, double *d_
 
 }  // namespace
 
-// Right-looking blocked Cholesky with one step of look-ahead: the panel of step k+1
-// (diagonal factor + TRSM) runs on a second, high-priority stream while the trailing
-// SYRK of step k runs on the caller's stream with a few SMs left free for it.
-//   S0 (caller):  [update next panel column k+1 | record E0] [SYRK rest of step k]
-//   S1 (aux):     wait E0 -> panel(k+1) -> record E1            (S0 waits E1 at k+1)
+// Right-looking blocked Cholesky, two 128-column steps per trailing update (K = 256: the
+// trailing matrix is read and written once per pair), with look-ahead: pair p covers
+// block columns a and b = a + 1.
+//   S1 (aux):  [panel a] [column b -= L_b,a L_b,a^T] [panel b] -> record E1
+//   S0 (main): wait E1 -> [the next pair's two columns, K = 256] -> record E0 -> [the rest
+//              of the trailing matrix, K = 256, leaving a few SMs to S1]
+//   S1 waits E0 before the next pair.  (Upper storage: the same on U = L^T.)
 int potrf(mo_ctx *ctx, View A, bool upper, int *d_info, double *d_bad, double *inv) {
   int rc = set_diag_smem();
   if (rc) return rc;
@@ -90,52 +92,50 @@ int potrf(mo_ctx *ctx, View A, bool upper, int *d_info, double *d_bad, double *i
   cudaStream_t s0 = ctx->stream, s1 = nullptr;
   if ((rc = aux_stream(ctx, &s1))) return rc;
   if ((rc = stream_wait(ctx, s1, s0, ctx->ev_fork))) return rc;
-  const int free_sms = 8;  // SMs the trailing update leaves to the look-ahead panel
-  {
-    StreamSwap sw(ctx, s1);
-    if ((rc = panel(ctx, A, upper, 0, NB, d_info, d_bad, inv, false))) return rc;
-  }
-  for (int k = 0; k < n; k += NB) {
-    const int b = min(NB, n - k);
-    const int rest = n - k - b;
-    if ((rc = stream_wait(ctx, s0, s1, ctx->ev_join))) return rc;  // panel k done
-    if (rest <= 0) break;
-    const int b2 = min(NB, rest);
-    // 1. next panel column: rows k+b.., columns k+b..k+b+b2, one triangle only
-    GemmOpts onext;
-    onext.mode = upper ? kGemmUpper : kGemmLower;
-    onext.stream_k = false;
-    if (!upper) {
-      const View A21 = A.sub(k + b, k, rest, b);
-      rc = gemm_ex(ctx, A.sub(k + b, k + b, rest, b2), A21, false, A.sub(k + b, k, b2, b), true,
-                   -1.0, 1.0, onext);
-    } else {
-      const View A12 = A.sub(k, k + b, b, rest);
-      rc = gemm_ex(ctx, A.sub(k + b, k + b, b2, rest), A.sub(k, k + b, b, b2), true, A12, false,
-                   -1.0, 1.0, onext);
-    }
-    if (rc) return rc;
-    if ((rc = stream_wait(ctx, s1, s0, ctx->ev_fork))) return rc;
-    // 2. panel k+b on the look-ahead stream
+  const int free_sms = 8;  // SMs the trailing update leaves to the look-ahead stream
+  // C (rows r0.., columns c0.., r x c) -= op(P) op(Q) over the panel columns [k0, k0 + K)
+  auto update = [&](int r0, int c0, int r, int c, int k0, int K, int mode, int max_ctas) {
+    GemmOpts o;
+    o.mode = mode;
+    o.stream_k = false;
+    o.max_ctas = max_ctas;
+    if (!upper)
+      return gemm_ex(ctx, A.sub(r0, c0, r, c), A.sub(r0, k0, r, K), false, A.sub(c0, k0, c, K), true,
+                     -1.0, 1.0, o);
+    return gemm_ex(ctx, A.sub(r0, c0, r, c), A.sub(k0, r0, K, r), true, A.sub(k0, c0, K, c), false,
+                   -1.0, 1.0, o);
+  };
+  for (int ka = 0; ka < n; ka += 2 * NB) {
+    const int ba = min(NB, n - ka), kb = ka + ba;
+    const int bb = kb < n ? min(NB, n - kb) : 0;
     {
       StreamSwap sw(ctx, s1);
-      if ((rc = panel(ctx, A, upper, k + b, b2, d_info, d_bad, inv, false))) return rc;
+      if ((rc = panel(ctx, A, upper, ka, ba, d_info, d_bad, inv, false))) return rc;
+      if (bb > 0) {
+        // column (row) block b, rows (columns) kb..n: the triangle of its diagonal block only
+        const int rest = n - kb;
+        if (!upper) rc = update(kb, kb, rest, bb, ka, ba, kGemmLower, 0);
+        else rc = update(kb, kb, bb, rest, ka, ba, kGemmUpper, 0);
+        if (rc) return rc;
+        if ((rc = panel(ctx, A, upper, kb, bb, d_info, d_bad, inv, false))) return rc;
+      }
     }
-    // 3. the rest of the trailing update on the caller's stream
-    const int r2 = rest - b2;
-    if (r2 > 0) {
-      GemmOpts ot;
-      ot.mode = upper ? kSyrkUpper : kSyrkLower;
-      ot.max_ctas = ctx->sms - free_sms;
-      const View C = A.sub(k + b + b2, k + b + b2, r2, r2);
-      if (!upper)
-        rc = gemm_ex(ctx, C, A.sub(k + b + b2, k, r2, b), false, A.sub(k + b + b2, k, r2, b),
-                     true, -1.0, 1.0, ot);
-      else
-        rc = gemm_ex(ctx, C, A.sub(k, k + b + b2, b, r2), true, A.sub(k, k + b + b2, b, r2),
-                     false, -1.0, 1.0, ot);
-      if (rc) return rc;
-    }
+    if ((rc = stream_wait(ctx, s0, s1, ctx->ev_join))) return rc;  // the pair's panels done
+    const int kc = kb + bb, rest = n - kc;
+    if (bb == 0 || rest <= 0) break;
+    const int K = ba + bb;
+    // 1. the next pair's block columns (rows for upper storage), K = 256
+    const int nn = min(2 * NB, rest);
+    if (!upper) rc = update(kc, kc, rest, nn, ka, K, kGemmLower, 0);
+    else rc = update(kc, kc, nn, rest, ka, K, kGemmUpper, 0);
+    if (rc) return rc;
+    if ((rc = stream_wait(ctx, s1, s0, ctx->ev_fork))) return rc;
+    // 2. the rest of the trailing matrix, K = 256
+    const int r2 = rest - nn;
+    if (r2 > 0 &&
+        (rc = update(kc + nn, kc + nn, r2, r2, ka, K, upper ? kSyrkUpper : kSyrkLower,
+                     ctx->sms - free_sms)))
+      return rc;
   }
   return MO_OK;
 }
