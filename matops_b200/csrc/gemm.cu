@@ -469,21 +469,20 @@ template <bool AK, bool BKM, bool TMA, bool NARROW>
 int launch_inst(const KParams &kp, const CUtensorMap &ta, const CUtensorMap &tb, int grid,
                 cudaStream_t st) {
   constexpr int SMEM_BYTES = Geo<NARROW>::SMEM;
-  static std::atomic<uint64_t> attr_done{0};
-  int dev = 0;
-  cudaGetDevice(&dev);
   auto kern = dgemm_tile_kernel<AK, BKM, TMA, NARROW>;
-  const uint64_t bit = 1ull << (dev & 63);
-  if (!(attr_done.load() & bit)) {
-    // setmaxnreg.inc only draws on the registers the CTA was launched with: refuse to
-    // launch (instead of waiting forever) if the build did not keep the 168-register split
+  // setmaxnreg.inc only draws on the registers the CTA was launched with: refuse to launch
+  // (instead of waiting forever) if the build did not keep the 168-register split (a
+  // property of the binary, checked once)
+  static std::atomic<int> regs_ok{0};
+  if (!regs_ok.load()) {
     cudaFuncAttributes fa;
     MO_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
     if (fa.numRegs * THREADS < 128 * PRODUCER_REGS + 256 * CONSUMER_REGS) return MO_ENOKERNEL;
-    MO_CUDA_TRY(
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-    attr_done.fetch_or(bit);
+    regs_ok.store(1);
   }
+  // the shared-memory limit is set on every launch (a cheap host call), so that it holds
+  // after a context reset
+  if (int rc = mo_smem_attr((const void *)kern, SMEM_BYTES)) return rc;
   kern<<<grid, THREADS, SMEM_BYTES, st>>>(ta, tb, kp);
   MO_CUDA_TRY(cudaGetLastError());
   return MO_OK;

@@ -508,15 +508,8 @@ bool c_tmap(CUtensorMap *tm, float *C, int64_t M, int64_t N, int64_t ldc) {
 
 template <int PREC>
 int launch_tc(mo_ctx *ctx, const CUtensorMap (&m)[5], const TcParams &p, int grid) {
-  static std::atomic<uint64_t> attr_done{0};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  const uint64_t bit = 1ull << (dev & 63);
-  if (!(attr_done.load() & bit)) {
-    MO_CUDA_TRY(cudaFuncSetAttribute(lp_gemm_tc_kernel<PREC>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, TSMEM));
-    attr_done.fetch_or(bit);
-  }
+  // set on every launch (a cheap host call), so that it holds after a context reset
+  if (int rc = mo_smem_attr((const void *)lp_gemm_tc_kernel<PREC>, TSMEM)) return rc;
   lp_gemm_tc_kernel<PREC><<<grid, TTHREADS, TSMEM, ctx->stream>>>(m[0], m[1], m[2], m[3], m[4], p);
   MO_CUDA_TRY(cudaGetLastError());
   return MO_OK;
