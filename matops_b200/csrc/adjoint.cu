@@ -94,8 +94,6 @@ int chol_adjoint_one(mo_ctx *ctx, View L, View G, const AdjScratch &w, bool stre
   cudaStream_t st = ctx->stream;
   GemmOpts plain;
   plain.stream_k = stream_k;
-  GemmOpts lower = plain;
-  lower.mode = kGemmLower;
   const int last = ((n - 1) / NBA) * NBA;
   int rc;
   for (int j0 = last; j0 >= 0; j0 -= NBA) {
@@ -107,7 +105,10 @@ int chol_adjoint_one(mo_ctx *ctx, View L, View G, const AdjScratch &w, bool stre
     if (below > 0) {
       const View B = L.sub(j0 + jb, j0, below, jb), Bbar = G.sub(j0 + jb, j0, below, jb);
       if ((rc = gemm_ex(ctx, Bbar, Bbar, false, Dinv, false, 1.0, 0.0, plain))) return rc;
-      if ((rc = gemm_ex(ctx, Dbar, Bbar, true, B, false, -1.0, 1.0, lower))) return rc;
+      // one 128 x 128 tile with K = rows below: as a plain product it is spread over the
+      // device by stream-K (a triangle-mode launch would run on one SM); the strict upper
+      // part of Dbar it also writes is never read and is overwritten at the end
+      if ((rc = gemm_ex(ctx, Dbar, Bbar, true, B, false, -1.0, 1.0, plain))) return rc;
       if (j0 > 0) {
         const View C = L.sub(j0 + jb, 0, below, j0), Cbar = G.sub(j0 + jb, 0, below, j0);
         if ((rc = gemm_ex(ctx, Cbar, Bbar, false, R, false, -1.0, 1.0, plain))) return rc;
