@@ -560,11 +560,20 @@ int launch_gemm(const GemmArgs &a, cudaStream_t stream) {
     kp.sk_iters = (int)((T - dp) * kp.kt);
     grid = sms;
     kp.sk_chunk = (kp.sk_iters + grid - 1) / grid;
-    if (kp.sk_chunk < 4) {  // too little work per CTA: stay data-parallel
-      kp.dp_tiles = (int)T;
-      kp.sk_iters = 0;
-      kp.sk_chunk = 1;
-      grid = (int)std::min<long long>(T, sms);
+    if (kp.sk_chunk < 4) {
+      // too little work for every CTA: fewer CTAs with 4 slabs each when that still uses
+      // more SMs than whole tiles would (a few tiles with a long K, e.g. one 128 x 128
+      // tile with K in the thousands), else data-parallel
+      const long long g2 = kp.sk_iters / 4;
+      if (kp.kt >= 32 && g2 > T) {
+        grid = (int)std::min<long long>(g2, sms);
+        kp.sk_chunk = (kp.sk_iters + grid - 1) / grid;
+      } else {
+        kp.dp_tiles = (int)T;
+        kp.sk_iters = 0;
+        kp.sk_chunk = 1;
+        grid = (int)std::min<long long>(T, sms);
+      }
     }
   }
 

@@ -29,6 +29,8 @@ def host(t):
                                    (129, 257, 65), (300, 5, 1000), (7, 300, 3),
                                    # few-wave shapes: K split over CTAs (stream-K partial sums)
                                    (1536, 1536, 256), (1280, 1408, 400), (1000, 700, 1333),
+                                   # a few tiles with a long K: fewer CTAs of 4 slabs each
+                                   (128, 128, 4096), (100, 250, 3000), (128, 384, 1100),
                                    # narrow C (N <= 64, M >= 2048): 256 x 64 tiles
                                    (2048, 64, 512), (2500, 33, 700), (4099, 1, 129), (3000, 64, 16)])
 def test_mult(gpu, oracle, rng, flags, m, n, k):
