@@ -2,7 +2,7 @@
 // The reference has no derivatives; these are the adjoints of DecomposeCHOL (chol.go:116)
 // and SolveCHOL (chol.go:147) for LOWER factors.
 //
-// Cholesky adjoint, blocked right to left (block size 128), in place on Lbar.  With the
+// Cholesky adjoint, blocked right to left (block size 256), in place on Lbar.  With the
 // factor partitioned at block column j as
 //       [ .  .      ]        R = L(j, 0:j)      D = L(j, j)
 //       [ R  D      ]        C = L(j+1:, 0:j)   B = L(j+1:, j)
@@ -10,7 +10,7 @@
 // and Rbar, Dbar, Cbar, Bbar the matching blocks of the adjoint storage, each step undoes
 // the forward step of the left-looking algorithm (B = (A_B - C R^T) D^-T, D = chol(A_D -
 // R R^T)) and leaves the adjoint of the lower-triangle entries of A in place of Dbar, Bbar:
-//   Bbar <- Bbar D^-1                      (GEMM with the 128 x 128 inverse of D)
+//   Bbar <- Bbar D^-1                      (GEMM with the inverse of D)
 //   Dbar <- Dbar - tril(Bbar^T B)          (GEMM, lower mode)
 //   Cbar <- Cbar - Bbar R                  (GEMM)
 //   Rbar <- Rbar - Bbar^T C                (GEMM)
@@ -19,7 +19,7 @@
 // Phi(X) = lower triangle of X with the diagonal halved.  The result is the adjoint with
 // respect to the lower-triangle entries of A; a last pass turns it into the symmetric
 // gradient (both triangles, off-diagonal entries halved).  Only L is read besides Lbar:
-// no forward panel is stored, and the extra device memory is five 128 x 128 blocks per
+// no forward panel is stored, and the extra device memory is five 256 x 256 blocks per
 // stream whatever n is.  The flops are about 2 n^3 / 3 (twice the factorization).
 //
 // Batched form: orders up to 512 run in one persistent kernel (each CTA takes whole matrices,
@@ -38,7 +38,8 @@ int trtri_blocks(mo_ctx *ctx, View A, int N, bool trans, bool lower_eff, bool un
 
 namespace {
 
-constexpr int NBA = 128;
+constexpr int NBA = 256;   // block columns per step of the single-matrix sweep
+constexpr int NBI = 128;   // order of the diagonal inverses trtri_blocks forms
 constexpr int NSTREAMS = 8;
 
 // Dz = tril(D), Gz = tril(G) (both jb x jb, ld NBA), zero elsewhere in the NBA x NBA blocks
@@ -57,6 +58,17 @@ __global__ void adj_phi_kernel(double *X) {
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < NBA * NBA; e += gridDim.x * blockDim.x) {
     const int i = e % NBA, j = e / NBA;
     X[e] = i > j ? X[e] : (i == j ? 0.5 * X[e] : 0.0);
+  }
+}
+
+// Di (NBA x NBA) = the 128 x 128 diagonal-block inverses of a jb x jb triangle (inv:
+// trtri_blocks' layout, NBI x NBI blocks back to back), zeros elsewhere
+__global__ void adj_place_kernel(const double *inv, double *Di, int jb) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < NBA * NBA; e += gridDim.x * blockDim.x) {
+    const int i = e % NBA, j = e / NBA, b = i / NBI;
+    Di[e] = (b == j / NBI && i < jb && j < jb)
+                ? inv[(size_t)b * NBI * NBI + (i - b * NBI) + (size_t)(j - b * NBI) * NBI]
+                : 0.0;
   }
 }
 
@@ -85,7 +97,7 @@ __global__ void adj_symmetrize_kernel(double *G, int64_t ld, int n) {
 }
 
 struct AdjScratch {
-  double *inv, *Dz, *X1, *X2;  // NBA x NBA each
+  double *inv, *Dz, *X1, *X2, *Di;  // NBA x NBA each (inv: trtri_blocks' 128-blocks)
 };
 
 // one matrix, on ctx->stream; stream_k must be off when several streams share the context
@@ -100,8 +112,19 @@ int chol_adjoint_one(mo_ctx *ctx, View L, View G, const AdjScratch &w, bool stre
     const int jb = std::min(NBA, n - j0), below = n - j0 - jb;
     const View D = L.sub(j0, j0, jb, jb), Dbar = G.sub(j0, j0, jb, jb);
     const View R = L.sub(j0, 0, jb, j0), Rbar = G.sub(j0, 0, jb, j0);
-    const View Dinv{w.inv, jb, jb, NBA};
+    // D^-1: the 128 x 128 diagonal blocks' inverses, then X21 = -X22 (D21 X11)
     if ((rc = trtri_blocks(ctx, D, jb, false, true, false, w.inv))) return rc;
+    adj_place_kernel<<<64, 256, 0, st>>>(w.inv, w.Di, jb);
+    MO_CUDA_TRY(cudaGetLastError());
+    if (jb > NBI) {
+      const int mc = jb - NBI;
+      const View X11{w.Di, NBI, NBI, NBA}, X22{w.Di + NBI + (size_t)NBI * NBA, mc, mc, NBA};
+      const View T{w.X2, mc, NBI, NBA}, X21{w.Di + NBI, mc, NBI, NBA};
+      if ((rc = gemm_ex(ctx, T, L.sub(j0 + NBI, j0, mc, NBI), false, X11, false, 1.0, 0.0, plain)))
+        return rc;
+      if ((rc = gemm_ex(ctx, X21, X22, false, T, false, -1.0, 0.0, plain))) return rc;
+    }
+    const View Dinv{w.Di, jb, jb, NBA};
     if (below > 0) {
       const View B = L.sub(j0 + jb, j0, below, jb), Bbar = G.sub(j0 + jb, j0, below, jb);
       if ((rc = gemm_ex(ctx, Bbar, Bbar, false, Dinv, false, 1.0, 0.0, plain))) return rc;
@@ -333,11 +356,11 @@ __global__ void __launch_bounds__(ABT) adj_batch_kernel(AdjBatchArgs p) {
   }
 }
 
-size_t scratch_doubles() { return 4 * (size_t)NBA * NBA; }
+size_t scratch_doubles() { return 5 * (size_t)NBA * NBA; }
 
 AdjScratch carve(double *base) {
   const size_t blk = (size_t)NBA * NBA;
-  return AdjScratch{base, base + blk, base + 2 * blk, base + 3 * blk};
+  return AdjScratch{base, base + blk, base + 2 * blk, base + 3 * blk, base + 4 * blk};
 }
 
 int adj_workspace(mo_ctx *ctx, size_t bytes, double **out) {
