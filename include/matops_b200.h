@@ -58,6 +58,11 @@ extern "C" {
 #define MO_ENOKERNEL (-23)   /* no sm_100a kernel image for this device               */
 #define MO_ESTATICLIMIT (-11) /* larger than the fixed scratch of mo_solve_trm_static   */
 #define MO_EBATCHN (-12)     /* a batched matrix order outside 1..MO_BATCH_MAX_N      */
+#define MO_EWORKSMALL (-13)  /* "work space too small"  qrwy.go:526 ("workspace too small",
+                                qrwym.go:667)                                         */
+#define MO_ENOWORK (-14)     /* "workspace not defined"                  qrwym.go:652 */
+#define MO_ECQSIZE (-15)     /* "C*Q: C.Cols != A.Rows"                  qrwym.go:656 */
+#define MO_ETSMALL (-16)     /* "reflector matrix T too small"           qrwy.go:550 */
 
 typedef struct mo_ctx mo_ctx;
 
@@ -213,6 +218,61 @@ MO_API int mo_update_trm(mo_ctx *ctx, mo_matrix C, mo_matrix A, mo_matrix B, dou
 MO_API int mo_inverse_trm(mo_ctx *ctx, mo_matrix A, int flags, int nb);
 
 /* ---- factorizations and solves ---- */
+
+/* ---- QR with the compact WY form (qrwy.go, qrwym.go, house.go) ----
+ *
+ * A (m x n) = Q R, k = min(m, n) reflectors H(j) = I - tau_j v_j v_j^T (LAPACK dlarfg,
+ * house.go:55-78), Q = H(0)...H(k-1) = I - Y T Y^T with Y the unit lower trapezoid stored
+ * below A's diagonal and T the k x k upper triangular block reflector (LAPACK dlarft).
+ * These compute the LAPACK quantities the reference's documentation names at every size.
+ * The reference's own transposed GEMV (calgo/dmvec_gemv.c:368-395) rescales its output by
+ * beta once per 68 rows, so its DecomposeQRT / BuildT / blocked DecomposeQR / MultQ give the
+ * same T only while at most 68 rows lie below each reflector (m <= 69), and a different,
+ * non-orthogonal Q beyond that.  W: the reference's workspace argument; data == NULL stands
+ * for nil.  W is checked as the reference checks it; the device works in context workspace
+ * (about (m + k) k + 2 max(m, n) 128 doubles).  m <= 148 * 895 rows, k <= 65535. */
+
+/* DecomposeQRT(A, T, W, nb), qrwy.go:517-538: A = Q R in place, T's upper k x k triangle
+ * set (its strict lower part untouched).  nb > 0 and A.cols > nb with a non-NULL W smaller
+ * than A.cols x nb -> MO_EWORKSMALL; T smaller than k x k -> MO_ETSMALL.  The device
+ * blocks by 32 / 128 whatever nb is (results agree to rounding).  Asynchronous. */
+MO_API int mo_decompose_qrt(mo_ctx *ctx, mo_matrix A, mo_matrix T, mo_matrix W, int nb);
+
+/* DecomposeQR(A, tau, W, nb), qrwy.go:474-497: as mo_decompose_qrt with the scalar factors
+ * in tau (a vector view of at least k entries) instead of T (LAPACK DGEQRF). */
+MO_API int mo_decompose_qr(mo_ctx *ctx, mo_matrix A, mo_matrix tau, mo_matrix W, int nb);
+
+/* BuildT(T, A, tau), qrwy.go:546-556: T's upper triangle <- the block reflector of A's
+ * reflectors and tau; columns whose tau is zero are not written (as the reference).  T
+ * smaller than A.cols x A.cols -> MO_ETSMALL. */
+MO_API int mo_build_t(mo_ctx *ctx, mo_matrix T, mo_matrix A, mo_matrix tau);
+
+/* MultQT(C, A, T, W, flags, nb), qrwym.go:646-688: C = Q C (MO_LEFT or no side bit),
+ * Q^T C (with MO_TRANS), C Q (MO_RIGHT), C Q^T (MO_RIGHT|MO_TRANS); Q from mo_decompose_qrt's
+ * A and T, applied nb reflectors at a time in the reference's order (nb == 0: T.cols).
+ * W NULL -> MO_ENOWORK; MO_RIGHT with C.cols != A.rows -> MO_ECQSIZE; W smaller than
+ * C.rows (MO_RIGHT) or C.cols (left) x nb -> MO_EWORKSMALL; left with C.rows != A.rows ->
+ * MO_EABSIZE (unchecked by the reference).  Asynchronous. */
+MO_API int mo_mult_qt(mo_ctx *ctx, mo_matrix C, mo_matrix A, mo_matrix T, mo_matrix W, int flags,
+                      int nb);
+
+/* MultQ(C, A, tau, W, flags, nb), qrwym.go:573-630: mo_mult_qt with Q from A and tau
+ * (DORMQR); nb == 0 needs no W. */
+MO_API int mo_mult_q(mo_ctx *ctx, mo_matrix C, mo_matrix A, mo_matrix tau, mo_matrix W, int flags,
+                     int nb);
+
+/* SolveQRT(B, A, T, W, flags, nb), qrwym.go:784-819, A m x n with m >= n: least squares
+ * X = argmin ||A X - B|| into B's first n rows (B = Q^T B, then R^-1); with MO_TRANS the
+ * minimum-norm solution of A^T X = B (B's first n rows = R^-T B, the rows below cleared,
+ * then B = Q B).  m < n or B.rows < n -> MO_EABSIZE. */
+MO_API int mo_solve_qrt(mo_ctx *ctx, mo_matrix B, mo_matrix A, mo_matrix T, mo_matrix W,
+                        int flags, int nb);
+
+/* SolveQR(B, A, tau, W, flags, nb), qrwym.go:717-760: mo_solve_qrt with Q from tau.  With
+ * MO_TRANS the reference rebinds B to an empty view before applying Q (qrwym.go:735); this
+ * applies Q as mo_solve_qrt does. */
+MO_API int mo_solve_qr(mo_ctx *ctx, mo_matrix B, mo_matrix A, mo_matrix tau, mo_matrix W,
+                       int flags, int nb);
 
 /* DecomposeCHOL(A, flags, nb), chol.go:116-127: A = L*L^T (MO_LOWER) or U^T*U (otherwise)
  * in place; the opposite strict triangle is not referenced.  Non-square -> MO_ENOTSQUARE.

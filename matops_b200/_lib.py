@@ -61,6 +61,13 @@ def lib() -> ctypes.CDLL:
         "mo_rank_update2_sym": [p, M, M, M, d, d, i],
         "mo_update_trm": [p, M, M, M, d, d, i],
         "mo_inverse_trm": [p, M, i, i],
+        "mo_decompose_qrt": [p, M, M, M, i],
+        "mo_decompose_qr": [p, M, M, M, i],
+        "mo_build_t": [p, M, M, M],
+        "mo_mult_qt": [p, M, M, M, M, i, i],
+        "mo_mult_q": [p, M, M, M, M, i, i],
+        "mo_solve_qrt": [p, M, M, M, M, i, i],
+        "mo_solve_qr": [p, M, M, M, M, i, i],
         "mo_mirror_create": [p, p, i64, ctypes.POINTER(p)],
         "mo_mirror_destroy": [p],
         "mo_mirror_find": [p, ctypes.POINTER(p), ctypes.POINTER(i64)],

@@ -197,6 +197,59 @@ def SolveLU(B, A, pivots: torch.Tensor, flags: int):
     return _err(rc)
 
 
+# ---- QR with the compact WY form (qrwy.go, qrwym.go) ----
+
+def _wview(W):
+    """the reference's optional workspace: None stands for a nil matrix"""
+    return _lib.MoMatrix(None, 0, 0, 1) if W is None else view(W)
+
+
+def _vec(tau):
+    """a 1-D or (k x 1) CUDA float64 tensor as a column vector view"""
+    if tau.dim() == 1:
+        tau = tau.unsqueeze(1)
+    return view(tau)
+
+
+def DecomposeQRT(A, T, W, nb: int):
+    """qrwy.go:517 -- A = Q R in place, T the block reflector (Q = I - Y T Y^T); returns
+    (A, err)"""
+    return A, _err(_lib.lib().mo_decompose_qrt(context(), view(A), view(T), _wview(W), nb))
+
+
+def DecomposeQR(A, tau, W, nb: int):
+    """qrwy.go:474 -- A = Q R in place, the reflectors' scalar factors in tau (DGEQRF);
+    returns (A, err)"""
+    return A, _err(_lib.lib().mo_decompose_qr(context(), view(A), _vec(tau), _wview(W), nb))
+
+
+def BuildT(T, A, tau):
+    """qrwy.go:546 -- T = the block reflector of A's reflectors and tau; returns (T, err)"""
+    return T, _err(_lib.lib().mo_build_t(context(), view(T), view(A), _vec(tau)))
+
+
+def MultQT(C, A, T, W, flags: int, nb: int):
+    """qrwym.go:646 -- C = Q C, Q^T C (TRANS), C Q (RIGHT), C Q^T (RIGHT|TRANS)"""
+    return _err(_lib.lib().mo_mult_qt(context(), view(C), view(A), view(T), _wview(W), flags, nb))
+
+
+def MultQ(C, A, tau, W, flags: int, nb: int):
+    """qrwym.go:573 -- MultQT with Q from A and tau (DORMQR)"""
+    return _err(_lib.lib().mo_mult_q(context(), view(C), view(A), _vec(tau), _wview(W), flags, nb))
+
+
+def SolveQRT(B, A, T, W, flags: int, nb: int):
+    """qrwym.go:784 -- least squares min ||A X - B|| (or, TRANS, min-norm A^T X = B) into B"""
+    return _err(_lib.lib().mo_solve_qrt(context(), view(B), view(A), view(T), _wview(W), flags,
+                                        nb))
+
+
+def SolveQR(B, A, tau, W, flags: int, nb: int):
+    """qrwym.go:717 -- SolveQRT with Q from A and tau"""
+    return _err(_lib.lib().mo_solve_qr(context(), view(B), view(A), _vec(tau), _wview(W), flags,
+                                       nb))
+
+
 # ---- mixed precision (no counterpart in the reference; LAPACK dsposv is the model) ----
 
 PREC_BF16X3, PREC_TF32X3 = 1, 2

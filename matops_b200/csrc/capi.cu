@@ -227,6 +227,10 @@ const char *mo_strerror(int s) {
     case MO_ENOKERNEL: return "no sm_100a kernel image for this device";
     case MO_ESTATICLIMIT: return "matrix order exceeds the fixed scratch of mo_solve_trm_static";
     case MO_EBATCHN: return "batched matrix order outside 1..MO_BATCH_MAX_N";
+    case MO_EWORKSMALL: return "work space too small";
+    case MO_ENOWORK: return "workspace not defined";
+    case MO_ECQSIZE: return "C*Q: C.Cols != A.Rows";
+    case MO_ETSMALL: return "reflector matrix T too small";
     default: return s > 0 ? "illegal value (non-positive pivot)" : "unknown error";
   }
 }

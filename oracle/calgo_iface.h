@@ -58,4 +58,10 @@ void dmmat_rank2_blk(mdata_t *C, const mdata_t *A, const mdata_t *B,
 void dmmat_trmupd_blk(mdata_t *C, const mdata_t *A, const mdata_t *B, double alpha, double beta,
                       int flags, int P, int S, int E, int vlen, int NB);
 
+/* the QR path's level-1/2 kernels (calgo/cmops.h:107, 117-119, 193) */
+double dvec_nrm2(const mvec_t *X, int N);
+void dmmat_scale_plus(mdata_t *A, const mdata_t *B, double alpha, double beta, int flags,
+                      int S, int L, int R, int E);
+void dmvec_trid_unb(mvec_t *X, const mdata_t *A, int flags, int N);
+
 #endif

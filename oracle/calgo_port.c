@@ -181,15 +181,37 @@ void dmvec_symv_rank(mdata_t *A, const mvec_t *X, double alpha, int flags, int S
   }
 }
 
-/* calgo/dmvec_gemv.c:353-427 (dmult_gemv_blocked), the non-transposed form used on this
- * path: per MB row block, y = beta*y (dscale_vec semantics), then y += alpha*A[:,S:L]*x. */
+/* 0: the transposed GEMV scales y by beta once per MB-row block of A (the reference's
+ * calgo/dmvec_gemv.c:368-395); 1: once in all (BLAS semantics, or_gemv_beta_once) */
+static int gemv_beta_once = 0;
+int or_gemv_beta_once(int on) {
+  int old = gemv_beta_once;
+  gemv_beta_once = on;
+  return old;
+}
+
+/* calgo/dmvec_gemv.c:353-427 (dmult_gemv_blocked).  Non-transposed: per MB row block,
+ * y = beta*y (dscale_vec semantics), then y += alpha*A[:,S:L]*x.  Transposed (y[R:E] +=
+ * alpha*A[S:L,R:E]^T x[S:L]): per MB block of A's rows S..L-1 the WHOLE of y[R:E] is first
+ * scaled by beta (calgo/dmvec_gemv.c:379-393), so y ends as beta^nblocks*y + ... when
+ * beta != 1 and L-S > MB. */
 void dmult_gemv_blocked(mvec_t *Y, const mdata_t *A, const mvec_t *X, double alpha, double beta,
                         int flags, int S, int L, int R, int E, int vlen, int MB) {
   (void)vlen;
   if (L - S <= 0 || E - R <= 0) return;
   if (flags & MTX_TRANSA) {
-    fprintf(stderr, "oracle: transposed GEMV is not on the restated path\n");
-    abort();
+    if (MB <= 0) MB = L - S;
+    for (int i = S; i < L; i += MB) {
+      const int nI = L - i < MB ? L - i : MB;
+      if (beta != 1.0 && (!gemv_beta_once || i == S))
+        scale_vec(&Y->md[(long)R * Y->inc], Y->inc, beta, E - R);
+      for (int r = R; r < E; r++) {
+        double s = 0.0;
+        for (int c = i; c < i + nI; c++) s += AT(A, c, r) * X->md[(long)c * X->inc];
+        Y->md[(long)r * Y->inc] += alpha * s;
+      }
+    }
+    return;
   }
   if (MB <= 0) MB = E - R;
   for (int i = R; i < E; i += MB) {
@@ -384,4 +406,55 @@ void dmvec_rank(mdata_t *A, const mvec_t *X, const mvec_t *Y, double alpha, int 
 /* calgo/dvec_util.c:250-264 (dvec_scal): X *= alpha */
 void dvec_scal(mvec_t *X, double alpha, int N) {
   for (int i = 0; i < N; i++) X->md[(long)i * X->inc] *= alpha;
+}
+
+/* calgo/dvec_util.c:120-141 (dvec_nrm2): sqrt of the sum of squares, no scaling */
+double dvec_nrm2(const mvec_t *X, int N) {
+  double s = 0.0;
+  for (int i = 0; i < N; i++) {
+    const double x = X->md[(long)i * X->inc];
+    s += x * x;
+  }
+  return sqrt(s);
+}
+
+/* calgo/dmmat_plus.c:86-116 (dmmat_scale_plus): A = alpha*A + beta*op(B) over rows R..E-1
+ * and columns S..L-1 of A (op per MTX_TRANSB; with MTX_TRANSA the same on A^T); alpha == 0
+ * does not read A */
+void dmmat_scale_plus(mdata_t *A, const mdata_t *B, double alpha, double beta, int flags,
+                      int S, int L, int R, int E) {
+  if (L - S <= 0 || E - R <= 0) return;
+  const int ta = (flags & MTX_TRANSA) != 0, tb = (flags & MTX_TRANSB) != 0;
+  for (int j = S; j < L; j++)
+    for (int i = R; i < E; i++) {
+      /* element (i, j) of op_A(A) and of op_B(B) */
+      double *a = ta ? &AT(A, j, i) : &AT(A, i, j);
+      const double b = tb ? AT(B, j, i) : AT(B, i, j);
+      *a = alpha == 0.0 ? beta * b : alpha * *a + beta * b;
+    }
+}
+
+/* calgo/dmvec_trid.c:209-230 (dmvec_trid_unb): X = op(A)*X for the N x N upper (MTX_UPPER)
+ * or lower triangle of A, unit diagonal with MTX_UNIT, op = transpose with MTX_TRANSA or
+ * MTX_TRANS */
+void dmvec_trid_unb(mvec_t *X, const mdata_t *A, int flags, int N) {
+  if (N <= 0) return;
+  const int unit = (flags & MTX_UNIT) != 0, upper = (flags & MTX_UPPER) != 0;
+  const int tr = (flags & (MTX_TRANSA | MTX_TRANS)) != 0;
+  double *x = X->md;
+  const long inc = X->inc;
+  /* effective upper: x_i depends on x_j with j >= i, so compute i upward */
+  if (upper != tr) {
+    for (int i = 0; i < N; i++) {
+      double s = unit ? x[i * inc] : 0.0;
+      for (int j = i + unit; j < N; j++) s += (upper ? AT(A, i, j) : AT(A, j, i)) * x[j * inc];
+      x[i * inc] = s;
+    }
+  } else {
+    for (int i = N - 1; i >= 0; i--) {
+      double s = unit ? x[i * inc] : 0.0;
+      for (int j = 0; j <= i - unit; j++) s += (upper ? AT(A, j, i) : AT(A, i, j)) * x[j * inc];
+      x[i * inc] = s;
+    }
+  }
 }

@@ -590,6 +590,344 @@ int or_solve_lu_fm(fm B, fm A, pv p, int flags) {
   return OR_OK;
 }
 
+/* ---------------- house.go, qrwy.go, qrwym.go: QR with the compact WY form ---------------- */
+
+enum {
+  OR_EWORKSMALL = -13, /* "work space too small" qrwy.go:526 / "workspace too small" qrwym.go:667 */
+  OR_ENOWORK = -14,    /* "workspace not defined"           qrwym.go:652 */
+  OR_ECQSIZE = -15,    /* "C*Q: C.Cols != A.Rows"           qrwym.go:656 */
+  OR_ETSMALL = -16     /* "reflector matrix T too small"    qrwy.go:550 */
+};
+
+/* mvec.go:362-376 (Norm2) over calgo/dvec_util.c:120 */
+static double Norm2(fm X) {
+  if (!is_vector(X)) return NAN;
+  mvec_t x = {X.d, X.c != 1 ? X.ld : 1};
+  return dvec_nrm2(&x, X.r * X.c);
+}
+
+/* mmult.go:478-490 (ScalePlus): A = alpha*A + beta*op(B) */
+static void ScalePlus(fm A, fm B, double alpha, double beta, int flags) {
+  mdata_t a = {A.d, A.ld}, b = {B.d, B.ld};
+  dmmat_scale_plus(&a, &b, alpha, beta, flags, 0, A.c, 0, A.r);
+}
+
+/* mvec.go:226-245 (MVMultTrm): X = op(A)*X, A triangular */
+static int MVMultTrm(fm X, fm A, int flags) {
+  if (A.r == 0 || A.c == 0) return OR_OK;
+  if (X.r != 1 && X.c != 1) return OR_ENOTVECTOR;
+  mdata_t a = {A.d, A.ld};
+  mvec_t x = {X.d, X.r == 1 ? X.ld : 1};
+  dmvec_trid_unb(&x, &a, flags, A.c);
+  return OR_OK;
+}
+
+/* element k of a row or column vector view */
+static inline double *vel(fm X, int k) { return X.c == 1 ? X.d + k : X.d + (intptr_t)k * X.ld; }
+
+/* house.go:18-32 (sqrtX2Y2, LAPACK dlapy2) */
+static double sqrtX2Y2(double x, double y) {
+  const double xa = fabs(x), ya = fabs(y);
+  const double w = xa > ya ? xa : ya, z = xa < ya ? xa : ya;
+  if (z == 0.0) return w;
+  return w * sqrt(1.0 + (z / w) * (z / w));
+}
+
+/* house.go:55-78 (computeHouseholder, LAPACK dlarfg): reflector of [a11; x]; x becomes v,
+ * a11 becomes beta, *tau the scalar factor (0 when x is zero) */
+static void computeHouseholder(fm a11, fm x, fm tau) {
+  const double nx = Norm2(x);
+  if (nx == 0.0) {
+    tau.d[0] = 0.0;
+    return;
+  }
+  const double alpha = a11.d[0];
+  const double sign = signbit(alpha) ? -1.0 : 1.0;
+  const double beta = -sign * sqrtX2Y2(alpha, nx);
+  InvScale(x, alpha - beta);
+  tau.d[0] = (beta - alpha) / beta;
+  a11.d[0] = beta;
+}
+
+/* house.go:97-122 (applyHouseholder, side LEFT): [a1; A2] = H*[a1; A2] with
+ * w1 = tau*(a1 + A2^T v), a1 -= w1, A2 -= v*w1 */
+static void applyHouseholderLeft(fm tau, fm v, fm a1, fm A2) {
+  const double t = tau.d[0];
+  if (t == 0.0) return;
+  const int n = a1.r * a1.c;
+  double *buf = (double *)malloc(sizeof(double) * (n > 0 ? n : 1));
+  for (int k = 0; k < n; k++) buf[k] = *vel(a1, k);
+  fm w1 = {buf, 1, n, 1};
+  MVMult(w1, A2, v, 1.0, 1.0, MTX_TRANSA);
+  Scale(w1, t);
+  for (int k = 0; k < n; k++) *vel(a1, k) -= buf[k];
+  MVRankUpdate(A2, v, w1, -1.0);
+  free(buf);
+}
+
+/* t01 = T00 * (-tau * (a10^T + A20^T a21)): column j of the block reflector
+ * (qrwy.go:61-70 and :121-129) */
+static void qr_t_column(fm T, int j, double tauval, fm a10, fm A20, fm a21) {
+  fm t01 = sub(T, 0, j, j, 1), T00 = sub(T, 0, 0, j, j);
+  for (int k = 0; k < j; k++) *vel(t01, k) = *vel(a10, k);
+  MVMult(t01, A20, a21, -tauval, -tauval, MTX_TRANSA);
+  MVMultTrm(t01, T00, MTX_UPPER);
+}
+
+/* qrwy.go:91-140 (unblockedQRT) */
+static void unblockedQRT(fm A, fm T) {
+  for (int j = 0; j < A.r && j < A.c; j++) {
+    fm a11 = sub(A, j, j, 1, 1), a21 = sub(A, j + 1, j, A.r - j - 1, 1);
+    fm a12 = sub(A, j, j + 1, 1, A.c - j - 1), A22 = sub(A, j + 1, j + 1, A.r - j - 1, A.c - j - 1);
+    fm t11 = sub(T, j, j, 1, 1);
+    computeHouseholder(a11, a21, t11);
+    applyHouseholderLeft(t11, a21, a12, A22);
+    const double tauval = t11.d[0];
+    if (tauval != 0.0) qr_t_column(T, j, tauval, sub(A, j, 0, 1, j), sub(A, j + 1, 0, A.r - j - 1, j), a21);
+  }
+}
+
+/* qrwy.go:146-181 (unblockedQR): tau(j) per reflector, no T */
+static void unblockedQR(fm A, fm tau) {
+  for (int j = 0; j < A.r && j < A.c && j < tau.r; j++) {
+    fm a11 = sub(A, j, j, 1, 1), a21 = sub(A, j + 1, j, A.r - j - 1, 1);
+    fm a12 = sub(A, j, j + 1, 1, A.c - j - 1), A22 = sub(A, j + 1, j + 1, A.r - j - 1, A.c - j - 1);
+    fm tau1 = sub(tau, j, 0, 1, 1);
+    computeHouseholder(a11, a21, tau1);
+    applyHouseholderLeft(tau1, a21, a12, A22);
+  }
+}
+
+/* qrwy.go:29-84 (unblkQRBlockReflector, LAPACK dlarft): T from the reflectors in A and tau */
+static void unblkQRBlockReflector(fm T, fm A, fm tau) {
+  for (int j = 0; j < A.r && j < A.c && j < tau.r; j++) {
+    const double tauval = tau.d[j];
+    if (tauval != 0.0) {
+      T.d[j + (intptr_t)j * T.ld] = tauval;
+      qr_t_column(T, j, tauval, sub(A, j, 0, 1, j), sub(A, j + 1, 0, A.r - j - 1, j),
+                  sub(A, j + 1, j, A.r - j - 1, 1));
+    }
+  }
+}
+
+/* qrwy.go:266-303 (updateWithQT): [C1; C2] = Q^T [C1; C2] (transpose) or Q [C1; C2] with
+ * Q = I - Y T Y^T, Y = [Y1 (unit lower); Y2] */
+static void updateWithQT(fm C1, fm C2, fm Y1, fm Y2, fm T, fm W, int transpose) {
+  ScalePlus(W, C1, 0.0, 1.0, MTX_TRANSB);
+  or_mult_trm_fm(W, Y1, 1.0, MTX_LOWER | MTX_UNIT | MTX_RIGHT);
+  or_mult_fm(W, C2, Y2, 1.0, 1.0, MTX_TRANSA);
+  int tflags = MTX_UPPER | MTX_RIGHT;
+  if (!transpose) tflags |= MTX_TRANSA;
+  or_mult_trm_fm(W, T, 1.0, tflags);
+  or_mult_fm(C2, Y2, W, -1.0, 1.0, MTX_TRANSB);
+  or_mult_trm_fm(W, Y1, 1.0, MTX_LOWER | MTX_UNIT | MTX_TRANSA | MTX_RIGHT);
+  ScalePlus(C1, W, 1.0, -1.0, MTX_TRANSB);
+}
+
+/* qrwy.go:315-348 (updateWithQTRight): [C1 C2] = [C1 C2] Q^T (transpose) or [C1 C2] Q */
+static void updateWithQTRight(fm C1, fm C2, fm Y1, fm Y2, fm T, fm W, int transpose) {
+  ScalePlus(W, C1, 0.0, 1.0, MTX_NOTRANS);
+  or_mult_trm_fm(W, Y1, 1.0, MTX_LOWER | MTX_UNIT | MTX_RIGHT);
+  or_mult_fm(W, C2, Y2, 1.0, 1.0, MTX_NOTRANS);
+  int tflags = MTX_UPPER | MTX_RIGHT;
+  if (transpose) tflags |= MTX_TRANSA;
+  or_mult_trm_fm(W, T, 1.0, tflags);
+  or_mult_fm(C2, W, Y2, -1.0, 1.0, MTX_TRANSB);
+  or_mult_trm_fm(W, Y1, 1.0, MTX_LOWER | MTX_UNIT | MTX_RIGHT | MTX_TRANSA);
+  ScalePlus(C1, W, 1.0, -1.0, MTX_NOTRANS);
+}
+
+/* qrwy.go:433-453 (updateQRTReflector): T = -T1 * (Y10^T Y11 + Y20^T Y21) * T2 */
+static void updateQRTReflector(fm T, fm Y10, fm Y20, fm Y11, fm Y21, fm T1, fm T2) {
+  if (Y10.c == 0) return;
+  ScalePlus(T, Y10, 0.0, 1.0, MTX_TRANSB);
+  or_mult_trm_fm(T, Y11, 1.0, MTX_LOWER | MTX_UNIT | MTX_RIGHT);
+  or_mult_fm(T, Y20, Y21, 1.0, 1.0, MTX_TRANSA);
+  or_mult_trm_fm(T, T1, -1.0, MTX_UPPER);
+  or_mult_trm_fm(T, T2, 1.0, MTX_UPPER | MTX_RIGHT);
+}
+
+/* qrwy.go:351-427 (blockedQRT); the partitions of partition.go clip the block to the
+ * columns left (repartition2x2to3x3, pBOTTOMRIGHT) */
+static void blockedQRT(fm A, fm T, fm W, int nb) {
+  for (int k = 0; k < A.r && k < A.c; ) {
+    const int b = imin(nb, A.c - k), bt = imin(nb, T.c - k), bw = imin(nb, W.r - k);
+    fm A10 = sub(A, k, 0, b, k), A11 = sub(A, k, k, b, b), A12 = sub(A, k, k + b, b, A.c - k - b);
+    fm A20 = sub(A, k + b, 0, A.r - k - b, k), A21 = sub(A, k + b, k, A.r - k - b, b);
+    fm A22 = sub(A, k + b, k + b, A.r - k - b, A.c - k - b);
+    fm T00 = sub(T, 0, 0, k, k), T01 = sub(T, 0, k, k, bt), T11 = sub(T, k, k, bt, bt);
+    fm W2 = sub(W, k + bw, 0, W.r - k - bw, W.c);
+    fm AL = sub(A, k, k, A.r - k, imin(nb, A.c - k));
+    unblockedQRT(AL, T11);
+    updateWithQT(A12, A22, A11, A21, T11, W2, 1);
+    updateQRTReflector(T01, A10, A20, A11, A21, T00, T11);
+    k += b;
+  }
+}
+
+/* qrwy.go:188-259 (blockedQR): DGEQRF with a scratch T per block; tau from its diagonal */
+static void blockedQR(fm A, fm tau, fm Twork, fm W, int nb) {
+  for (int k = 0; k < A.r && k < A.c; ) {
+    const int b = imin(nb, A.c - k), bw = imin(nb, W.r - k);
+    fm A11 = sub(A, k, k, b, b), A12 = sub(A, k, k + b, b, A.c - k - b);
+    fm A21 = sub(A, k + b, k, A.r - k - b, b), A22 = sub(A, k + b, k + b, A.r - k - b, A.c - k - b);
+    fm W2 = sub(W, k + bw, 0, W.r - k - bw, W.c);
+    fm AL = sub(A, k, k, A.r - k, imin(nb, A.c - k));
+    unblockedQRT(AL, Twork);
+    const int tb = imin(nb, tau.r - k);
+    for (int i = 0; i < tb; i++) tau.d[k + i] = Twork.d[i + (intptr_t)i * Twork.ld];
+    updateWithQT(A12, A22, A11, A21, Twork, W2, 1);
+    k += b;
+  }
+}
+
+/* qrwy.go:474-497 (DecomposeQR) */
+int or_decompose_qr_fm(fm A, fm tau, fm W, int nb) {
+  if (nb == 0 || A.c <= nb) {
+    unblockedQR(A, tau);
+    return OR_OK;
+  }
+  double *tw = (double *)calloc((size_t)nb * nb, sizeof(double));
+  double *wa = NULL;
+  if (W.d == NULL) {
+    wa = (double *)calloc((size_t)A.c * nb, sizeof(double));
+    W = (fm){wa, A.c, nb, A.c};
+  } else if (W.c < nb || W.r < A.c) {
+    free(tw);
+    return OR_EWORKSMALL;
+  }
+  blockedQR(A, tau, (fm){tw, nb, nb, nb}, sub(W, 0, 0, A.c, nb), nb);
+  free(tw);
+  free(wa);
+  return OR_OK;
+}
+
+/* qrwy.go:517-538 (DecomposeQRT) */
+int or_decompose_qrt_fm(fm A, fm T, fm W, int nb) {
+  if (nb == 0 || A.c <= nb) {
+    unblockedQRT(A, T);
+    return OR_OK;
+  }
+  double *wa = NULL;
+  if (W.d == NULL) {
+    wa = (double *)calloc((size_t)A.c * nb, sizeof(double));
+    W = (fm){wa, A.c, nb, A.c};
+  } else if (W.c < nb || W.r < A.c) {
+    return OR_EWORKSMALL;
+  }
+  blockedQRT(A, T, sub(W, 0, 0, A.c, nb), nb);
+  free(wa);
+  return OR_OK;
+}
+
+/* qrwy.go:546-556 (BuildT) */
+int or_build_t_fm(fm T, fm A, fm tau) {
+  if (T.c < A.c || T.r < A.c) return OR_ETSMALL;
+  unblkQRBlockReflector(T, A, tau);
+  return OR_OK;
+}
+
+/* qrwym.go:382-462 (blockedMultQTLeft) */
+static void blockedMultQTLeft(fm C, fm A, fm T, fm W, int nb, int flags) {
+  if (flags & MTX_TRANS) {
+    /* top-left to bottom-right: Q^T C */
+    int kc = 0;
+    for (int k = 0; k < A.r && k < A.c; ) {
+      const int b = imin(nb, A.c - k), bt = imin(nb, T.c - k);
+      const int bc = imin(b, C.r - kc);
+      fm A11 = sub(A, k, k, b, b), A21 = sub(A, k + b, k, A.r - k - b, b);
+      fm T11 = sub(T, k, k, bt, bt);
+      fm C1 = sub(C, kc, 0, bc, C.c), C2 = sub(C, kc + bc, 0, C.r - kc - bc, C.c);
+      updateWithQT(C1, C2, A11, A21, T11, sub(W, 0, 0, C1.c, b), 1);
+      k += b;
+      kc += bc;
+    }
+  } else {
+    /* bottom-right to top-left: Q C; the A and C partitions start mb = rows - cols above
+     * the bottom, T's at its own bottom-right corner */
+    const int mb = A.r - A.c;
+    int ka = A.r - mb, kt = T.r, nc = C.r - mb;
+    int ca = A.c;
+    while (ka > 0 && ca > 0) {
+      const int b = imin(nb, ka), bt = imin(nb, kt);
+      const int bc = imin(b, nc);
+      fm A11 = sub(A, ka - b, ka - b, b, b), A21 = sub(A, ka, ka - b, A.r - ka, b);
+      fm T11 = sub(T, kt - bt, kt - bt, bt, bt);
+      fm C1 = sub(C, nc - bc, 0, bc, C.c), C2 = sub(C, nc, 0, C.r - nc, C.c);
+      updateWithQT(C1, C2, A11, A21, T11, sub(W, 0, 0, C1.c, b), 0);
+      ka -= b;
+      ca -= b;
+      kt -= bt;
+      nc -= bc;
+    }
+  }
+}
+
+/* qrwym.go:469-566 (blockedMultQTRight) */
+static void blockedMultQTRight(fm C, fm A, fm T, fm W, int nb, int flags) {
+  if (flags & MTX_TRANS) {
+    /* bottom-right to top-left: C Q^T */
+    const int mb = A.r - A.c, cb = C.c - A.c;
+    int ka = A.r - mb, kt = T.r, kc = C.c - cb;
+    int ca = A.c;
+    while (ka > 0 && ca > 0) {
+      const int b = imin(nb, ka), bt = imin(nb, kt), bc = imin(b, kc);
+      fm A11 = sub(A, ka - b, ka - b, b, b), A21 = sub(A, ka, ka - b, A.r - ka, b);
+      fm T11 = sub(T, kt - bt, kt - bt, bt, bt);
+      fm C1 = sub(C, 0, kc - bc, C.r, bc), C2 = sub(C, 0, kc, C.r, C.c - kc);
+      updateWithQTRight(C1, C2, A11, A21, T11, sub(W, 0, 0, C1.r, b), 1);
+      ka -= b;
+      ca -= b;
+      kt -= bt;
+      kc -= bc;
+    }
+  } else {
+    /* top-left to bottom-right: C Q */
+    int kc = 0;
+    for (int k = 0; k < A.r && k < A.c; ) {
+      const int b = imin(nb, A.c - k), bt = imin(nb, T.c - k), bc = imin(b, C.c - kc);
+      fm A11 = sub(A, k, k, b, b), A21 = sub(A, k + b, k, A.r - k - b, b);
+      fm T11 = sub(T, k, k, bt, bt);
+      fm C1 = sub(C, 0, kc, C.r, bc), C2 = sub(C, 0, kc + bc, C.r, C.c - kc - bc);
+      updateWithQTRight(C1, C2, A11, A21, T11, sub(W, 0, 0, C1.r, b), 0);
+      k += b;
+      kc += bc;
+    }
+  }
+}
+
+/* qrwym.go:646-688 (MultQT); W.d == NULL stands for a nil workspace */
+int or_mult_qt_fm(fm C, fm A, fm T, fm W, int flags, int nb) {
+  if (nb == 0) nb = T.c;
+  if (W.d == NULL) return OR_ENOWORK;
+  if (flags & MTX_RIGHT) {
+    if (C.c != A.r) return OR_ECQSIZE;
+    if (W.c < nb || W.r < C.r) return OR_EWORKSMALL;
+    blockedMultQTRight(C, A, T, sub(W, 0, 0, C.r, nb), nb, flags);
+  } else {
+    if (W.c < nb || W.r < C.c) return OR_EWORKSMALL;
+    blockedMultQTLeft(C, A, T, sub(W, 0, 0, C.c, nb), nb, flags);
+  }
+  return OR_OK;
+}
+
+/* qrwym.go:784-819 (SolveQRT).  With MTX_TRANS the rows of B below the first A.c are
+ * cleared before Q is applied (the reference's intent, qrwym.go:795-797). */
+int or_solve_qrt_fm(fm B, fm A, fm T, fm W, int flags, int nb) {
+  fm R = sub(A, 0, 0, A.c, A.c), BT = sub(B, 0, 0, A.c, B.c);
+  if (flags & MTX_TRANS) {
+    int rc = or_solve_trm_fm(BT, R, 1.0, MTX_LEFT | MTX_UPPER | MTX_TRANSA);
+    fm BB = sub(B, A.c, 0, B.r - A.c, B.c);
+    for (int j = 0; j < BB.c; j++)
+      for (int i = 0; i < BB.r; i++) BB.d[i + (intptr_t)j * BB.ld] = 0.0;
+    (void)rc;
+    return or_mult_qt_fm(B, A, T, W, MTX_LEFT, nb);
+  }
+  int rc = or_mult_qt_fm(B, A, T, W, MTX_LEFT | MTX_TRANS, nb);
+  if (rc) return rc;
+  return or_solve_trm_fm(BT, R, 1.0, MTX_LEFT | MTX_UPPER);
+}
+
 /* ---------------- flat C entry points for the ctypes harness ---------------- */
 
 #define FM(p, r, c, ld) ((fm){(p), (r), (c), (ld)})
@@ -664,4 +1002,28 @@ void or_blocking_params(int mb, int nb, int kb) {
   vpLen = kb;
   nB = nb;
   mB = mb;
+}
+/* QR entry points; a NULL W stands for the reference's nil workspace */
+int or_decompose_qrt(double *A, int ar, int ac, int lda, double *T, int tr, int tc, int ldt,
+                     double *W, int wr, int wc, int ldw, int nb) {
+  return or_decompose_qrt_fm(FM(A, ar, ac, lda), FM(T, tr, tc, ldt), FM(W, wr, wc, ldw), nb);
+}
+int or_decompose_qr(double *A, int ar, int ac, int lda, double *tau, int taur, double *W, int wr,
+                    int wc, int ldw, int nb) {
+  return or_decompose_qr_fm(FM(A, ar, ac, lda), FM(tau, taur, 1, taur > 0 ? taur : 1),
+                            FM(W, wr, wc, ldw), nb);
+}
+int or_build_t(double *T, int tr, int tc, int ldt, double *A, int ar, int ac, int lda, double *tau,
+               int taur) {
+  return or_build_t_fm(FM(T, tr, tc, ldt), FM(A, ar, ac, lda), FM(tau, taur, 1, taur > 0 ? taur : 1));
+}
+int or_mult_qt(double *C, int cr, int cc, int ldc, double *A, int ar, int ac, int lda, double *T,
+               int tr, int tc, int ldt, double *W, int wr, int wc, int ldw, int flags, int nb) {
+  return or_mult_qt_fm(FM(C, cr, cc, ldc), FM(A, ar, ac, lda), FM(T, tr, tc, ldt),
+                       FM(W, wr, wc, ldw), flags, nb);
+}
+int or_solve_qrt(double *B, int br, int bc, int ldb, double *A, int ar, int ac, int lda, double *T,
+                 int tr, int tc, int ldt, double *W, int wr, int wc, int ldw, int flags, int nb) {
+  return or_solve_qrt_fm(FM(B, br, bc, ldb), FM(A, ar, ac, lda), FM(T, tr, tc, ldt),
+                         FM(W, wr, wc, ldw), flags, nb);
 }

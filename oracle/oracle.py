@@ -33,6 +33,10 @@ ERRORS = {
     -5: "A, B size mismatch",
     -6: "X not a vector.",
     -7: "MultSym: size mismatch",
+    -13: "work space too small",
+    -14: "workspace not defined",
+    -15: "C*Q: C.Cols != A.Rows",
+    -16: "reflector matrix T too small",
 }
 
 
@@ -85,6 +89,11 @@ class Oracle:
         L.or_num_workers.argtypes = [i]
         L.or_blocking_params.argtypes = [i, i, i]
         L.or_blocking_params.restype = None
+        L.or_decompose_qrt.argtypes = M + M + M + [i]
+        L.or_decompose_qr.argtypes = M + [p, i] + [p, i, i, i] + [i]
+        L.or_build_t.argtypes = M + M + [p, i]
+        L.or_mult_qt.argtypes = M + M + M + M + [i, i]
+        L.or_solve_qrt.argtypes = M + M + M + M + [i, i]
 
     # each method returns the raw status code (0 = nil error)
     def Mult(self, C, A, B, alpha, beta, flags):
@@ -129,6 +138,46 @@ class Oracle:
     def SolveLU(self, B, A, pivots: np.ndarray, flags):
         assert pivots.dtype == np.int64 and pivots.flags.c_contiguous
         return self.lib.or_solve_lu(*view(B), *view(A), ctypes.c_void_p(pivots.ctypes.data), len(pivots), flags)
+
+    # QR (qrwy.go, qrwym.go); W=None is the reference's nil workspace
+    @staticmethod
+    def _wview(W):
+        if W is None:
+            return ctypes.c_void_p(0), 0, 0, 1
+        return view(W)
+
+    def DecomposeQRT(self, A, T, W, nb):
+        """qrwy.go:517: A = Q R in place (R on and above the diagonal, the reflectors below),
+        T the block reflector, Q = I - Y T Y^T"""
+        return self.lib.or_decompose_qrt(*view(A), *view(T), *self._wview(W), nb)
+
+    def DecomposeQR(self, A, tau: np.ndarray, W, nb):
+        """qrwy.go:474: LAPACK DGEQRF form (tau, no T)"""
+        assert tau.dtype == np.float64 and tau.flags.c_contiguous
+        return self.lib.or_decompose_qr(*view(A), ctypes.c_void_p(tau.ctypes.data), len(tau),
+                                        *self._wview(W), nb)
+
+    def BuildT(self, T, A, tau: np.ndarray):
+        """qrwy.go:546: block reflector T from the reflectors in A and tau"""
+        assert tau.dtype == np.float64 and tau.flags.c_contiguous
+        return self.lib.or_build_t(*view(T), *view(A), ctypes.c_void_p(tau.ctypes.data), len(tau))
+
+    def MultQT(self, C, A, T, W, flags, nb):
+        """qrwym.go:646: C = Q C, Q^T C (MO_TRANS), C Q, C Q^T (MO_RIGHT)"""
+        return self.lib.or_mult_qt(*view(C), *view(A), *view(T), *self._wview(W), flags, nb)
+
+    def SolveQRT(self, B, A, T, W, flags, nb):
+        """qrwym.go:784: least squares min ||A X - B|| or (MO_TRANS) min-norm A^T X = B"""
+        return self.lib.or_solve_qrt(*view(B), *view(A), *view(T), *self._wview(W), flags, nb)
+
+    def GemvBetaOnce(self, on: bool) -> bool:
+        """Port only: make the transposed GEMV apply beta once (BLAS semantics) instead of
+        once per 68-row block as calgo/dmvec_gemv.c:379-393 does; returns the old mode"""
+        if self.which != "port":
+            raise RuntimeError("the reference's own kernels have no such switch")
+        f = self.lib.or_gemv_beta_once
+        f.argtypes = [ctypes.c_int]
+        return bool(f(1 if on else 0))
 
     def NumWorkers(self, n: int) -> int:
         return self.lib.or_num_workers(n)

@@ -199,3 +199,118 @@ def test_reference_gemv_unaligned_bug_is_real(ref_oracle, oracle):
     lu, piv = sl.lu_factor(A)
     assert np.array_equal(p1, piv) and rel(a1, lu) <= 1e-12
     assert rel(a2, lu) > 1e-3
+
+
+# ---------------- QR (qrwy.go, qrwym.go) ----------------
+
+GOLDEN_QR = os.path.join(os.path.dirname(__file__), "golden", "qr.npz")
+
+
+@pytest.fixture(scope="module")
+def golden_qr():
+    z = np.load(GOLDEN_QR)
+    cases = {}
+    for k in z.files:
+        name, field = k.split("/")
+        cases.setdefault(name, {})[field] = z[k]
+    return cases
+
+
+def qr_names(prefix):
+    z = np.load(GOLDEN_QR)
+    return sorted({k.split("/")[0] for k in z.files if k.startswith(prefix)})
+
+
+@pytest.mark.parametrize("name", qr_names("qrt_"))
+def test_golden_decompose_qrt(oracle, golden_qr, name):
+    """the port in the reference's GEMV semantics reproduces the reference, the 200 x 120
+    case (beta applied per 68-row block) included"""
+    c = golden_qr[name]
+    N = c["A"].shape[1]
+    R, T = F(c["A"]), F(np.zeros((N, N)))
+    assert oracle.DecomposeQRT(R, T, F(np.zeros((N, max(int(c["nb"]), 1)))), int(c["nb"])) == 0
+    assert rel(R, c["QR"]) <= 1e-12
+    assert rel(np.triu(T), np.triu(c["T"])) <= 1e-12
+
+
+@pytest.mark.parametrize("name", qr_names("qr_"))
+def test_golden_decompose_qr_build_t(oracle, golden_qr, name):
+    c = golden_qr[name]
+    N = c["A"].shape[1]
+    R, tau = F(c["A"]), np.zeros(N)
+    assert oracle.DecomposeQR(R, tau, F(np.zeros((N, max(int(c["nb"]), 1)))), int(c["nb"])) == 0
+    assert rel(R, c["QR"]) <= 1e-12 and np.abs(tau - c["tau"]).max() <= 1e-13
+    T = F(np.zeros((N, N)))
+    assert oracle.BuildT(T, F(c["QR"]), c["tau"].copy()) == 0
+    assert rel(np.triu(T), np.triu(c["T"])) <= 1e-12
+
+
+@pytest.mark.parametrize("name", qr_names("multqt_") + qr_names("solveqrt_"))
+def test_golden_mult_solve_qrt(oracle, golden_qr, name):
+    c = golden_qr[name]
+    if name == "solveqrt_minnorm":
+        QR, T = F(c["QR"]), F(c["T"])
+    else:
+        QR, T = F(golden_qr["qrt_60x40_nb12"]["QR"]), F(golden_qr["qrt_60x40_nb12"]["T"])
+    if name.startswith("multqt_"):
+        R = F(c["C"])
+        assert oracle.MultQT(R, QR, T, F(np.zeros((60, 40))), int(c["flags"]), int(c["nb"])) == 0
+    else:
+        R = F(c["B"])
+        assert oracle.SolveQRT(R, QR, T, F(np.zeros((30, 40))), int(c["flags"]), int(c["nb"])) == 0
+    assert rel(R, c["R"]) <= 1e-12
+
+
+def test_reference_qrt_gemv_beta_quirk(oracle, golden_qr):
+    """The reference's T recurrence goes through a transposed GEMV that scales y by beta
+    once per 68-row block (calgo/dmvec_gemv.c:379-393), with beta = -tau (qrwy.go:66): its
+    200 x 120 factorization is not A = Q R (golden, from its own kernels).  With one beta
+    per product (BLAS semantics, what the device computes) the same drivers give A = Q R."""
+    c = golden_qr["qrt_200x120_nb32"]
+    A, QR, T = c["A"], c["QR"], c["T"]
+    M, N = A.shape
+
+    def recon(QR, T):
+        Y = np.tril(QR, -1) + np.eye(M, N)
+        R = np.vstack([np.triu(QR[:N]), np.zeros((M - N, N))])
+        return R - Y @ (np.triu(T) @ (Y.T @ R))
+
+    assert rel(recon(QR, T), A) > 1e-2  # the reference's own result
+    old = oracle.GemvBetaOnce(True)
+    try:
+        R2, T2 = F(A), F(np.zeros((N, N)))
+        assert oracle.DecomposeQRT(R2, T2, F(np.zeros((N, 32))), 32) == 0
+    finally:
+        oracle.GemvBetaOnce(old)
+    assert rel(recon(R2, T2), A) <= 100 * M * EPS
+    q, r = np.linalg.qr(A)
+    assert rel(np.abs(np.triu(R2[:N])), np.abs(r)) <= 1e-12
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_port_vs_ref_qr(oracle, ref_oracle, seed):
+    rng = np.random.default_rng(100 + seed)
+    M, N, nb = 150, 90, 16
+    A = colmajor(rng.uniform(-1, 1, (M, N)), ld=even_ld(M))
+    outs = []
+    for o in (oracle, ref_oracle):
+        R, T = colmajor(A, ld=even_ld(M)), colmajor(np.zeros((N, N)))
+        assert o.DecomposeQRT(R, T, colmajor(np.zeros((N, nb))), nb) == 0
+        C = colmajor(rng.uniform(-1, 1, (M, 20)) if not outs else outs[0][2].copy())
+        C0 = C.copy(order="F")
+        assert o.MultQT(C, R, T, colmajor(np.zeros((20, N))), LEFT | 0x80, 0) == 0
+        outs.append((R, T, C0, C))
+    assert rel(outs[0][0], outs[1][0]) <= 1e-12
+    assert rel(np.triu(outs[0][1]), np.triu(outs[1][1])) <= 1e-12
+    assert rel(outs[0][3], outs[1][3]) <= 1e-12
+
+
+def test_oracle_qr_errors(oracle):
+    A = colmajor(np.ones((10, 8)))
+    assert oracle.DecomposeQRT(A, colmajor(np.zeros((8, 8))), colmajor(np.zeros((7, 2))), 2) == -13
+    C = colmajor(np.ones((10, 3)))
+    T = colmajor(np.zeros((8, 8)))
+    assert oracle.MultQT(C, A, T, None, LEFT, 0) == -14
+    assert oracle.MultQT(colmajor(np.ones((3, 9))), A, T, colmajor(np.zeros((3, 8))), RIGHT, 0) == -15
+    assert oracle.MultQT(C, A, T, colmajor(np.zeros((3, 4))), LEFT, 0) == -13
+    assert oracle.BuildT(colmajor(np.zeros((7, 8))), A, np.zeros(8)) == -16
