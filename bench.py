@@ -141,6 +141,17 @@ def run_case(args):
                              reps=max(1, args.steps), tune=tune)
         print(json.dumps({"case": args.case, **res}), flush=True)
         return 0
+    elif kind == "dgeqrt":
+        # dgeqrt:N -- DecomposeQRT of an N x N iid N(0,1) matrix
+        n = dims[0]
+        A0 = mo.matrix(n, n)
+        A0.normal_(generator=g)
+        A, T = mo.matrix(n, n), mo.matrix(n, n)
+
+        def fn():
+            A.copy_(A0)
+            assert mo.DecomposeQRT(A, T, None, 0)[1] is None
+        flops = 4.0 * n ** 3 / 3.0
     elif kind in ("dpotrf", "dgetrf"):
         n = dims[0]
         A0 = mo.matrix(n, n)
@@ -177,20 +188,22 @@ def run_case(args):
 
 
 def kappa_spd(mo, n, kappa, seed, dev):
-    """A = Q diag(s) Q^T, Q from the Householder QR of an iid N(0,1) matrix (seed), s
-    log-spaced from 1 to kappa; built on the device in FP64 (torch QR is harness only)."""
+    """A = Q diag(s) Q^T, Q from the Householder QR of an iid N(0,1) matrix (seed) -- this
+    package's DecomposeQRT + MultQT (qrwy.go:517, qrwym.go:646) applied to the identity --
+    and s log-spaced from 1 to kappa; built on the device in FP64."""
     import torch
     g = torch.Generator(device=dev).manual_seed(seed)
-    M = torch.randn(n, n, dtype=torch.float64, device=dev, generator=g)
-    Q, R = torch.linalg.qr(M)
-    del M
-    Q *= torch.sign(torch.diagonal(R)).unsqueeze(0)
-    del R
+    F = mo.matrix(n, n)
+    F.copy_(torch.randn(n, n, dtype=torch.float64, device=dev, generator=g))
+    T = mo.matrix(n, n)
+    assert mo.DecomposeQRT(F, T, None, 0)[1] is None
+    Qc = mo.matrix(n, n)
+    Qc.zero_()
+    Qc.diagonal().fill_(1.0)
+    assert mo.MultQT(Qc, F, T, mo.matrix(n, 128), mo.LEFT, 128) is None
+    del F, T
     s = torch.logspace(0, float(torch.log10(torch.tensor(kappa))), n, dtype=torch.float64,
                        device=dev)
-    Qc = mo.matrix(n, n)
-    Qc.copy_(Q)
-    del Q
     QS = mo.matrix(n, n)
     QS.copy_(Qc * s.unsqueeze(0))
     A = mo.matrix(n, n)
@@ -198,6 +211,54 @@ def kappa_spd(mo, n, kappa, seed, dev):
     del QS, Qc
     A.copy_((A + A.t()) * 0.5)
     return A
+
+
+def qr_leg(mo, dev, n, fp64_peak, nrhs=64, reps=3):
+    """DecomposeQRT (qrwy.go:517) of an n x n iid N(0,1) matrix and the least-squares
+    SolveQRT (qrwym.go:784) of nrhs right-hand sides with it, FP64 on the device, timed with
+    CUDA events; ||A - Q R|| / ||A|| from MultQT on R."""
+    import torch
+    g = torch.Generator(device=dev).manual_seed(6)
+    A0 = mo.matrix(n, n)
+    A0.copy_(torch.randn(n, n, dtype=torch.float64, device=dev, generator=g))
+    B0 = mo.matrix(n, nrhs)
+    B0.uniform_(-1.0, 1.0, generator=g)
+    A, T, B = mo.matrix(n, n), mo.matrix(n, n), mo.matrix(n, nrhs)
+    W = mo.matrix(nrhs, n)  # the reference's workspace rule: B.cols x T.cols
+    fts, sts = [], []
+    for it in range(reps + 1):
+        A.copy_(A0)
+        T.zero_()
+        B.copy_(B0)
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record()
+        assert mo.DecomposeQRT(A, T, None, 0)[1] is None
+        ev[1].record()
+        assert mo.SolveQRT(B, A, T, W, 0, 0) is None
+        ev[2].record()
+        torch.cuda.synchronize()
+        if it:
+            fts.append(ev[0].elapsed_time(ev[1]))
+            sts.append(ev[1].elapsed_time(ev[2]))
+    f_ms, s_ms = min(fts), min(sts)
+    R = mo.matrix(n, n)
+    R.copy_(torch.triu(A))
+    assert mo.MultQT(R, A, T, mo.matrix(n, 128), mo.LEFT, 128) is None
+    residual = float(torch.linalg.norm(R - A0) / torch.linalg.norm(A0))
+    del R
+    Rb = B0.clone()
+    assert mo.Mult(Rb, A0, B, -1.0, 1.0, 0) is None
+    berr = float(torch.linalg.norm(Rb) / (torch.linalg.norm(A0) * torch.linalg.norm(B)
+                                          + torch.linalg.norm(B0)))
+    fp64 = fp64_peak
+    geqrf, with_t = 4.0 * n ** 3 / 3.0, 2.0 * n ** 3
+    return {"n": n, "factor_ms": f_ms, "factor_tflops": geqrf / (f_ms * 1e-3) / 1e12,
+            "factor_tflops_incl_T": with_t / (f_ms * 1e-3) / 1e12,
+            "frac_fp64_peak_incl_T": with_t / (f_ms * 1e-3) / 1e12 / fp64,
+            "solve_ms": s_ms, "nrhs": nrhs, "residual_A_minus_QR": residual, "solve_berr": berr,
+            "flops": "4n^3/3 (DGEQRF count); incl_T adds the n^3 x 2/3 of the full block "
+                     "reflector T that DecomposeQRT returns"}
 
 
 def mixed_leg(mo, n, nrhs, kappas, precs, dev, reps=2):
@@ -943,6 +1004,10 @@ def main():
                     "reference": "tests/golden/n16384.npz (oracle/_ref DecomposeLU, nb=64)"}
         del L0, Lb0, LA, LB
         torch.cuda.empty_cache()
+        extras["qr"] = {}
+        for nq in sorted({min(8192, n), n}):
+            extras["qr"][f"n={nq}"] = qr_leg(mo, dev, nq, fp64_peak)
+            torch.cuda.empty_cache()
         # the mixed-precision configuration: n in {8192, 16384}, 16 RHS, kappa sweep, both
         # split formats (A = Q diag(s) Q^T, Q from Householder QR, s log-spaced 1..kappa)
         extras["mixed_ir"] = {}

@@ -249,7 +249,9 @@ MO_API int mo_build_t(mo_ctx *ctx, mo_matrix T, mo_matrix A, mo_matrix tau);
 
 /* MultQT(C, A, T, W, flags, nb), qrwym.go:646-688: C = Q C (MO_LEFT or no side bit),
  * Q^T C (with MO_TRANS), C Q (MO_RIGHT), C Q^T (MO_RIGHT|MO_TRANS); Q from mo_decompose_qrt's
- * A and T, applied nb reflectors at a time in the reference's order (nb == 0: T.cols).
+ * A and T, in the reference's order of reflectors.  nb (0: T.cols) sizes the W check as in
+ * the reference; the device applies 256 reflectors at a time whatever nb is (results agree
+ * to rounding).
  * W NULL -> MO_ENOWORK; MO_RIGHT with C.cols != A.rows -> MO_ECQSIZE; W smaller than
  * C.rows (MO_RIGHT) or C.cols (left) x nb -> MO_EWORKSMALL; left with C.rows != A.rows ->
  * MO_EABSIZE (unchecked by the reference).  Asynchronous. */

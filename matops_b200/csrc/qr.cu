@@ -45,6 +45,7 @@ constexpr int kQrBlock = 128;   // columns per trailing update (the K of its pro
 constexpr int kQrThreads = 256;
 constexpr int kQrRowsPerCta = 256;  // panel rows per CTA aimed at
 constexpr int kQrMaxSmem = 220 * 1024;
+constexpr int kQrApply = 256;   // reflectors per block when Q is applied to a matrix
 
 struct QrScratch {
   double *part;        // [2][grid][32]: per-CTA column products, double-buffered by column
@@ -445,6 +446,10 @@ int qr_factor(mo_ctx *ctx, View A, View T, double *tau, int64_t tau_inc) {
   int rc = qr_workspace(ctx, m, k, (int64_t)max(n, 1) * kQrBlock, grid, q);
   if (rc) return rc;
   const View Yv{q.Y, m, k, m}, Tv{q.Tw, k, k, k}, Zv{q.Z, k, kQrPanel, k};
+  // the products read T's blocks below the diagonal and Y's rows above each panel inside
+  // a 128-column block as zeros (the panels write only their own rows and T blocks)
+  MO_CUDA_TRY(cudaMemsetAsync(q.Tw, 0, (size_t)k * k * sizeof(double), ctx->stream));
+  MO_CUDA_TRY(cudaMemsetAsync(q.Y, 0, (size_t)m * k * sizeof(double), ctx->stream));
   for (int kb = 0; kb < k; kb += kQrBlock) {
     const int bo = min(kQrBlock, k - kb);
     for (int kp = kb; kp < kb + bo; kp += kQrPanel) {
@@ -497,8 +502,11 @@ int qr_build_t(mo_ctx *ctx, int m, int k, const double *tau_c, QrWork &q) {
 }
 
 // C = Q C, Q^T C (MO_TRANS), C Q (MO_RIGHT), C Q^T (MO_RIGHT|MO_TRANS) with Q = I - Y T Y^T
-// of k reflectors (q.Y, q.Tw), in blocks of nb reflectors ordered as qrwym.go:382-566
-// takes them: forward for Q^T C and C Q, backward (aligned at k) for Q C and C Q^T.
+// of k reflectors (q.Y, q.Tw), in blocks of nb reflectors in the order qrwym.go:382-566
+// takes them: forward for Q^T C and C Q, backward (aligned at k) for Q C and C Q^T.  Each
+// block reads only its reflectors' rows s..m, so blocks of a few hundred reflectors take
+// about a third of the flops of one block of all k (which multiplies the zeros above Y's
+// diagonal and the whole of T).
 int qr_apply(mo_ctx *ctx, View C, int m, int k, int flags, int nb, QrWork &q) {
   const bool right = (flags & MO_RIGHT) != 0, trans = (flags & MO_TRANS) != 0;
   const bool forward = right ? !trans : trans;
@@ -608,7 +616,8 @@ int apply_q(mo_ctx *ctx, View C, View A, View T, const double *tau, int64_t tau_
   const int m = A.rows, k = std::min(A.rows, A.cols);
   if (k == 0 || C.rows == 0 || C.cols == 0) return MO_OK;
   if (k > 65535) return MO_EINVAL;
-  if (nb <= 0 || nb > k) nb = k;
+  // the device's own blocking (results agree with any nb to rounding)
+  nb = std::min(mo::kQrApply, k);
   const int64_t wsize = std::max((int64_t)std::max(C.rows, C.cols) * nb, (int64_t)k);
   mo::QrWork q;
   int rc = mo::qr_prepare(ctx, A, k, T, wsize, q);

@@ -928,6 +928,102 @@ int or_solve_qrt_fm(fm B, fm A, fm T, fm W, int flags, int nb) {
   return or_solve_trm_fm(BT, R, 1.0, MTX_LEFT | MTX_UPPER);
 }
 
+/* house.go:152-183 (applyHHTo2x1, side LEFT) with the caller's w1 */
+static void applyHHTo2x1Left(double tval, fm v, fm a1, fm A2, fm w1) {
+  if (tval == 0.0) return;
+  const int n = a1.r * a1.c;
+  for (int k = 0; k < n; k++) *vel(w1, k) = *vel(a1, k);
+  MVMult(w1, A2, v, 1.0, 1.0, MTX_TRANSA);
+  Scale(w1, tval);
+  for (int k = 0; k < n; k++) *vel(a1, k) -= *vel(w1, k);
+  MVRankUpdate(A2, v, w1, -1.0);
+}
+
+/* qrwyk.go:20-90 (unblockedBuildQ, LAPACK DORG2R): Q = H(0)...H(k-1) in place from the last
+ * column to the first; tau(j) is element j of tau (a column vector) counted from its end as
+ * the reference's partitions do.  "zero the upper part" (a01.SetIndexes(0.0)) is taken to
+ * clear the column above the diagonal (DORG2R). */
+static void unblockedBuildQ(fm A, fm tau, fm w) {
+  int k = A.c, nt = tau.r * tau.c;
+  while (k > 0 && nt > 0) {
+    const int j = k - 1;
+    const double t = *vel(tau, nt - 1);
+    fm a21 = sub(A, j + 1, j, A.r - j - 1, 1), a12 = sub(A, j, j + 1, 1, A.c - j - 1);
+    fm A22 = sub(A, j + 1, j + 1, A.r - j - 1, A.c - j - 1);
+    applyHHTo2x1Left(t, a21, a12, A22, sub(w, 0, 0, 1, A.c - j - 1));
+    Scale(a21, -t);
+    A.d[j + (intptr_t)j * A.ld] = 1.0 - t;
+    for (int i = 0; i < j; i++) A.d[i + (intptr_t)j * A.ld] = 0.0;
+    k--;
+    nt--;
+  }
+}
+
+/* qrwyk.go:93-150 (blockedBuildQ, DORGQR) and :153-229 (blockedBuildQT): blocks of nb
+ * columns from the bottom-right; T11 from tau by unblkQRBlockReflector (BuildQ) or from T's
+ * diagonal block (BuildQT), the trailing columns take Q_b, the block's own columns the
+ * unblocked form */
+static void blockedBuildQ_(fm A, fm tau, fm T, fm W, int nb) {
+  double *twork = NULL;
+  fm Tk = {NULL, 0, 0, 1};
+  if (!T.d) {
+    twork = (double *)calloc((size_t)nb * nb, sizeof(double));
+    Tk = (fm){twork, nb, nb, nb};
+  }
+  int k = A.c, nt = T.d ? T.r : tau.r * tau.c;
+  while (k > 0 && A.r > 0) {
+    const int b = imin(nb, k), bt = T.d ? imin(nb, nt) : imin(nb, nt);
+    fm A11 = sub(A, k - b, k - b, b, b), A12 = sub(A, k - b, k, b, A.c - k);
+    fm A21 = sub(A, k, k - b, A.r - k, b), A22 = sub(A, k, k, A.r - k, A.c - k);
+    fm AL = sub(A, k - b, k - b, A.r - k + b, b);
+    fm T11, tau1;
+    double *diag = NULL;
+    if (T.d) {
+      T11 = sub(T, nt - bt, nt - bt, bt, bt);
+      diag = (double *)malloc(sizeof(double) * (bt > 0 ? bt : 1));
+      for (int i = 0; i < bt; i++) diag[i] = T11.d[i + (intptr_t)i * T11.ld];
+      tau1 = (fm){diag, bt, 1, bt > 0 ? bt : 1};
+    } else {
+      tau1 = sub(tau, nt - bt, 0, bt, 1);
+      T11 = sub(Tk, 0, 0, b, b);
+      unblkQRBlockReflector(T11, AL, tau1);
+    }
+    updateWithQT(A12, A22, A11, A21, T11, sub(W, 0, 0, A12.c, b), 0);
+    unblockedBuildQ(AL, tau1, sub(W, 0, 0, 1, b));
+    for (int j = k - b; j < k; j++)
+      for (int i = 0; i < k - b; i++) A.d[i + (intptr_t)j * A.ld] = 0.0;
+    free(diag);
+    k -= b;
+    nt -= bt;
+  }
+  free(twork);
+}
+
+/* qrwyk.go:232-267 (BuildQ) */
+int or_build_q_fm(fm A, fm tau, fm W, int nb) {
+  if (nb != 0 && W.d == NULL) return OR_ENOWORK;
+  if (nb != 0 && (W.c < nb || W.r < A.c)) return OR_EWORKSMALL;
+  if (A.r < A.c) return OR_EABSIZE;
+  if (nb == 0) {
+    double *w = (double *)calloc((size_t)(A.c > 0 ? A.c : 1), sizeof(double));
+    unblockedBuildQ(A, tau, (fm){w, 1, A.c, 1});
+    free(w);
+  } else {
+    blockedBuildQ_(A, tau, (fm){NULL, 0, 0, 1}, sub(W, 0, 0, A.c, nb), nb);
+  }
+  return OR_OK;
+}
+
+/* qrwyk.go:278-293 (BuildQT) */
+int or_build_qt_fm(fm A, fm T, fm W, int nb) {
+  if (nb == 0) nb = A.c;
+  if (W.d == NULL) return OR_ENOWORK;
+  if (W.c < nb || W.r < A.c) return OR_EWORKSMALL;
+  if (A.r < A.c) return OR_EABSIZE;
+  blockedBuildQ_(A, (fm){NULL, 0, 0, 1}, T, sub(W, 0, 0, A.c, nb), nb);
+  return OR_OK;
+}
+
 /* ---------------- flat C entry points for the ctypes harness ---------------- */
 
 #define FM(p, r, c, ld) ((fm){(p), (r), (c), (ld)})
@@ -1026,4 +1122,13 @@ int or_solve_qrt(double *B, int br, int bc, int ldb, double *A, int ar, int ac, 
                  int tr, int tc, int ldt, double *W, int wr, int wc, int ldw, int flags, int nb) {
   return or_solve_qrt_fm(FM(B, br, bc, ldb), FM(A, ar, ac, lda), FM(T, tr, tc, ldt),
                          FM(W, wr, wc, ldw), flags, nb);
+}
+int or_build_q(double *A, int ar, int ac, int lda, double *tau, int taur, double *W, int wr, int wc,
+               int ldw, int nb) {
+  return or_build_q_fm(FM(A, ar, ac, lda), FM(tau, taur, 1, taur > 0 ? taur : 1),
+                       FM(W, wr, wc, ldw), nb);
+}
+int or_build_qt(double *A, int ar, int ac, int lda, double *T, int tr, int tc, int ldt, double *W,
+                int wr, int wc, int ldw, int nb) {
+  return or_build_qt_fm(FM(A, ar, ac, lda), FM(T, tr, tc, ldt), FM(W, wr, wc, ldw), nb);
 }

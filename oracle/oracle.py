@@ -94,6 +94,8 @@ class Oracle:
         L.or_build_t.argtypes = M + M + [p, i]
         L.or_mult_qt.argtypes = M + M + M + M + [i, i]
         L.or_solve_qrt.argtypes = M + M + M + M + [i, i]
+        L.or_build_q.argtypes = M + [p, i] + [p, i, i, i] + [i]
+        L.or_build_qt.argtypes = M + M + M + [i]
 
     # each method returns the raw status code (0 = nil error)
     def Mult(self, C, A, B, alpha, beta, flags):
@@ -169,6 +171,16 @@ class Oracle:
     def SolveQRT(self, B, A, T, W, flags, nb):
         """qrwym.go:784: least squares min ||A X - B|| or (MO_TRANS) min-norm A^T X = B"""
         return self.lib.or_solve_qrt(*view(B), *view(A), *view(T), *self._wview(W), flags, nb)
+
+    def BuildQ(self, A, tau: np.ndarray, W, nb):
+        """qrwyk.go:232: A := the first A.cols columns of Q = H(0)...H(k-1) (DORGQR)"""
+        assert tau.dtype == np.float64 and tau.flags.c_contiguous
+        return self.lib.or_build_q(*view(A), ctypes.c_void_p(tau.ctypes.data), len(tau),
+                                   *self._wview(W), nb)
+
+    def BuildQT(self, A, T, W, nb):
+        """qrwyk.go:278: BuildQ with the reflector block T of DecomposeQRT"""
+        return self.lib.or_build_qt(*view(A), *view(T), *self._wview(W), nb)
 
     def GemvBetaOnce(self, on: bool) -> bool:
         """Port only: make the transposed GEMV apply beta once (BLAS semantics) instead of

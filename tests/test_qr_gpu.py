@@ -40,6 +40,8 @@ def lapack():
 
 def dev(gpu, a):
     import torch
+    if a.ndim != 2 or (a.shape[0] > 1 and a.strides[0] != 8):
+        a = np.asfortranarray(a)
     ld = a.strides[1] // 8 if a.shape[1] > 1 else max(a.shape[0], 1)
     t = gpu.matrix(max(ld, 1), max(a.shape[1], 1))
     t.zero_()
@@ -66,7 +68,13 @@ def qr_bound(m, n, A):
 def test_decompose_qrt(gpu, ref, lapack, rng, m, n, nb):
     A0 = colmajor(rng.uniform(-1, 1, (m, n)), ld=even_ld(m) + 2)
     k = min(m, n)
-    T0 = colmajor(rng.uniform(-1, 1, (k + 3, k + 3)))  # strict lower part must stay
+    # T exactly k x k: the reference partitions T by its own size, so a larger T puts its
+    # last block out of step with A's.  Its upper triangle starts at zero, as in the
+    # reference's tests: where a reflector is the identity (tau = 0, e.g. a square matrix's
+    # last column) the reference leaves T's column above the diagonal as it was and its
+    # blocked recurrence reads it; the device writes the zeros of the dlarft definition.
+    # The strict lower part must stay untouched.
+    T0 = colmajor(np.tril(rng.uniform(-1, 1, (k, k)), -1))
     Ag, Tg = dev(gpu, A0), dev(gpu, T0)
     Wg = gpu.matrix(max(n, 1), max(nb, 1))
     A_, err = gpu.DecomposeQRT(Ag, Tg, Wg, nb)
