@@ -263,6 +263,18 @@ MO_API int mo_mult_qt(mo_ctx *ctx, mo_matrix C, mo_matrix A, mo_matrix T, mo_mat
 MO_API int mo_mult_q(mo_ctx *ctx, mo_matrix C, mo_matrix A, mo_matrix tau, mo_matrix W, int flags,
                      int nb);
 
+/* BuildQ(A, tau, W, nb), qrwyk.go:232-267 (DORGQR): A (m x n, m >= n, the reflectors of
+ * mo_decompose_qr) := the first n columns of Q, columns of the identity taking the
+ * reflectors in reverse order.  nb != 0 with W NULL -> MO_ENOWORK, W smaller than A.cols x nb
+ * -> MO_EWORKSMALL; m < n -> MO_EABSIZE.  tau's first n entries are used (the reference
+ * counts them from tau's end).  The reference's "zero the upper part" (qrwyk.go:75, :143) is
+ * taken to clear the entries above the diagonal, as DORGQR does. */
+MO_API int mo_build_q(mo_ctx *ctx, mo_matrix A, mo_matrix tau, mo_matrix W, int nb);
+
+/* BuildQT(A, T, W, nb), qrwyk.go:278-293: mo_build_q with Q from mo_decompose_qrt's T
+ * (nb == 0: A.cols; W NULL -> MO_ENOWORK). */
+MO_API int mo_build_qt(mo_ctx *ctx, mo_matrix A, mo_matrix T, mo_matrix W, int nb);
+
 /* SolveQRT(B, A, T, W, flags, nb), qrwym.go:784-819, A m x n with m >= n: least squares
  * X = argmin ||A X - B|| into B's first n rows (B = Q^T B, then R^-1); with MO_TRANS the
  * minimum-norm solution of A^T X = B (B's first n rows = R^-T B, the rows below cleared,

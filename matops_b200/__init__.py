@@ -13,5 +13,5 @@ from .api import (  # noqa: F401
     IRInfo, SolveCHOLMixed, LPGemm, BATCH_CHOL, BATCH_LU, BATCH_MAX_N, BatchPlan,
     DecomposeCHOLAdjoint, DecomposeCHOLAdjointBatched, SolveCHOLAdjoint, SetSpinLimit, Mirror,
     context, MultSym, MultTrm, RankUpdate2Sym, UpdateTrm, InverseTrm,
-    DecomposeQRT, DecomposeQR, BuildT, MultQT, MultQ, SolveQRT, SolveQR,
+    DecomposeQRT, DecomposeQR, BuildT, MultQT, MultQ, SolveQRT, SolveQR, BuildQ, BuildQT,
 )

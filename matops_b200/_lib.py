@@ -68,6 +68,8 @@ def lib() -> ctypes.CDLL:
         "mo_mult_q": [p, M, M, M, M, i, i],
         "mo_solve_qrt": [p, M, M, M, M, i, i],
         "mo_solve_qr": [p, M, M, M, M, i, i],
+        "mo_build_q": [p, M, M, M, i],
+        "mo_build_qt": [p, M, M, M, i],
         "mo_mirror_create": [p, p, i64, ctypes.POINTER(p)],
         "mo_mirror_destroy": [p],
         "mo_mirror_find": [p, ctypes.POINTER(p), ctypes.POINTER(i64)],

@@ -228,6 +228,16 @@ def BuildT(T, A, tau):
     return T, _err(_lib.lib().mo_build_t(context(), view(T), view(A), _vec(tau)))
 
 
+def BuildQ(A, tau, W, nb: int):
+    """qrwyk.go:232 -- A := the first A.cols columns of Q (DORGQR); returns (A, err)"""
+    return A, _err(_lib.lib().mo_build_q(context(), view(A), _vec(tau), _wview(W), nb))
+
+
+def BuildQT(A, T, W, nb: int):
+    """qrwyk.go:278 -- BuildQ with Q from DecomposeQRT's T; returns (A, err)"""
+    return A, _err(_lib.lib().mo_build_qt(context(), view(A), view(T), _wview(W), nb))
+
+
 def MultQT(C, A, T, W, flags: int, nb: int):
     """qrwym.go:646 -- C = Q C, Q^T C (TRANS), C Q (RIGHT), C Q^T (RIGHT|TRANS)"""
     return _err(_lib.lib().mo_mult_qt(context(), view(C), view(A), view(T), _wview(W), flags, nb))

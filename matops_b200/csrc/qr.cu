@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(kQrThreads, 1)
                           // 32 different banks
   double *slab = smem;    // [w][S]
   double *red = smem + (size_t)kQrPanel * S;  // [8][32] per-warp partial sums
-  __shared__ double s_q[32], s_w[32], s_z[32], s_t[32 * 33], s_scal[4];
+  __shared__ double s_w[32], s_z[32], s_t[32 * 33], s_scal[4];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int G = gridDim.x, cta = blockIdx.x;
   const int r0 = cta * rpc, nr = max(0, min(rpc, R - r0));
@@ -155,23 +155,21 @@ __global__ void __launch_bounds__(kQrThreads, 1)
   for (int j = 0; j < kmax; ++j) {
     const int par = j & 1;
     if (!qr_grid_barrier(sc.bar, (unsigned)(j + 1) * G, status, sc.abort_flag)) return;
-    // sum the CTAs' partials in one fixed order (every CTA gets the same values)
+    // sum the CTAs' partials in one fixed order (every CTA gets the same values); warp 0
+    // fetches the pivot row in the same round trip
     {
       double acc = 0.0;
       for (int g = warp; g < G; g += 8) acc += __ldcg(&sc.part[((size_t)par * G + g) * 32 + lane]);
       red[warp * 32 + lane] = acc;
     }
+    const double prc = warp == 0 ? __ldcg(&sc.prow[par * 32 + lane]) : 0.0;
     __syncthreads();
-    if (tid < 32) {
-      double s = 0.0;
+    if (warp == 0) {
+      double q = 0.0;
 #pragma unroll
-      for (int g = 0; g < 8; ++g) s += red[g * 32 + tid];
-      s_q[tid] = s;
-    }
-    __syncthreads();
-    if (tid == 0) {
-      // computeHouseholder (house.go:55-78) on [alpha; x] with ||x||^2 = q_j
-      const double s = s_q[j], alpha = __ldcg(&sc.prow[par * 32 + j]);
+      for (int g = 0; g < 8; ++g) q += red[g * 32 + lane];
+      // computeHouseholder (house.go:55-78) on [alpha; x] with ||x||^2 = q_j, in every lane
+      const double s = __shfl_sync(0xffffffffu, q, j), alpha = __shfl_sync(0xffffffffu, prc, j);
       double tau = 0.0, denom = 1.0, beta = alpha;
       if (s != 0.0) {
         const double sign = signbit(alpha) ? -1.0 : 1.0;
@@ -179,19 +177,18 @@ __global__ void __launch_bounds__(kQrThreads, 1)
         denom = alpha - beta;
         tau = (beta - alpha) / beta;
       }
-      s_scal[0] = tau;
-      s_scal[1] = denom;
-      s_scal[2] = beta;
+      // p_c = row j + v^T (rows below j) of column c, with v = x / denom
+      const double p = lane < w ? prc + q / denom : 0.0;
+      s_w[lane] = tau * p;   // applyHouseholder's w1 (columns right of j)
+      s_z[lane] = -tau * p;  // the dlarft vector (columns left of j)
+      if (lane == 0) {
+        s_scal[0] = tau;
+        s_scal[1] = denom;
+        s_scal[2] = beta;
+      }
     }
     __syncthreads();
     const double tau = s_scal[0], denom = s_scal[1], beta = s_scal[2];
-    if (tid < 32) {
-      // p_c = row j + v^T (rows below j) of column c, with v = x / denom
-      const double p = tid < w ? __ldcg(&sc.prow[par * 32 + tid]) + s_q[tid] / denom : 0.0;
-      s_w[tid] = tau * p;   // applyHouseholder's w1 (columns right of j)
-      s_z[tid] = -tau * p;  // the dlarft vector (columns left of j)
-    }
-    __syncthreads();
     if (tau != 0.0) {
       // H(j) applied to this CTA's rows: v = x / denom, rows below j lose v_i w, row j
       // loses w and takes beta on the diagonal
@@ -235,6 +232,48 @@ __global__ void __launch_bounds__(kQrThreads, 1)
       const int c = e / w, r = e - c * w;
       Tb[r + (int64_t)c * ldt] = r <= c ? s_t[c * 33 + r] : 0.0;
     }
+}
+
+// The 128-column block's T from its four 32 x 32 panel blocks (on the diagonal of Tb, ld
+// ldt, zeros below) and the Gram matrix Zin = Y_b^T Y_b (ld ldz): for panel p the rows above
+// it are T(0:32p, p) = -T(0:32p, 0:32p) Zin(0:32p, p) T_pp (qrwy.go:433-453 at panel
+// granularity).  One CTA; the block lives in shared memory.
+constexpr int kQrTBlockSmem = (128 * 129 + 96 * 33) * 8;
+__global__ void __launch_bounds__(256) qr_t_block_kernel(double *Tb, int64_t ldt,
+                                                         const double *Zin, int64_t ldz, int bo) {
+  extern __shared__ double sm[];
+  double *T = sm;               // [128][129], T(r, c) at c * 129 + r
+  double *M1 = sm + 128 * 129;  // [32][33] x rows: M1(r, c) at c * 97 + r (r < 96)
+  const int tid = threadIdx.x;
+  for (int e = tid; e < bo * bo; e += 256) {
+    const int c = e / bo, r = e - c * bo;
+    T[c * 129 + r] = Tb[r + (int64_t)c * ldt];
+  }
+  __syncthreads();
+  for (int p0 = kQrPanel; p0 < bo; p0 += kQrPanel) {
+    const int w = min(kQrPanel, bo - p0), R = p0;
+    // M1 = Zin(0:R, p0:p0+w) T(p0:p0+w, p0:p0+w)
+    for (int e = tid; e < R * w; e += 256) {
+      const int c = e / R, r = e - c * R;
+      double acc = 0.0;
+      for (int l = 0; l <= c; ++l)
+        acc = fma(Zin[r + (int64_t)(p0 + l) * ldz], T[(p0 + c) * 129 + p0 + l], acc);
+      M1[c * 97 + r] = acc;
+    }
+    __syncthreads();
+    // T(0:R, p0:p0+w) = -T(0:R, 0:R) M1  (T upper triangular)
+    for (int e = tid; e < R * w; e += 256) {
+      const int c = e / R, r = e - c * R;
+      double acc = 0.0;
+      for (int l = r; l < R; ++l) acc = fma(T[l * 129 + r], M1[c * 97 + l], acc);
+      T[(p0 + c) * 129 + r] = -acc;
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < bo * bo; e += 256) {
+    const int c = e / bo, r = e - c * bo;
+    if (r < (c / kQrPanel) * kQrPanel) Tb[r + (int64_t)c * ldt] = T[c * 129 + r];
+  }
 }
 
 // Y (m x k) = the explicit unit lower trapezoid of A's reflectors (zeros above)
@@ -312,8 +351,8 @@ struct QrWork {
   double *Tw = nullptr;  // k x k dense T, zeros below the diagonal (ld k)
   double *W = nullptr;   // products' scratch, wsize doubles each
   double *W2 = nullptr;
-  double *Z = nullptr;   // k x 32
-  double *X = nullptr;   // k x 32
+  double *Z = nullptr;   // k x 128
+  double *X = nullptr;   // k x 128
   QrScratch sc{};
 };
 
@@ -322,7 +361,7 @@ size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 // Carve the context workspace into the buffers above (panel scratch for `grid` CTAs).
 int qr_workspace(mo_ctx *ctx, int m, int k, int64_t wsize, int grid, QrWork &q) {
   const size_t by = align256((size_t)m * k * 8), bt = align256((size_t)k * k * 8);
-  const size_t bw = align256((size_t)wsize * 8), bz = align256((size_t)k * kQrPanel * 8);
+  const size_t bw = align256((size_t)wsize * 8), bz = align256((size_t)k * kQrBlock * 8);
   const size_t bp = align256((size_t)2 * grid * 32 * 8), br = align256(2 * 32 * 8);
   const size_t total = by + bt + 2 * bw + 2 * bz + bp + br + 256;
   char *ws = nullptr;
@@ -445,7 +484,7 @@ int qr_factor(mo_ctx *ctx, View A, View T, double *tau, int64_t tau_inc) {
   QrWork q;
   int rc = qr_workspace(ctx, m, k, (int64_t)max(n, 1) * kQrBlock, grid, q);
   if (rc) return rc;
-  const View Yv{q.Y, m, k, m}, Tv{q.Tw, k, k, k}, Zv{q.Z, k, kQrPanel, k};
+  const View Yv{q.Y, m, k, m}, Tv{q.Tw, k, k, k};
   // the products read T's blocks below the diagonal and Y's rows above each panel inside
   // a 128-column block as zeros (the panels write only their own rows and T blocks)
   MO_CUDA_TRY(cudaMemsetAsync(q.Tw, 0, (size_t)k * k * sizeof(double), ctx->stream));
@@ -455,25 +494,30 @@ int qr_factor(mo_ctx *ctx, View A, View T, double *tau, int64_t tau_inc) {
     for (int kp = kb; kp < kb + bo; kp += kQrPanel) {
       const int bp = min(kQrPanel, kb + bo - kp);
       if ((rc = panel(ctx, A, kp, bp, q, k))) return rc;
-      if (kp > 0) {
-        // Z = Y(kp:m, 0:kp)^T Y(kp:m, kp:kp+bp): the panel's rows above kp are zero
-        const View Z = Zv.sub(0, 0, kp, bp);
-        if ((rc = gemm(ctx, Z, Yv.sub(kp, 0, m - kp, kp), true, Yv.sub(kp, kp, m - kp, bp),
-                       false, 1.0, 0.0)))
-          return rc;
-        if ((rc = t_columns(ctx, k, kp, bp, View{q.Z, kp, bp, k}, q))) return rc;
-      }
+      // the rest of this 128-column block takes the panel's reflectors
       const int c0 = kp + bp, rest = kb + bo - c0;
       if (rest > 0 &&
           (rc = apply_left_t(ctx, A.sub(kp, c0, m - kp, rest), Yv.sub(kp, kp, m - kp, bp),
                              Tv.sub(kp, kp, bp, bp), q)))
         return rc;
     }
+    const View Yb = Yv.sub(kb, kb, m - kb, bo), Tb = Tv.sub(kb, kb, bo, bo);
+    if (bo > kQrPanel) {
+      // the block's T: its panels' T blocks joined through Y_b^T Y_b
+      const View Zin{q.W2, bo, bo, bo};
+      if ((rc = gemm(ctx, Zin, Yb, true, Yb, false, 1.0, 0.0))) return rc;
+      if ((rc = mo_smem_attr((const void *)qr_t_block_kernel, kQrTBlockSmem))) return rc;
+      qr_t_block_kernel<<<1, 256, kQrTBlockSmem, ctx->stream>>>(Tb.d, k, q.W2, bo, bo);
+      MO_CUDA_TRY(cudaGetLastError());
+    }
+    if (kb > 0) {
+      // T's rows above the block: -T(0:kb, 0:kb) (Y(kb:m, 0:kb)^T Y_b) T_b
+      const View Z{q.Z, kb, bo, kb};
+      if ((rc = gemm(ctx, Z, Yv.sub(kb, 0, m - kb, kb), true, Yb, false, 1.0, 0.0))) return rc;
+      if ((rc = t_columns(ctx, k, kb, bo, Z, q))) return rc;
+    }
     const int c0 = kb + bo, nt = n - c0;
-    if (nt > 0 &&
-        (rc = apply_left_t(ctx, A.sub(kb, c0, m - kb, nt), Yv.sub(kb, kb, m - kb, bo),
-                           Tv.sub(kb, kb, bo, bo), q)))
-      return rc;
+    if (nt > 0 && (rc = apply_left_t(ctx, A.sub(kb, c0, m - kb, nt), Yb, Tb, q))) return rc;
   }
   if (T.d && (rc = t_out(ctx, q, k, T, nullptr))) return rc;
   if (tau) {
@@ -574,6 +618,33 @@ void qr_zero_rows(mo_ctx *ctx, View B, int r0) {
     const dim3 g((B.rows - r0 + 255) / 256, std::min(65535, B.cols - c0));
     qr_zero_rows_kernel<<<g, 256, 0, ctx->stream>>>(B.at(0, c0), B.ld, r0, B.rows);
   }
+}
+
+// A (m x n) := the first n columns of the identity
+__global__ void __launch_bounds__(256) qr_eye_kernel(double *A, int64_t lda, int m) {
+  const int i = blockIdx.x * 256 + threadIdx.x, c = blockIdx.y;
+  if (i < m) A[i + (int64_t)c * lda] = i == c ? 1.0 : 0.0;
+}
+
+// BuildQ / BuildQT's device part: A (m x n, m >= n) := Q [I_n; 0] with Q from A's n
+// reflectors and T (or tau)
+int qr_build_q(mo_ctx *ctx, View A, View T, const double *tau, int64_t tau_inc) {
+  const int m = A.rows, n = A.cols;
+  if (n == 0 || m == 0) return MO_OK;
+  if (n > kQrMaxCols) return MO_EINVAL;
+  const int b = std::min(kQrApply, n);
+  QrWork q;
+  int rc = qr_prepare(ctx, A, n, T, std::max((int64_t)n * b, (int64_t)n), q);
+  if (rc) return rc;
+  if (!T.d) {
+    qr_tau_copy(ctx, tau, tau_inc, n, q.W2);
+    if ((rc = qr_build_t(ctx, m, n, q.W2, q))) return rc;
+  }
+  if ((rc = launch_grid2(m, n, [&](dim3 g) {
+         qr_eye_kernel<<<g, 256, 0, ctx->stream>>>(A.d, A.ld, m);
+       })))
+    return rc;
+  return qr_apply(ctx, A, m, n, MO_LEFT, b, q);
 }
 
 }  // namespace mo
@@ -766,6 +837,36 @@ int mo_solve_qr(mo_ctx *ctx, mo_matrix Bm, mo_matrix Am, mo_matrix taum, mo_matr
   int64_t inc = 1;
   if ((rc = tau_view(taum, k, &tau, &inc))) return rc;
   return solve_q(ctx, B, A, View{nullptr, 0, 0, 1}, tau, inc, Wm, flags, nb, nb != 0);
+}
+
+// qrwyk.go:232-267
+int mo_build_q(mo_ctx *ctx, mo_matrix Am, mo_matrix taum, mo_matrix Wm, int nb) {
+  int rc = mo::enter(ctx);
+  if (rc) return rc;
+  View A;
+  if ((rc = mo::to_view(Am, A))) return rc;
+  if (nb != 0 && is_nil(Wm)) return MO_ENOWORK;
+  if (nb != 0 && (Wm.cols < nb || Wm.rows < A.cols)) return MO_EWORKSMALL;
+  if (A.rows < A.cols) return MO_EABSIZE;
+  double *tau = nullptr;
+  int64_t inc = 1;
+  if ((rc = tau_view(taum, A.cols, &tau, &inc))) return rc;
+  return mo::qr_build_q(ctx, A, View{nullptr, 0, 0, 1}, tau, inc);
+}
+
+// qrwyk.go:278-293
+int mo_build_qt(mo_ctx *ctx, mo_matrix Am, mo_matrix Tm, mo_matrix Wm, int nb) {
+  int rc = mo::enter(ctx);
+  if (rc) return rc;
+  View A, T;
+  if ((rc = mo::to_view(Am, A)) || (rc = mo::to_view(Tm, T))) return rc;
+  if (nb == 0) nb = A.cols;
+  if (is_nil(Wm)) return MO_ENOWORK;
+  if (Wm.cols < nb || Wm.rows < A.cols) return MO_EWORKSMALL;
+  if (A.rows < A.cols) return MO_EABSIZE;
+  if (T.rows < A.cols || T.cols < A.cols) return MO_ETSMALL;
+  if (A.cols > 0 && !T.d) return MO_EINVAL;
+  return mo::qr_build_q(ctx, A, T, nullptr, 0);
 }
 
 }  // extern "C"

@@ -4,7 +4,8 @@ Runs the restated Go drivers of qrwy.go / qrwym.go / house.go (oracle/drivers.c)
 against hrautila/matops's calgo/ C files compiled from their sources
 (oracle/_ref/libmatops_ref.so, `make -C oracle ref`), on seeded uniform [0, 1) inputs of
 the shapes of the reference's own QR tests (qr_test.go:13-205: 60 x 40 with nb 4 and 12,
-30 right-hand sides, a 40 x 40 minimum-norm system) and on a 200 x 120 case where more
+30 right-hand sides, a 40 x 40 minimum-norm system, BuildQ / BuildQT of qrwyk.go) and on
+a 200 x 120 case where more
 than 68 rows lie below the first columns, so that the reference's transposed GEMV scales
 by beta once per 68-row block (calgo/dmvec_gemv.c:379-393).  Every case stores its inputs
 and the reference outputs.
@@ -75,6 +76,19 @@ def main():
     R = F(B)
     assert ref.SolveQRT(R, QRs, Ts, F(np.zeros((30, 40))), TRANS, 12) == 0
     put("solveqrt_minnorm", B=B, R=R, flags=TRANS, nb=12, QR=QRs, T=Ts, A=As)
+    # BuildQ / BuildQT (qrwyk.go:232, :278) on fresh 60 x 40 factorizations
+    for nb in (0, 12):
+        A = F(rng.uniform(size=(60, 40)))
+        R, tau = F(A), np.zeros(40)
+        assert ref.DecomposeQR(R, tau, None, 0) == 0
+        Q = F(R)
+        assert ref.BuildQ(Q, tau, F(np.zeros((40, max(nb, 1)))), nb) == 0
+        put(f"buildq_{nb}", A=A, QR=R, tau=tau, Q=Q, nb=nb)
+        R2, T2 = F(A), F(np.zeros((40, 40)))
+        assert ref.DecomposeQRT(R2, T2, None, 0) == 0
+        Q2 = F(R2)
+        assert ref.BuildQT(Q2, T2, F(np.zeros((40, 40))), nb) == 0
+        put(f"buildqt_{nb}", A=A, QR=R2, T=T2, Q=Q2, nb=nb)
     np.savez_compressed(os.path.join(HERE, "qr.npz"), **out)
     print(f"wrote {len(out)} arrays")
 

@@ -314,3 +314,16 @@ def test_oracle_qr_errors(oracle):
     assert oracle.MultQT(colmajor(np.ones((3, 9))), A, T, colmajor(np.zeros((3, 8))), RIGHT, 0) == -15
     assert oracle.MultQT(C, A, T, colmajor(np.zeros((3, 4))), LEFT, 0) == -13
     assert oracle.BuildT(colmajor(np.zeros((7, 8))), A, np.zeros(8)) == -16
+
+
+@pytest.mark.parametrize("name", qr_names("buildq_") + qr_names("buildqt_"))
+def test_golden_build_q(oracle, golden_qr, name):
+    c = golden_qr[name]
+    Q = F(c["QR"])
+    if name.startswith("buildqt_"):
+        assert oracle.BuildQT(Q, F(c["T"]), F(np.zeros((40, 40))), int(c["nb"])) == 0
+    else:
+        assert oracle.BuildQ(Q, c["tau"].copy(), F(np.zeros((40, max(int(c["nb"]), 1)))),
+                             int(c["nb"])) == 0
+    assert rel(Q, c["Q"]) <= 1e-12
+    assert fro(Q.T @ Q - np.eye(40)) <= 100 * 60 * EPS

@@ -247,3 +247,33 @@ def test_decompose_qrt_large_properties(gpu, rng, n):
     assert gpu.MultQT(E, A, T, W, LEFT, 0) is None
     assert gpu.MultQT(E, A, T, W, LEFT | TRANS, 0) is None
     assert (torch.linalg.norm(E - E0) / 8.0).item() <= 8 * n * EPS
+
+
+@pytest.mark.parametrize("m,n,nb", [(60, 40, 0), (60, 40, 12), (500, 300, 32), (1024, 1024, 0)])
+def test_build_q(gpu, ref, lapack, rng, m, n, nb):
+    import torch
+    A0 = colmajor(rng.uniform(-1, 1, (m, n)))
+    o = oracle_for(m, ref, lapack) if nb else ref  # the unblocked BuildQ uses no beta != 1 GEMV
+    # BuildQ from DecomposeQR's reflectors (the same device reflectors for both)
+    Ag = dev(gpu, A0)
+    tau = torch.zeros(n, dtype=torch.float64, device="cuda")
+    assert gpu.DecomposeQR(Ag, tau, None, 0)[1] is None
+    Ah, th = host(Ag), tau.cpu().numpy().copy()
+    _, err = gpu.BuildQ(Ag, tau, gpu.matrix(n, max(nb, 1)), nb)
+    assert err is None
+    Qr = Ah.copy(order="F")
+    assert o.BuildQ(Qr, th, np.zeros((n, max(nb, 1)), order="F"), nb) == 0
+    Qh = host(Ag)
+    assert fro(Qh - Qr) <= 32 * m * EPS * np.sqrt(n)
+    assert fro(Qh.T @ Qh - np.eye(n)) <= 32 * m * EPS * np.sqrt(n)
+    assert fro(Qh @ np.triu(Ah[:n]) - A0) <= 32 * m * EPS * fro(A0)
+    # BuildQT from DecomposeQRT
+    Ag2, Tg = dev(gpu, A0), dev(gpu, np.zeros((n, n)))
+    assert gpu.DecomposeQRT(Ag2, Tg, None, 0)[1] is None
+    R2 = np.triu(host(Ag2)[:n])
+    _, err = gpu.BuildQT(Ag2, Tg, gpu.matrix(n, n), nb)
+    assert err is None
+    Q2 = host(Ag2)
+    assert fro(Q2 @ R2 - A0) <= 32 * m * EPS * fro(A0)
+    _, err = gpu.BuildQ(dev(gpu, colmajor(np.ones((3, 5)))), tau[:5], None, 0)
+    assert err is not None and err.code == -5
