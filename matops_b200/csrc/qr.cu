@@ -276,6 +276,70 @@ __global__ void __launch_bounds__(256) qr_t_block_kernel(double *Tb, int64_t ldt
   }
 }
 
+// Split-K product for a small C with a long K: C (M x N) = A^T B, A (K x M) and B (K x N)
+// column-major.  Grid (chunks, tiles): each CTA multiplies one chunk of K rows for one
+// 64 x 64 tile of C (16 x 16 threads, 4 x 4 outputs each, 32-row slabs staged in shared
+// memory) and stores its partial tile; tn_reduce_kernel sums the chunks in order.  The
+// engine would run such a product as one 128 x 128 tile whose K is split over ~100 CTAs
+// and summed by one of them.
+constexpr int kTnTile = 64, kTnSlab = 32;
+__global__ void __launch_bounds__(256) tn_partial_kernel(const double *A, int64_t lda,
+                                                         const double *B, int64_t ldb, int M,
+                                                         int N, int K, int kc, double *part) {
+  __shared__ double As[kTnSlab][kTnTile + 1], Bs[kTnSlab][kTnTile + 1];
+  const int tiles_m = (M + kTnTile - 1) / kTnTile;
+  const int tile = blockIdx.y, tm = tile % tiles_m, tn = tile / tiles_m;
+  const int m0 = tm * kTnTile, n0 = tn * kTnTile;
+  const int k_begin = blockIdx.x * kc, k_end = min(K, k_begin + kc);
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  double acc[4][4] = {};
+  for (int k0 = k_begin; k0 < k_end; k0 += kTnSlab) {
+    // slab rows k0..k0+31 of A's columns m0.. and B's columns n0.. (zeros past the edges)
+    for (int e = tid; e < kTnSlab * kTnTile; e += 256) {
+      const int kk = e & (kTnSlab - 1), c = e / kTnSlab;
+      const int k = k0 + kk;
+      As[kk][c] = (k < k_end && m0 + c < M) ? A[k + (int64_t)(m0 + c) * lda] : 0.0;
+      Bs[kk][c] = (k < k_end && n0 + c < N) ? B[k + (int64_t)(n0 + c) * ldb] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < kTnSlab; ++kk) {
+      double a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+  double *out = part + ((size_t)blockIdx.x * gridDim.y + tile) * (kTnTile * kTnTile);
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) out[(ty + 16 * i) + (tx + 16 * j) * kTnTile] = acc[i][j];
+}
+
+// C = alpha * (sum of the chunks' partial tiles, in chunk order) + beta * C (beta == 0: C
+// not read)
+__global__ void __launch_bounds__(256) tn_reduce_kernel(const double *part, int chunks, int tiles,
+                                                        int M, int N, double *C, int64_t ldc,
+                                                        double alpha, double beta) {
+  const int64_t e = (int64_t)blockIdx.x * 256 + threadIdx.x;
+  if (e >= (int64_t)M * N) return;
+  const int i = (int)(e % M), j = (int)(e / M);
+  const int tiles_m = (M + kTnTile - 1) / kTnTile;
+  const int tile = (i / kTnTile) + (j / kTnTile) * tiles_m;
+  const int off = (i % kTnTile) + (j % kTnTile) * kTnTile;
+  double s = 0.0;
+  for (int c = 0; c < chunks; ++c) s += part[((size_t)c * tiles + tile) * (kTnTile * kTnTile) + off];
+  double *cp = C + i + (int64_t)j * ldc;
+  *cp = beta == 0.0 ? alpha * s : fma(alpha, s, beta * *cp);
+}
+
 // Y (m x k) = the explicit unit lower trapezoid of A's reflectors (zeros above)
 __global__ void __launch_bounds__(256) qr_expand_y_kernel(const double *A, int64_t lda, int m,
                                                           int k, double *Y, int64_t ldy) {
@@ -358,14 +422,21 @@ struct QrWork {
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
+// bytes of the buffers below (panel scratch for `grid` CTAs)
+size_t qr_workspace_bytes(int m, int k, int64_t wsize, int grid) {
+  const size_t by = align256((size_t)m * k * 8), bt = align256((size_t)k * k * 8);
+  const size_t bw = align256((size_t)wsize * 8), bz = align256((size_t)k * kQrBlock * 8);
+  const size_t bp = align256((size_t)2 * grid * 32 * 8), br = align256(2 * 32 * 8);
+  return by + bt + 2 * bw + 2 * bz + bp + br + 256;
+}
+
 // Carve the context workspace into the buffers above (panel scratch for `grid` CTAs).
 int qr_workspace(mo_ctx *ctx, int m, int k, int64_t wsize, int grid, QrWork &q) {
   const size_t by = align256((size_t)m * k * 8), bt = align256((size_t)k * k * 8);
   const size_t bw = align256((size_t)wsize * 8), bz = align256((size_t)k * kQrBlock * 8);
   const size_t bp = align256((size_t)2 * grid * 32 * 8), br = align256(2 * 32 * 8);
-  const size_t total = by + bt + 2 * bw + 2 * bz + bp + br + 256;
   char *ws = nullptr;
-  int rc = workspace(ctx, total, (void **)&ws);
+  int rc = workspace(ctx, qr_workspace_bytes(m, k, wsize, grid), (void **)&ws);
   if (rc) return rc;
   q.Y = (double *)ws;
   ws += by;
@@ -440,15 +511,49 @@ int t_columns(mo_ctx *ctx, int k, int kp, int bp, View Zsrc, QrWork &q) {
   return rc;
 }
 
+// C = alpha * A^T B + beta * C: split-K kernels when C is small and K long, else the
+// engine (its stream-K scratch doubles as the partial-tile buffer: same stream, in order)
+int tn_product(mo_ctx *ctx, View C, View A, View B, double alpha, double beta,
+               double *part = nullptr) {
+  const int M = C.rows, N = C.cols, K = A.rows;
+  if (M <= 0 || N <= 0) return MO_OK;
+  const int tiles = ((M + kTnTile - 1) / kTnTile) * ((N + kTnTile - 1) / kTnTile);
+  const size_t cap = gemm_partial_bytes(ctx->sms) / sizeof(double) / (kTnTile * kTnTile);
+  if (K < 1024 || tiles > 16 || K <= 0) {
+    GemmOpts o;
+    o.stream_k = part == nullptr;  // a caller's buffer: the product may overlap another
+    return gemm_ex(ctx, C, A, true, B, false, alpha, beta, o);
+  }
+  if (!part) part = ctx->sk_partial;
+  // chunks of at least 128 rows, about two CTAs per SM, within the partial buffer
+  int chunks = std::max(1, std::min<int>(K / 128, (2 * ctx->sms + tiles - 1) / tiles));
+  chunks = std::min<int>(chunks, (int)(cap / tiles));
+  const int kc = ((K + chunks - 1) / chunks + kTnSlab - 1) / kTnSlab * kTnSlab;
+  chunks = (K + kc - 1) / kc;
+  ProfScope ps;
+  prof_begin(ctx, ps, MO_PROF_GEMM);
+  tn_partial_kernel<<<dim3(chunks, tiles), 256, 0, ctx->stream>>>(A.d, A.ld, B.d, B.ld, M, N, K,
+                                                                    kc, part);
+  const int64_t mn = (int64_t)M * N;
+  tn_reduce_kernel<<<(unsigned)((mn + 255) / 256), 256, 0, ctx->stream>>>(
+      part, chunks, tiles, M, N, C.d, C.ld, alpha, beta);
+  prof_end(ctx, ps, 2.0 * M * N * (double)K, 8.0 * ((double)K * (M + N) + 2.0 * M * N));
+  MO_CUDA_TRY(cudaGetLastError());
+  return MO_OK;
+}
+
 // C (rows s.. of A's columns right of a block) = Q_b^T C for the block's reflectors:
 // W = C^T Y_b, W = W T_b, C -= Y_b W^T (qrwy.go:266-303 with transpose)
-int apply_left_t(mo_ctx *ctx, View C, const View &Yb, const View &Tb, QrWork &q) {
+int apply_left_t(mo_ctx *ctx, View C, const View &Yb, const View &Tb, QrWork &q,
+                 int max_ctas = 0) {
   const int nc = C.cols, b = Yb.cols;
   if (nc <= 0 || b <= 0) return MO_OK;
   const View W{q.W, nc, b, nc}, W2{q.W2, nc, b, nc};
-  int rc = gemm(ctx, W, C, true, Yb, false, 1.0, 0.0);
-  if (!rc) rc = gemm(ctx, W2, W, false, Tb, false, 1.0, 0.0);
-  if (!rc) rc = gemm(ctx, C, Yb, false, W2, true, -1.0, 1.0);
+  GemmOpts o;
+  o.max_ctas = max_ctas;
+  int rc = tn_product(ctx, W, C, Yb, 1.0, 0.0);
+  if (!rc) rc = gemm_ex(ctx, W2, W, false, Tb, false, 1.0, 0.0, o);
+  if (!rc) rc = gemm_ex(ctx, C, Yb, false, W2, true, -1.0, 1.0, o);
   return rc;
 }
 
@@ -473,8 +578,44 @@ __global__ void qr_tau_in_kernel(const double *tau, int64_t inc, int k, double *
 
 }  // namespace
 
+// One 128-column block [kb, kb + bo): its 32-column panels, the rest of the block after each
+// panel, the block's T (the panels' T blocks joined through Y_b^T Y_b) and T's rows above
+// it, all on the context's stream.
+int factor_block(mo_ctx *ctx, View A, int kb, int bo, int k, QrWork &q) {
+  const int m = A.rows;
+  const View Yv{q.Y, m, k, m}, Tv{q.Tw, k, k, k};
+  int rc;
+  for (int kp = kb; kp < kb + bo; kp += kQrPanel) {
+    const int bp = min(kQrPanel, kb + bo - kp);
+    if ((rc = panel(ctx, A, kp, bp, q, k))) return rc;
+    // the rest of the block takes the panel's reflectors
+    const int c0 = kp + bp, rest = kb + bo - c0;
+    if (rest > 0 &&
+        (rc = apply_left_t(ctx, A.sub(kp, c0, m - kp, rest), Yv.sub(kp, kp, m - kp, bp),
+                           Tv.sub(kp, kp, bp, bp), q)))
+      return rc;
+  }
+  const View Yb = Yv.sub(kb, kb, m - kb, bo), Tb = Tv.sub(kb, kb, bo, bo);
+  if (bo > kQrPanel) {
+    const View Zin{q.W2, bo, bo, bo};
+    if ((rc = tn_product(ctx, Zin, Yb, Yb, 1.0, 0.0))) return rc;
+    if ((rc = mo_smem_attr((const void *)qr_t_block_kernel, kQrTBlockSmem))) return rc;
+    qr_t_block_kernel<<<1, 256, kQrTBlockSmem, ctx->stream>>>(Tb.d, k, q.W2, bo, bo);
+    MO_CUDA_TRY(cudaGetLastError());
+  }
+  if (kb > 0) {
+    // T's rows above the block: -T(0:kb, 0:kb) (Y(kb:m, 0:kb)^T Y_b) T_b
+    const View Z{q.Z, kb, bo, kb};
+    if ((rc = tn_product(ctx, Z, Yv.sub(kb, 0, m - kb, kb), Yb, 1.0, 0.0))) return rc;
+    if ((rc = t_columns(ctx, k, kb, bo, Z, q))) return rc;
+  }
+  return MO_OK;
+}
+
 // The device part of DecomposeQRT / DecomposeQR: A (m x n) factored in place; T's upper
-// k x k triangle written when T.d, tau (k entries, stride tau_inc) when tau.
+// k x k triangle written when T.d, tau (k entries, stride tau_inc) when tau.  (Factoring
+// the next block on a second stream beside the trailing update was measured slower: the
+// update then runs without the panel's SMs and the T products without stream-K.)
 int qr_factor(mo_ctx *ctx, View A, View T, double *tau, int64_t tau_inc) {
   const int m = A.rows, n = A.cols, k = min(m, n);
   if (k == 0) return MO_OK;
@@ -491,33 +632,11 @@ int qr_factor(mo_ctx *ctx, View A, View T, double *tau, int64_t tau_inc) {
   MO_CUDA_TRY(cudaMemsetAsync(q.Y, 0, (size_t)m * k * sizeof(double), ctx->stream));
   for (int kb = 0; kb < k; kb += kQrBlock) {
     const int bo = min(kQrBlock, k - kb);
-    for (int kp = kb; kp < kb + bo; kp += kQrPanel) {
-      const int bp = min(kQrPanel, kb + bo - kp);
-      if ((rc = panel(ctx, A, kp, bp, q, k))) return rc;
-      // the rest of this 128-column block takes the panel's reflectors
-      const int c0 = kp + bp, rest = kb + bo - c0;
-      if (rest > 0 &&
-          (rc = apply_left_t(ctx, A.sub(kp, c0, m - kp, rest), Yv.sub(kp, kp, m - kp, bp),
-                             Tv.sub(kp, kp, bp, bp), q)))
-        return rc;
-    }
-    const View Yb = Yv.sub(kb, kb, m - kb, bo), Tb = Tv.sub(kb, kb, bo, bo);
-    if (bo > kQrPanel) {
-      // the block's T: its panels' T blocks joined through Y_b^T Y_b
-      const View Zin{q.W2, bo, bo, bo};
-      if ((rc = gemm(ctx, Zin, Yb, true, Yb, false, 1.0, 0.0))) return rc;
-      if ((rc = mo_smem_attr((const void *)qr_t_block_kernel, kQrTBlockSmem))) return rc;
-      qr_t_block_kernel<<<1, 256, kQrTBlockSmem, ctx->stream>>>(Tb.d, k, q.W2, bo, bo);
-      MO_CUDA_TRY(cudaGetLastError());
-    }
-    if (kb > 0) {
-      // T's rows above the block: -T(0:kb, 0:kb) (Y(kb:m, 0:kb)^T Y_b) T_b
-      const View Z{q.Z, kb, bo, kb};
-      if ((rc = gemm(ctx, Z, Yv.sub(kb, 0, m - kb, kb), true, Yb, false, 1.0, 0.0))) return rc;
-      if ((rc = t_columns(ctx, k, kb, bo, Z, q))) return rc;
-    }
+    if ((rc = factor_block(ctx, A, kb, bo, k, q))) return rc;
     const int c0 = kb + bo, nt = n - c0;
-    if (nt > 0 && (rc = apply_left_t(ctx, A.sub(kb, c0, m - kb, nt), Yb, Tb, q))) return rc;
+    if (nt > 0 && (rc = apply_left_t(ctx, A.sub(kb, c0, m - kb, nt), Yv.sub(kb, kb, m - kb, bo),
+                                     Tv.sub(kb, kb, bo, bo), q)))
+      return rc;
   }
   if (T.d && (rc = t_out(ctx, q, k, T, nullptr))) return rc;
   if (tau) {
@@ -561,7 +680,7 @@ int qr_apply(mo_ctx *ctx, View C, int m, int k, int flags, int nb, QrWork &q) {
     if (!right) {
       const int nc = C.cols;
       const View Cs = C.sub(s, 0, m - s, nc), W{q.W, nc, b, nc}, W2{q.W2, nc, b, nc};
-      int r = gemm(ctx, W, Cs, true, Yb, false, 1.0, 0.0);
+      int r = tn_product(ctx, W, Cs, Yb, 1.0, 0.0);
       if (!r) r = gemm(ctx, W2, W, false, Tb, !trans, 1.0, 0.0);
       if (!r) r = gemm(ctx, Cs, Yb, false, W2, true, -1.0, 1.0);
       return r;
