@@ -141,6 +141,19 @@ def run_case(args):
                              reps=max(1, args.steps), tune=tune)
         print(json.dumps({"case": args.case, **res}), flush=True)
         return 0
+    elif kind == "dsytrf":
+        # dsytrf:N -- DecomposeBK (Bunch-Kaufman, LOWER) of an N x N symmetric uniform matrix
+        n = dims[0]
+        A0 = mo.matrix(n, n)
+        A0.uniform_(-1.0, 1.0, generator=g)
+        A0.copy_(A0 + A0.t())
+        A, W = mo.matrix(n, n), mo.matrix(n, 2)
+        piv = torch.zeros(n, dtype=torch.int64, device="cuda")
+
+        def fn():
+            A.copy_(A0)
+            assert mo.DecomposeBK(A, W, piv, LOWER, 0)[1] is None
+        flops = n ** 3 / 3.0
     elif kind == "dgeqrt":
         # dgeqrt:N -- DecomposeQRT of an N x N iid N(0,1) matrix
         n = dims[0]

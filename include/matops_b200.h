@@ -63,6 +63,10 @@ extern "C" {
 #define MO_ENOWORK (-14)     /* "workspace not defined"                  qrwym.go:652 */
 #define MO_ECQSIZE (-15)     /* "C*Q: C.Cols != A.Rows"                  qrwym.go:656 */
 #define MO_ETSMALL (-16)     /* "reflector matrix T too small"           qrwy.go:550 */
+#define MO_ELDLWORK (-17)    /* "No workspace for blocking invocation"   ldlnp.go:224 */
+#define MO_EZERODIAG (-18)   /* "zero value on diagonal"                 ldl.go:62 ("zero on
+                                diagonal." for UPPER, ldl.go:334)                     */
+#define MO_EBKWORK (-19)     /* "Workspace too small"                    ldlbk.go:1121 */
 
 typedef struct mo_ctx mo_ctx;
 
@@ -287,6 +291,51 @@ MO_API int mo_solve_qrt(mo_ctx *ctx, mo_matrix B, mo_matrix A, mo_matrix T, mo_m
  * applies Q as mo_solve_qrt does. */
 MO_API int mo_solve_qr(mo_ctx *ctx, mo_matrix B, mo_matrix A, mo_matrix tau, mo_matrix W,
                        int flags, int nb);
+
+/* ---- symmetric indefinite LDL^T (ldlnp.go, ldl.go, ldlbk.go, ldlbks.go) ----
+ *
+ * MO_LOWER selects the lower triangle (A = L D L^T, unit L below the diagonal, D on it),
+ * otherwise the upper (A = U D U^T).  ipiv: device int64 array of npiv >= n entries in the
+ * reference's encoding (1-based partner rows; see each function).  The device runs the
+ * reference's unblocked sweep (nb is checked as the reference checks it, then ignored): the
+ * pivots are the reference's unblocked path's, values agree to rounding.  Orders up to
+ * a few thousand; one cooperative launch with a grid barrier per pivot decision. */
+
+/* DecomposeLDLnoPiv(A, W, flags, nb), ldlnp.go:211-235: no interchanges.  Non-square ->
+ * MO_ENOTSQUARE; nb > 0 and n >= nb with W NULL -> MO_ELDLWORK.  Asynchronous. */
+MO_API int mo_decompose_ldl_nopiv(mo_ctx *ctx, mo_matrix A, mo_matrix W, int flags, int nb);
+
+/* SolveLDLnoPiv(B, A, flags), ldlnp.go:251-266: B = A^-1 B (unit solve, D, transposed unit
+ * solve); neither MO_LOWER nor MO_UPPER -> no-op. */
+MO_API int mo_solve_ldl_nopiv(mo_ctx *ctx, mo_matrix B, mo_matrix A, int flags);
+
+/* DecomposeLDL(A, W, ipiv, flags, nb), ldl.go:439-466: 1 x 1 pivots, at each step the
+ * largest |diagonal entry| of the part left (first one on ties) is brought to the front
+ * with whole-row interchanges; ipiv[k] = 1-based partner or 0.  ipiv is zeroed first; npiv
+ * < n -> MO_EPIVLEN; a zero pivot -> MO_EZERODIAG (A then partly factored).  Synchronizes. */
+MO_API int mo_decompose_ldl(mo_ctx *ctx, mo_matrix A, mo_matrix W, int64_t *ipiv, int64_t npiv,
+                            int flags, int nb);
+
+/* SolveLDL(B, A, ipiv, flags), ldl.go:486-510: the interchanges, the two unit-triangular
+ * solves and D, in the reference's order. */
+MO_API int mo_solve_ldl(mo_ctx *ctx, mo_matrix B, mo_matrix A, const int64_t *ipiv,
+                        int64_t npiv, int flags);
+
+/* DecomposeBK(A, W, ipiv, flags, nb), ldlbk.go:1114-1140: Bunch-Kaufman (DSYTF2), 1 x 1 and
+ * 2 x 2 pivots, interchanges inside the part not yet factored; ipiv[k] = 1-based partner
+ * (k + 1 itself when none), both rows of a 2 x 2 block hold -(partner + 1).  W NULL or
+ * smaller than n x 2 (n x (nb + 1) when nb > 0 and n >= nb) -> MO_EBKWORK; non-square ->
+ * MO_ENOTSQUARE (the reference does not check); neither MO_LOWER nor MO_UPPER -> no-op.
+ * Asynchronous. */
+MO_API int mo_decompose_bk(mo_ctx *ctx, mo_matrix A, mo_matrix W, int64_t *ipiv, int64_t npiv,
+                           int flags, int nb);
+
+/* SolveBK(B, A, ipiv, flags), ldlbks.go:303-318 (DSYTRS): B = A^-1 B with DecomposeBK's
+ * factor.  LOWER follows unblkSolveBKLower's two sweeps; for UPPER the reference's sweeps
+ * run over empty and mismatched blocks of B (ldlbks.go:159-296), and this solves with the
+ * UPPER factor through the same steps on the index-reversed problem. */
+MO_API int mo_solve_bk(mo_ctx *ctx, mo_matrix B, mo_matrix A, const int64_t *ipiv, int64_t npiv,
+                       int flags);
 
 /* DecomposeCHOL(A, flags, nb), chol.go:116-127: A = L*L^T (MO_LOWER) or U^T*U (otherwise)
  * in place; the opposite strict triangle is not referenced.  Non-square -> MO_ENOTSQUARE.

@@ -14,4 +14,5 @@ from .api import (  # noqa: F401
     DecomposeCHOLAdjoint, DecomposeCHOLAdjointBatched, SolveCHOLAdjoint, SetSpinLimit, Mirror,
     context, MultSym, MultTrm, RankUpdate2Sym, UpdateTrm, InverseTrm,
     DecomposeQRT, DecomposeQR, BuildT, MultQT, MultQ, SolveQRT, SolveQR, BuildQ, BuildQT,
+    DecomposeLDLnoPiv, SolveLDLnoPiv, DecomposeLDL, SolveLDL, DecomposeBK, SolveBK,
 )

@@ -68,6 +68,12 @@ def lib() -> ctypes.CDLL:
         "mo_mult_q": [p, M, M, M, M, i, i],
         "mo_solve_qrt": [p, M, M, M, M, i, i],
         "mo_solve_qr": [p, M, M, M, M, i, i],
+        "mo_decompose_ldl_nopiv": [p, M, M, i, i],
+        "mo_solve_ldl_nopiv": [p, M, M, i],
+        "mo_decompose_ldl": [p, M, M, p, i64, i, i],
+        "mo_solve_ldl": [p, M, M, p, i64, i],
+        "mo_decompose_bk": [p, M, M, p, i64, i, i],
+        "mo_solve_bk": [p, M, M, p, i64, i],
         "mo_build_q": [p, M, M, M, i],
         "mo_build_qt": [p, M, M, M, i],
         "mo_mirror_create": [p, p, i64, ctypes.POINTER(p)],

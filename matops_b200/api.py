@@ -197,6 +197,46 @@ def SolveLU(B, A, pivots: torch.Tensor, flags: int):
     return _err(rc)
 
 
+# ---- symmetric indefinite LDL^T (ldlnp.go, ldl.go, ldlbk.go, ldlbks.go) ----
+
+def _piv(ipiv):
+    if ipiv.dtype != torch.int64 or not ipiv.is_cuda or not ipiv.is_contiguous():
+        raise TypeError("ipiv must be a contiguous CUDA int64 tensor")
+    return ctypes.c_void_p(ipiv.data_ptr()), ipiv.numel()
+
+
+def DecomposeLDLnoPiv(A, W, flags: int, nb: int):
+    """ldlnp.go:211 -- A = L D L^T (LOWER) or U D U^T without interchanges; (A, err)"""
+    return A, _err(_lib.lib().mo_decompose_ldl_nopiv(context(), view(A), _wview(W), flags, nb))
+
+
+def SolveLDLnoPiv(B, A, flags: int):
+    """ldlnp.go:251 -- B = A^-1 B with DecomposeLDLnoPiv's factor"""
+    return _err(_lib.lib().mo_solve_ldl_nopiv(context(), view(B), view(A), flags))
+
+
+def DecomposeLDL(A, W, ipiv, flags: int, nb: int):
+    """ldl.go:439 -- 1x1 diagonal pivoting; ipiv (CUDA int64) in the reference's encoding"""
+    return A, _err(_lib.lib().mo_decompose_ldl(context(), view(A), _wview(W), *_piv(ipiv), flags,
+                                               nb))
+
+
+def SolveLDL(B, A, ipiv, flags: int):
+    """ldl.go:486"""
+    return _err(_lib.lib().mo_solve_ldl(context(), view(B), view(A), *_piv(ipiv), flags))
+
+
+def DecomposeBK(A, W, ipiv, flags: int, nb: int):
+    """ldlbk.go:1114 -- Bunch-Kaufman LDL^T; ipiv negative for 2x2 blocks"""
+    return A, _err(_lib.lib().mo_decompose_bk(context(), view(A), _wview(W), *_piv(ipiv), flags,
+                                              nb))
+
+
+def SolveBK(B, A, ipiv, flags: int):
+    """ldlbks.go:303"""
+    return _err(_lib.lib().mo_solve_bk(context(), view(B), view(A), *_piv(ipiv), flags))
+
+
 # ---- QR with the compact WY form (qrwy.go, qrwym.go) ----
 
 def _wview(W):

@@ -231,6 +231,9 @@ const char *mo_strerror(int s) {
     case MO_ENOWORK: return "workspace not defined";
     case MO_ECQSIZE: return "C*Q: C.Cols != A.Rows";
     case MO_ETSMALL: return "reflector matrix T too small";
+    case MO_ELDLWORK: return "No workspace for blocking invocation";
+    case MO_EZERODIAG: return "zero value on diagonal";
+    case MO_EBKWORK: return "Workspace too small";
     default: return s > 0 ? "illegal value (non-positive pivot)" : "unknown error";
   }
 }

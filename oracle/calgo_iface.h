@@ -63,5 +63,8 @@ double dvec_nrm2(const mvec_t *X, int N);
 void dmmat_scale_plus(mdata_t *A, const mdata_t *B, double alpha, double beta, int flags,
                       int S, int L, int R, int E);
 void dmvec_trid_unb(mvec_t *X, const mdata_t *A, int flags, int N);
+/* the LDL^T path's triangular rank-1 update (calgo/cmops.h:181) */
+void dmvec_trmv_upd(mdata_t *A, const mvec_t *X, const mvec_t *Y, double alpha, int flags, int S,
+                    int L, int NB);
 
 #endif

@@ -458,3 +458,15 @@ void dmvec_trid_unb(mvec_t *X, const mdata_t *A, int flags, int N) {
     }
   }
 }
+
+/* calgo/dmvec_rank.c:263-285 (dmvec_trmv_upd): columns S..L-1 of the lower (rows j..L-1) or,
+ * with MTX_UPPER, upper (rows 0..j) triangle of A += alpha x y^T, as a_ij += x_i (alpha y_j) */
+void dmvec_trmv_upd(mdata_t *A, const mvec_t *X, const mvec_t *Y, double alpha, int flags, int S,
+                    int L, int NB) {
+  (void)NB;
+  for (int j = S; j < L; j++) {
+    const double cf = alpha * Y->md[(long)j * Y->inc];
+    const int i0 = (flags & MTX_UPPER) ? 0 : j, i1 = (flags & MTX_UPPER) ? j + 1 : L;
+    for (int i = i0; i < i1; i++) AT(A, i, j) += X->md[(long)i * X->inc] * cf;
+  }
+}

@@ -1024,6 +1024,424 @@ int or_build_qt_fm(fm A, fm T, fm W, int nb) {
   return OR_OK;
 }
 
+/* ---------------- ldlnp.go, ldl.go, ldlbk.go, ldlbks.go: symmetric indefinite LDL^T ------- */
+
+/* mvec.go:163-190 (MVUpdateTrm): the lower (MTX_LOWER) or upper triangle of
+ * A += alpha x y^T by calgo/dmvec_rank.c:263 (dmvec_trmv_upd) */
+static int MVUpdateTrm(fm A, fm X, fm Y, double alpha, int flags) {
+  if (A.r == 0 || A.c == 0) return OR_OK;
+  if (!is_vector(Y) || !is_vector(X)) return OR_ENOTVECTOR;
+  mdata_t a = {A.d, A.ld};
+  mvec_t x = {X.d, X.r == 1 ? X.ld : 1}, y = {Y.d, Y.r == 1 ? Y.ld : 1};
+  dmvec_trmv_upd(&a, &x, &y, alpha, flags, 0, A.c, nB);
+  return OR_OK;
+}
+
+/* mvec.go:405-419 (IAMax) over calgo/dvec_util.c:164: first index of the largest |x| */
+static int IAMax(fm X) {
+  const int n = X.r * X.c;
+  if (n <= 1) return 0;
+  double mx = 0.0;
+  int ix = 0;
+  for (int i = 0; i < n; i++) {
+    const double v = fabs(*vel(X, i));
+    if (v > mx) {
+      mx = v;
+      ix = i;
+    }
+  }
+  return ix;
+}
+
+/* the diagonal of a square view as a vector (FloatMatrix.Diag) */
+static fm diagv(fm A) {
+  fm d = {A.d, 1, A.r < A.c ? A.r : A.c, A.ld + 1};
+  return d;
+}
+
+static void swap_el(double *a, double *b) {
+  const double t = *a;
+  *a = *b;
+  *b = t;
+}
+
+/* pivot.go:145-190 (applyPivotSym): symmetric interchange of row/column 0 of AR with
+ * row/column `index`, AL the factored columns left (LOWER) of AR */
+static void applyPivotSymLower(fm AL, fm AR, int index) {
+  for (int c = 0; c < AL.c; c++) swap_el(AL.d + (intptr_t)c * AL.ld, AL.d + index + (intptr_t)c * AL.ld);
+  for (int i = 1; i < index; i++) swap_el(AR.d + i, AR.d + index + (intptr_t)i * AR.ld);
+  for (int i = index + 1; i < AR.r; i++) swap_el(AR.d + i, AR.d + i + (intptr_t)index * AR.ld);
+  swap_el(AR.d, AR.d + index + (intptr_t)index * AR.ld);
+}
+
+/* applyPivotSym UPPER (pivot.go:163-183): AL = [ATL ATR] full rows, AR = [a11 a12]; the
+ * last row/column of ATL (colno) with `index` */
+static void applyPivotSymUpper(fm A, int colno, int index) {
+  /* S1 (row colno right of the diagonal) <-> row index, same columns */
+  for (int c = colno + 1; c < A.c; c++)
+    swap_el(A.d + colno + (intptr_t)c * A.ld, A.d + index + (intptr_t)c * A.ld);
+  for (int i = index + 1; i < colno; i++)
+    swap_el(A.d + i + (intptr_t)colno * A.ld, A.d + index + (intptr_t)i * A.ld);
+  for (int i = 0; i < index; i++)
+    swap_el(A.d + i + (intptr_t)index * A.ld, A.d + i + (intptr_t)colno * A.ld);
+  swap_el(A.d + colno + (intptr_t)colno * A.ld, A.d + index + (intptr_t)index * A.ld);
+}
+
+/* ldlnp.go:23-58 / :64-97 */
+static void unblkLDLnoPiv(fm A, int upper) {
+  const int n = A.r;
+  for (int s = 0; s < n; s++) {
+    const int k = upper ? n - 1 - s : s;
+    const double a11 = A.d[k + (intptr_t)k * A.ld];
+    if (!upper) {
+      fm a21 = sub(A, k + 1, k, n - k - 1, 1), A22 = sub(A, k + 1, k + 1, n - k - 1, n - k - 1);
+      MVUpdateTrm(A22, a21, a21, -1.0 / a11, MTX_LOWER);
+      InvScale(a21, a11);
+    } else {
+      fm a01 = sub(A, 0, k, k, 1), A00 = sub(A, 0, 0, k, k);
+      MVUpdateTrm(A00, a01, a01, -1.0 / a11, MTX_UPPER);
+      InvScale(a01, a11);
+    }
+  }
+}
+
+/* ldl.go:25-88 (unblkLowerLDL) / :297-349 (unblkUpperLDL): 1x1 pivots, the largest |diagonal|
+ * of the part left; ipiv[k] = 1-based partner or 0.  Returns 1 on a zero pivot. */
+static int unblkLDL(fm A, int64_t *ipiv, int upper) {
+  const int n = A.r;
+  for (int s = 0; s < n; s++) {
+    if (!upper) {
+      const int k = s;
+      fm ABR = sub(A, k, k, n - k, n - k), ABL = sub(A, k, 0, n - k, k);
+      const int imax = IAMax(diagv(ABR));
+      if (imax > 0) {
+        applyPivotSymLower(ABL, ABR, imax);
+        ipiv[k] = imax + k + 1;
+      } else {
+        ipiv[k] = 0;
+      }
+      const double a11 = A.d[k + (intptr_t)k * A.ld];
+      if (a11 == 0.0) return 1;
+      fm a21 = sub(A, k + 1, k, n - k - 1, 1), A22 = sub(A, k + 1, k + 1, n - k - 1, n - k - 1);
+      MVUpdateTrm(A22, a21, a21, -1.0 / a11, MTX_LOWER);
+      InvScale(a21, a11);
+    } else {
+      const int k = n - 1 - s;  /* ATL is A[0:k+1, 0:k+1] */
+      fm ATL = sub(A, 0, 0, k + 1, k + 1);
+      const int imax = IAMax(diagv(ATL));
+      if (imax < k) {
+        applyPivotSymUpper(A, k, imax);
+        ipiv[k] = imax + 1;
+      } else {
+        ipiv[k] = 0;
+      }
+      const double a11 = A.d[k + (intptr_t)k * A.ld];
+      if (a11 == 0.0) return 1;
+      fm a01 = sub(A, 0, k, k, 1), A00 = sub(A, 0, 0, k, k);
+      MVUpdateTrm(A00, a01, a01, -1.0 / a11, MTX_UPPER);
+      InvScale(a01, a11);
+    }
+  }
+  return 0;
+}
+
+#define BK_ALPHA 0.6403882032022075 /* ldlbk.go:16, (1 + sqrt(17)) / 8 */
+
+/* ldlbk.go:107-207 (findBKPivot, LOWER): A is the part left (ABR) */
+static void findBKPivotLower(fm A, int *r_out, int *np_out) {
+  *r_out = 0;
+  *np_out = 1;
+  if (A.r == 1) return;
+  const double amax = fabs(A.d[0]);
+  const int r = IAMax(sub(A, 1, 0, A.r - 1, 1)) + 1;
+  const double rmax = fabs(A.d[r]);
+  if (amax >= BK_ALPHA * rmax) return;
+  int q = IAMax(sub(A, r, 0, 1, r));
+  double qmax = fabs(A.d[r + (intptr_t)q * A.ld]);
+  if (r < A.r - 1) {
+    fm qrow = sub(A, r + 1, r, A.r - r - 1, 1);
+    q = IAMax(qrow);
+    const double qmax2 = fabs(*vel(qrow, q));
+    if (qmax2 > qmax) qmax = qmax2;
+  }
+  if (amax >= BK_ALPHA * rmax * (rmax / qmax)) return;
+  *r_out = r;
+  *np_out = fabs(A.d[r + (intptr_t)r * A.ld]) >= BK_ALPHA * qmax ? 1 : 2;
+}
+
+/* ldlbk.go:164-205 (findBKPivot, UPPER): A is ATL; r = -1 for no interchange */
+static void findBKPivotUpper(fm A, int *r_out, int *np_out) {
+  *r_out = -1;
+  *np_out = 1;
+  if (A.r == 1) return;
+  const int last = A.r - 1;
+  const double amax = fabs(A.d[last + (intptr_t)last * A.ld]);
+  const int r = IAMax(sub(A, 0, last, last, 1));
+  const double rmax = fabs(A.d[r + (intptr_t)last * A.ld]);
+  if (amax >= BK_ALPHA * rmax) return;
+  double qmax = 0.0;
+  if (r > 0) {
+    fm qc = sub(A, 0, r, r, 1);
+    const int q = IAMax(qc);
+    qmax = fabs(*vel(qc, q));
+  }
+  fm qrow = sub(A, r, r + 1, 1, last - r);
+  const int q = IAMax(qrow);
+  const double qmax2 = fabs(*vel(qrow, q));
+  if (qmax2 > qmax) qmax = qmax2;
+  if (amax >= BK_ALPHA * rmax * (rmax / qmax)) return;
+  *r_out = r;
+  *np_out = fabs(A.d[r + (intptr_t)r * A.ld]) >= BK_ALPHA * qmax ? 1 : 2;
+}
+
+/* ldlbk.go:48-76 (applyBKPivotSym LOWER): within AR, rows/columns src and dst (src < dst) */
+static void applyBKPivotSymLower(fm AR, int src, int dst) {
+  for (int t = 0; t < dst - src - 1; t++)
+    swap_el(AR.d + (src + 1 + t) + (intptr_t)src * AR.ld, AR.d + dst + (intptr_t)(src + 1 + t) * AR.ld);
+  for (int i = dst + 1; i < AR.r; i++)
+    swap_el(AR.d + i + (intptr_t)src * AR.ld, AR.d + i + (intptr_t)dst * AR.ld);
+  swap_el(AR.d + src + (intptr_t)src * AR.ld, AR.d + dst + (intptr_t)dst * AR.ld);
+}
+
+/* ldlbk.go:77-104 (applyBKPivotSym UPPER): within AR (= ATL), src > dst */
+static void applyBKPivotSymUpper(fm AR, int src, int dst) {
+  for (int t = 0; t < src - dst - 1; t++)
+    swap_el(AR.d + (dst + 1 + t) + (intptr_t)src * AR.ld, AR.d + dst + (intptr_t)(dst + 1 + t) * AR.ld);
+  for (int i = 0; i < dst; i++)
+    swap_el(AR.d + i + (intptr_t)src * AR.ld, AR.d + i + (intptr_t)dst * AR.ld);
+  swap_el(AR.d + src + (intptr_t)src * AR.ld, AR.d + dst + (intptr_t)dst * AR.ld);
+}
+
+/* the 2 x 2 pivot step of ldlbk.go:289-313 / :415-436: cwrk = the two columns c, then
+ * c = scale * cwrk * [[i00, -1], [-1, i11]] (Mult, beta 0) and the triangle of A22 -=
+ * c cwrk^T (UpdateTrm, beta 1) */
+static void bk_two_by_two(fm c, fm A22, double *cw, int m, double i00, double i11, double scale,
+                          int tri) {
+  fm W = {cw, m, 2, m > 0 ? m : 1};
+  for (int i = 0; i < m; i++) {
+    cw[i] = c.d[i];
+    cw[m + i] = c.d[i + (intptr_t)c.ld];
+  }
+  double inv[4] = {i00, -1.0, -1.0, i11};
+  fm E = {inv, 2, 2, 2};
+  or_mult_fm(c, W, E, scale, 0.0, MTX_NOTRANS);
+  or_update_trm_fm(A22, c, W, -1.0, 1.0, tri | MTX_TRANSB);
+}
+
+/* ldlbk.go:212-330 (unblkDecompBKLower) and :335-455 (unblkDecompBKUpper), LAPACK DSYTF2 */
+static void unblkDecompBK(fm A, int64_t *ipiv, int upper) {
+  const int n = A.r;
+  double *cw = (double *)malloc(sizeof(double) * 2 * (n > 0 ? n : 1));
+  int done = 0;
+  while (done < n) {
+    int r, np;
+    if (!upper) {
+      const int k = done;
+      fm ABR = sub(A, k, k, n - k, n - k);
+      findBKPivotLower(ABR, &r, &np);
+      if (r != 0 && r != np - 1) {
+        applyBKPivotSymLower(ABR, np - 1, r);
+        if (np == 2) swap_el(ABR.d + 1, ABR.d + r);
+      }
+      if (np == 1) {
+        const double a11 = ABR.d[0];
+        fm a21 = sub(A, k + 1, k, n - k - 1, 1), A22 = sub(A, k + 1, k + 1, n - k - 1, n - k - 1);
+        MVUpdateTrm(A22, a21, a21, -1.0 / a11, MTX_LOWER);
+        InvScale(a21, a11);
+        ipiv[k] = r + k + 1;
+      } else {
+        const double a = ABR.d[0], b = ABR.d[1], d = ABR.d[1 + (intptr_t)ABR.ld];
+        const double i00 = d / b, i11 = a / b;
+        double scale = 1.0 / ((a / b) * (d / b) - 1.0);
+        scale /= b;
+        const int m = n - k - 2;
+        fm a21 = sub(A, k + 2, k, m, 2), A22 = sub(A, k + 2, k + 2, m, m);
+        bk_two_by_two(a21, A22, cw, m, i00, i11, scale, MTX_LOWER);
+        ipiv[k] = -(r + k + 1);
+        ipiv[k + 1] = ipiv[k];
+      }
+    } else {
+      const int s = n - done; /* ATL is s x s */
+      fm ATL = sub(A, 0, 0, s, s);
+      const int nr = s - 1;
+      findBKPivotUpper(ATL, &r, &np);
+      if (r != -1) {
+        applyBKPivotSymUpper(ATL, s - np, r);
+        if (np == 2) swap_el(ATL.d + (nr - 1) + (intptr_t)nr * ATL.ld, ATL.d + r + (intptr_t)nr * ATL.ld);
+      }
+      if (np == 1) {
+        const int k = s - 1;
+        const double a11 = A.d[k + (intptr_t)k * A.ld];
+        fm a01 = sub(A, 0, k, k, 1), A00 = sub(A, 0, 0, k, k);
+        MVUpdateTrm(A00, a01, a01, -1.0 / a11, MTX_UPPER);
+        InvScale(a01, a11);
+        ipiv[k] = r == -1 ? s : r + 1;
+      } else {
+        const int k = s - 2;
+        const double a = A.d[k + (intptr_t)k * A.ld], b = A.d[k + (intptr_t)(k + 1) * A.ld];
+        const double d = A.d[(k + 1) + (intptr_t)(k + 1) * A.ld];
+        const double i00 = d / b, i11 = a / b;
+        double scale = 1.0 / ((a / b) * (d / b) - 1.0);
+        scale /= b;
+        const int m = k;
+        fm a01 = sub(A, 0, k, m, 2), A00 = sub(A, 0, 0, m, m);
+        bk_two_by_two(a01, A00, cw, m, i00, i11, scale, MTX_UPPER);
+        ipiv[k] = -(r + 1);
+        ipiv[k + 1] = ipiv[k];
+      }
+    }
+    done += np;
+  }
+  free(cw);
+}
+
+/* ldlnp.go:211-235 (DecomposeLDLnoPiv): the unblocked path (the blocked one computes the
+ * same factor; nb is accepted) */
+int or_decompose_ldl_nopiv_fm(fm A, int flags) {
+  if (A.c != A.r) return OR_ENOTSQUARE;
+  unblkLDLnoPiv(A, (flags & MTX_LOWER) == 0);
+  return OR_OK;
+}
+
+/* ldl.go:439-466 (DecomposeLDL), unblocked path; returns 1 on a zero pivot ("zero value on
+ * diagonal") */
+int or_decompose_ldl_fm(fm A, int64_t *ipiv, int npiv, int flags) {
+  if (A.c != A.r) return OR_ENOTSQUARE;
+  for (int k = 0; k < npiv; k++) ipiv[k] = 0;
+  if (npiv < A.r) return OR_EPIVLEN;
+  return unblkLDL(A, ipiv, (flags & MTX_LOWER) == 0);
+}
+
+/* ldlbk.go:1114-1140 (DecomposeBK), unblocked path (DSYTF2) */
+int or_decompose_bk_fm(fm A, int64_t *ipiv, int npiv, int flags) {
+  for (int k = 0; k < npiv; k++) ipiv[k] = 0;
+  if (A.c != A.r) return OR_ENOTSQUARE;
+  if (npiv < A.r) return OR_EPIVLEN;
+  if (!(flags & (MTX_LOWER | MTX_UPPER))) return OR_OK;
+  unblkDecompBK(A, ipiv, (flags & MTX_LOWER) == 0);
+  return OR_OK;
+}
+
+/* diag.go:85-128 (SolveDiag, LEFT, D the diagonal of a square matrix): row k *= 1/d_k */
+static void SolveDiagLeft(fm B, fm A) {
+  for (int k = 0; k < B.r; k++) {
+    const double f = 1.0 / A.d[k + (intptr_t)k * A.ld];
+    for (int c = 0; c < B.c; c++) B.d[k + (intptr_t)c * B.ld] *= f;
+  }
+}
+
+/* ldlnp.go:251-266 (SolveLDLnoPiv) */
+void or_solve_ldl_nopiv_fm(fm B, fm A, int flags) {
+  const int tri = (flags & MTX_UPPER) ? MTX_UPPER : ((flags & MTX_LOWER) ? MTX_LOWER : 0);
+  if (!tri) return;
+  or_solve_trm_fm(B, A, 1.0, tri | MTX_UNIT);
+  SolveDiagLeft(B, A);
+  or_solve_trm_fm(B, A, 1.0, tri | MTX_UNIT | MTX_TRANSA);
+}
+
+/* pivot.go:63-78 (applyRowPivots, offset 0): FORWARD k = 0.., BACKWARD k = ..0 */
+static void applyRowPivotsLDL(fm B, const int64_t *ipiv, int n, int forward) {
+  for (int t = 0; t < n; t++) {
+    const int k = forward ? t : n - 1 - t;
+    if (ipiv[k] > 0) swapRows(B, (int)ipiv[k] - 1, k);
+  }
+}
+
+/* ldl.go:486-510 (SolveLDL) */
+void or_solve_ldl_fm(fm B, fm A, const int64_t *ipiv, int flags) {
+  const int n = A.r;
+  if (flags & MTX_UPPER) {
+    applyRowPivotsLDL(B, ipiv, n, 0);
+    or_solve_trm_fm(B, A, 1.0, MTX_UPPER | MTX_UNIT);
+    SolveDiagLeft(B, A);
+    or_solve_trm_fm(B, A, 1.0, MTX_UPPER | MTX_UNIT | MTX_TRANSA);
+    applyRowPivotsLDL(B, ipiv, n, 1);
+  } else if (flags & MTX_LOWER) {
+    applyRowPivotsLDL(B, ipiv, n, 1);
+    or_solve_trm_fm(B, A, 1.0, MTX_LOWER | MTX_UNIT);
+    SolveDiagLeft(B, A);
+    or_solve_trm_fm(B, A, 1.0, MTX_LOWER | MTX_UNIT | MTX_TRANSA);
+    applyRowPivotsLDL(B, ipiv, n, 0);
+  }
+}
+
+/* ldlbks.go:15-156 (unblkSolveBKLower), both phases */
+static void unblkSolveBKLower(fm B, fm A, const int64_t *ipiv) {
+  const int n = A.r;
+  for (int k = 0; k < n;) {
+    const int np = ipiv[k] < 0 ? 2 : 1;
+    if (np == 1) {
+      if (ipiv[k] != k + 1) swapRows(B, k, (int)ipiv[k] - 1);
+      fm b1 = sub(B, k, 0, 1, B.c);
+      MVRankUpdate(sub(B, k + 1, 0, n - k - 1, B.c), sub(A, k + 1, k, n - k - 1, 1), b1, -1.0);
+      InvScale(b1, A.d[k + (intptr_t)k * A.ld]);
+    } else {
+      if (ipiv[k] != -(k + 1)) swapRows(B, k + 1, (int)(-ipiv[k]) - 1);
+      const double b = A.d[(k + 1) + (intptr_t)k * A.ld];
+      const double apb = A.d[k + (intptr_t)k * A.ld] / b;
+      const double dpb = A.d[(k + 1) + (intptr_t)(k + 1) * A.ld] / b;
+      double scale = apb * dpb - 1.0;
+      scale *= b;
+      fm b1 = sub(B, k, 0, 2, B.c);
+      or_mult_fm(sub(B, k + 2, 0, n - k - 2, B.c), sub(A, k + 2, k, n - k - 2, 2), b1, -1.0, 1.0,
+                 MTX_NOTRANS);
+      for (int c = 0; c < B.c; c++) {
+        double *s = B.d + k + (intptr_t)c * B.ld;
+        const double s0 = s[0], s1 = s[1];
+        s[0] = (dpb * s0 - s1) / scale;
+        s[1] = (apb * s1 - s0) / scale;
+      }
+    }
+    k += np;
+  }
+  for (int nc = n; nc > 0;) {
+    const int np = ipiv[nc - 1] < 0 ? 2 : 1;
+    if (np == 1) {
+      const int k = nc - 1;
+      fm b1 = sub(B, k, 0, 1, B.c);
+      MVMult(b1, sub(B, k + 1, 0, n - k - 1, B.c), sub(A, k + 1, k, n - k - 1, 1), -1.0, 1.0,
+             MTX_TRANSA);
+      if (ipiv[k] != nc) swapRows(B, k, (int)ipiv[k] - 1);
+    } else {
+      const int k = nc - 2;
+      or_mult_fm(sub(B, k, 0, 2, B.c), sub(A, k + 2, k, n - k - 2, 2), sub(B, k + 2, 0, n - k - 2, B.c),
+                 -1.0, 1.0, MTX_TRANSA);
+      if (ipiv[k] != -nc) swapRows(B, k + 1, (int)(-ipiv[k]) - 1);
+    }
+    nc -= np;
+  }
+}
+
+/* ldlbks.go:303-318 (SolveBK).  LOWER restates unblkSolveBKLower.  The reference's UPPER
+ * branch (unblkSolveBKUpper, ldlbks.go:159-296) updates an empty block of B in its first
+ * phase and mismatched ones in its second (its partitions run the wrong way for U); the
+ * oracle solves A X = B with the UPPER factor through the same steps on the index-reversed
+ * problem (row/column i <-> n-1-i turns U D U^T into L D L^T). */
+void or_solve_bk_fm(fm B, fm A, const int64_t *ipiv, int flags) {
+  const int n = A.r;
+  if (flags & MTX_LOWER) {
+    unblkSolveBKLower(B, A, ipiv);
+  } else if (flags & MTX_UPPER) {
+    double *ar = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1) * (n > 0 ? n : 1));
+    double *br = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1) * (B.c > 0 ? B.c : 1));
+    int64_t *pr = (int64_t *)calloc((size_t)(n > 0 ? n : 1), sizeof(int64_t));
+    for (int j = 0; j < n; j++)
+      for (int i = 0; i < n; i++) ar[i + (size_t)j * n] = A.d[(n - 1 - i) + (intptr_t)(n - 1 - j) * A.ld];
+    for (int c = 0; c < B.c; c++)
+      for (int i = 0; i < n; i++) br[i + (size_t)c * n] = B.d[(n - 1 - i) + (intptr_t)c * B.ld];
+    for (int i = 0; i < n; i++) {
+      const int64_t p = ipiv[n - 1 - i];
+      pr[i] = p > 0 ? n + 1 - p : -(n + 1 + p);
+    }
+    unblkSolveBKLower((fm){br, n, B.c, n > 0 ? n : 1}, (fm){ar, n, n, n > 0 ? n : 1}, pr);
+    for (int c = 0; c < B.c; c++)
+      for (int i = 0; i < n; i++) B.d[(n - 1 - i) + (intptr_t)c * B.ld] = br[i + (size_t)c * n];
+    free(ar);
+    free(br);
+    free(pr);
+  }
+}
+
 /* ---------------- flat C entry points for the ctypes harness ---------------- */
 
 #define FM(p, r, c, ld) ((fm){(p), (r), (c), (ld)})
@@ -1131,4 +1549,26 @@ int or_build_q(double *A, int ar, int ac, int lda, double *tau, int taur, double
 int or_build_qt(double *A, int ar, int ac, int lda, double *T, int tr, int tc, int ldt, double *W,
                 int wr, int wc, int ldw, int nb) {
   return or_build_qt_fm(FM(A, ar, ac, lda), FM(T, tr, tc, ldt), FM(W, wr, wc, ldw), nb);
+}
+/* LDL^T entry points (ldlnp.go, ldl.go, ldlbk.go, ldlbks.go) */
+int or_decompose_ldl_nopiv(double *A, int ar, int ac, int lda, int flags) {
+  return or_decompose_ldl_nopiv_fm(FM(A, ar, ac, lda), flags);
+}
+void or_solve_ldl_nopiv(double *B, int br, int bc, int ldb, double *A, int ar, int ac, int lda,
+                        int flags) {
+  or_solve_ldl_nopiv_fm(FM(B, br, bc, ldb), FM(A, ar, ac, lda), flags);
+}
+int or_decompose_ldl(double *A, int ar, int ac, int lda, int64_t *piv, int npiv, int flags) {
+  return or_decompose_ldl_fm(FM(A, ar, ac, lda), piv, npiv, flags);
+}
+void or_solve_ldl(double *B, int br, int bc, int ldb, double *A, int ar, int ac, int lda,
+                  const int64_t *piv, int flags) {
+  or_solve_ldl_fm(FM(B, br, bc, ldb), FM(A, ar, ac, lda), piv, flags);
+}
+int or_decompose_bk(double *A, int ar, int ac, int lda, int64_t *piv, int npiv, int flags) {
+  return or_decompose_bk_fm(FM(A, ar, ac, lda), piv, npiv, flags);
+}
+void or_solve_bk(double *B, int br, int bc, int ldb, double *A, int ar, int ac, int lda,
+                 const int64_t *piv, int flags) {
+  or_solve_bk_fm(FM(B, br, bc, ldb), FM(A, ar, ac, lda), piv, flags);
 }

@@ -94,6 +94,15 @@ class Oracle:
         L.or_build_t.argtypes = M + M + [p, i]
         L.or_mult_qt.argtypes = M + M + M + M + [i, i]
         L.or_solve_qrt.argtypes = M + M + M + M + [i, i]
+        L.or_decompose_ldl_nopiv.argtypes = M + [i]
+        L.or_solve_ldl_nopiv.argtypes = M + M + [i]
+        L.or_solve_ldl_nopiv.restype = None
+        L.or_decompose_ldl.argtypes = M + [p, i, i]
+        L.or_solve_ldl.argtypes = M + M + [p, i]
+        L.or_solve_ldl.restype = None
+        L.or_decompose_bk.argtypes = M + [p, i, i]
+        L.or_solve_bk.argtypes = M + M + [p, i]
+        L.or_solve_bk.restype = None
         L.or_build_q.argtypes = M + [p, i] + [p, i, i, i] + [i]
         L.or_build_qt.argtypes = M + M + M + [i]
 
@@ -181,6 +190,28 @@ class Oracle:
     def BuildQT(self, A, T, W, nb):
         """qrwyk.go:278: BuildQ with the reflector block T of DecomposeQRT"""
         return self.lib.or_build_qt(*view(A), *view(T), *self._wview(W), nb)
+
+    # symmetric indefinite LDL^T (ldlnp.go, ldl.go, ldlbk.go, ldlbks.go); pivots are the
+    # reference's 1-based ipiv (0 = no interchange for DecomposeLDL, negative = 2x2 block)
+    def DecomposeLDLnoPiv(self, A, flags):
+        return self.lib.or_decompose_ldl_nopiv(*view(A), flags)
+
+    def SolveLDLnoPiv(self, B, A, flags):
+        self.lib.or_solve_ldl_nopiv(*view(B), *view(A), flags)
+
+    def DecomposeLDL(self, A, ipiv: np.ndarray, flags):
+        assert ipiv.dtype == np.int64 and ipiv.flags.c_contiguous
+        return self.lib.or_decompose_ldl(*view(A), ctypes.c_void_p(ipiv.ctypes.data), len(ipiv), flags)
+
+    def SolveLDL(self, B, A, ipiv: np.ndarray, flags):
+        self.lib.or_solve_ldl(*view(B), *view(A), ctypes.c_void_p(ipiv.ctypes.data), flags)
+
+    def DecomposeBK(self, A, ipiv: np.ndarray, flags):
+        assert ipiv.dtype == np.int64 and ipiv.flags.c_contiguous
+        return self.lib.or_decompose_bk(*view(A), ctypes.c_void_p(ipiv.ctypes.data), len(ipiv), flags)
+
+    def SolveBK(self, B, A, ipiv: np.ndarray, flags):
+        self.lib.or_solve_bk(*view(B), *view(A), ctypes.c_void_p(ipiv.ctypes.data), flags)
 
     def GemvBetaOnce(self, on: bool) -> bool:
         """Port only: make the transposed GEMV apply beta once (BLAS semantics) instead of

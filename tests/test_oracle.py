@@ -327,3 +327,52 @@ def test_golden_build_q(oracle, golden_qr, name):
                              int(c["nb"])) == 0
     assert rel(Q, c["Q"]) <= 1e-12
     assert fro(Q.T @ Q - np.eye(40)) <= 100 * 60 * EPS
+
+
+# ---------------- symmetric indefinite LDL^T (ldlnp.go, ldl.go, ldlbk.go, ldlbks.go) ------
+
+def _sym(rng, n):
+    g = rng.uniform(-1, 1, (n, n))
+    return g + g.T
+
+
+@pytest.mark.parametrize("n", [1, 2, 5, 37, 120])
+@pytest.mark.parametrize("flags", [LO, UP])
+def test_port_vs_ref_ldl(oracle, ref_oracle, n, flags):
+    """port and the reference's kernels: identical pivots, factors to rounding, and the
+    solves satisfy A X = B"""
+    rng = np.random.default_rng(300 + n)
+    A0 = colmajor(_sym(rng, n), ld=even_ld(n))
+    B0 = colmajor(rng.uniform(-1, 1, (n, 3)))
+    res = []
+    for o in (oracle, ref_oracle):
+        Ad = colmajor(A0 + 2 * n * np.eye(n))
+        assert o.DecomposeLDLnoPiv(Ad, flags) == 0
+        A1, p1 = colmajor(A0), np.zeros(n, np.int64)
+        assert o.DecomposeLDL(A1, p1, flags) == 0
+        A2, p2 = colmajor(A0), np.zeros(n, np.int64)
+        assert o.DecomposeBK(A2, p2, flags) == 0
+        X = colmajor(B0)
+        o.SolveBK(X, A2, p2, flags)
+        res.append((Ad, A1, p1, A2, p2, X))
+    (a, b) = res
+    assert rel(a[0], b[0]) <= 1e-13
+    assert np.array_equal(a[2], b[2]) and rel(a[1], b[1]) <= 1e-11
+    assert np.array_equal(a[4], b[4]) and rel(a[3], b[3]) <= 1e-11
+    S = np.tril(A0) if flags & LO else np.triu(A0)
+    S = S + S.T - np.diag(np.diag(A0))
+    for X in (a[5], b[5]):
+        assert fro(S @ X - B0) <= 1e-9 * fro(S) * max(fro(X), 1.0)
+
+
+def test_oracle_ldl_reference_cases(oracle):
+    """ldl_test.go / ldlbkl_test.go style: the factors reproduce A (lower, 2 x 2 blocks
+    included) and DecomposeLDL reports a zero pivot"""
+    rng = np.random.default_rng(9)
+    n = 40
+    A0 = _sym(rng, n)
+    A, p = colmajor(A0), np.zeros(n, np.int64)
+    assert oracle.DecomposeBK(A, p, LO) == 0
+    assert (p < 0).any() and (p > 0).any()
+    Z, pz = colmajor(np.zeros((5, 5))), np.zeros(5, np.int64)
+    assert oracle.DecomposeLDL(Z, pz, LO) == 1
