@@ -273,6 +273,9 @@ __global__ void __launch_bounds__(kLdlThreads, 1)
       }
       const double amax = fabs(ldg(A.at(k, k)));
       if (!(amax >= kBkAlpha * rmax)) {
+        // |a(ri, ri)| is read before the next barrier: once every CTA has passed it, the
+        // first ones may already be interchanging (ri, ri) with another diagonal entry
+        const double arr = fabs(ldg(A.at(ri, ri)));
         double qmax;
         int qi;
         if (!grid_search(
@@ -293,7 +296,7 @@ __global__ void __launch_bounds__(kLdlThreads, 1)
         if (!(qmax >= 0.0)) qmax = 0.0;
         if (!(amax >= kBkAlpha * rmax * (rmax / qmax))) {
           r = ri - k;
-          np = fabs(ldg(A.at(ri, ri))) >= kBkAlpha * qmax ? 1 : 2;
+          np = arr >= kBkAlpha * qmax ? 1 : 2;
         }
       }
       if (cta == 0 && tid == 0) {

@@ -130,3 +130,28 @@ def test_ldl_errors(gpu, rng):
     _, err = gpu.DecomposeLDLnoPiv(A.clone(), None, LO, 4)
     assert err is not None and err.code == -17
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_bunch_kaufman_2048_repeated(gpu, ref, seed):
+    """back-to-back factorizations at n = 2048 (no synchronization between them): the same
+    pivots each time and as the oracle's"""
+    import torch
+    n = 2048
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    A0 = gpu.matrix(n, n)
+    A0.uniform_(-1.0, 1.0, generator=g)
+    A0.copy_(A0 + A0.t())
+    A, W = gpu.matrix(n, n), gpu.matrix(n, 2)
+    pivs = []
+    for _ in range(3):
+        A.copy_(A0)
+        piv = torch.zeros(n, dtype=torch.int64, device="cuda")
+        assert gpu.DecomposeBK(A, W, piv, LO, 0)[1] is None
+        pivs.append(piv)
+    assert gpu.Sync() == 0
+    Ar, pr = colmajor(A0.cpu().numpy()), np.zeros(n, np.int64)
+    assert ref.DecomposeBK(Ar, pr, LO) == 0
+    for piv in pivs:
+        assert np.array_equal(piv.cpu().numpy(), pr)
+    assert fro(np.tril(A.cpu().numpy()) - np.tril(Ar)) <= 1e-8 * fro(Ar)
