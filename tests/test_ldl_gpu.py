@@ -155,3 +155,45 @@ def test_bunch_kaufman_2048_repeated(gpu, ref, seed):
     for piv in pivs:
         assert np.array_equal(piv.cpu().numpy(), pr)
     assert fro(np.tril(A.cpu().numpy()) - np.tril(Ar)) <= 1e-8 * fro(Ar)
+
+
+def _golden():
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "ldl.npz"))
+    cases = {}
+    for k in z.files:
+        name, field = k.split("/")
+        cases.setdefault(name, {})[field] = z[k]
+    return cases
+
+
+@pytest.mark.parametrize("name", sorted(_golden()))
+def test_golden_ldl_device(gpu, name):
+    """the device against the reference's kernels' outputs (tests/golden/ldl.npz): the
+    reference's own Bunch-Kaufman test tables and seeded cases"""
+    import torch
+    c = _golden()[name]
+    fl = int(c["flags"])
+    A0 = c["A"]
+    n = A0.shape[0]
+    Ag = dev(gpu, A0)
+    piv = torch.zeros(n, dtype=torch.int64, device="cuda")
+    if name.startswith("np_"):
+        assert gpu.DecomposeLDLnoPiv(Ag, None, fl, 0)[1] is None
+    elif "bk" in name:
+        assert gpu.DecomposeBK(Ag, gpu.matrix(n, 2), piv, fl, 0)[1] is None
+    else:
+        assert gpu.DecomposeLDL(Ag, None, piv, fl, 0)[1] is None
+    if "piv" in c:
+        assert np.array_equal(piv.cpu().numpy(), c["piv"])
+    Ah = Ag.cpu().numpy()
+    assert fro(tri(Ah, fl) - tri(c["LDL"], fl)) <= 1e-10 * max(fro(c["LDL"]), 1.0)
+    if "X" in c:
+        Bg = dev(gpu, c["B"])
+        if name.startswith("np_"):
+            assert gpu.SolveLDLnoPiv(Bg, Ag, fl) is None
+        elif "bk" in name:
+            assert gpu.SolveBK(Bg, Ag, piv, fl) is None
+        else:
+            assert gpu.SolveLDL(Bg, Ag, piv, fl) is None
+        assert fro(Bg.cpu().numpy() - c["X"]) <= 1e-9 * max(fro(c["X"]), 1.0)

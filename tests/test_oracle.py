@@ -376,3 +376,43 @@ def test_oracle_ldl_reference_cases(oracle):
     assert (p < 0).any() and (p > 0).any()
     Z, pz = colmajor(np.zeros((5, 5))), np.zeros(5, np.int64)
     assert oracle.DecomposeLDL(Z, pz, LO) == 1
+
+
+GOLDEN_LDL = os.path.join(os.path.dirname(__file__), "golden", "ldl.npz")
+
+
+def _ldl_cases():
+    z = np.load(GOLDEN_LDL)
+    cases = {}
+    for k in z.files:
+        name, field = k.split("/")
+        cases.setdefault(name, {})[field] = z[k]
+    return cases
+
+
+@pytest.mark.parametrize("name", sorted(_ldl_cases()))
+def test_golden_ldl(oracle, name):
+    """the port reproduces the reference's kernels: pivots exactly, factors and solutions
+    to rounding (the reference's Bunch-Kaufman test tables included)"""
+    c = _ldl_cases()[name]
+    fl = int(c["flags"])
+    A = F(c["A"])
+    n = A.shape[0]
+    if name.startswith("np_"):
+        assert oracle.DecomposeLDLnoPiv(A, fl) == 0
+    else:
+        p = np.zeros(n, np.int64)
+        fn = oracle.DecomposeBK if ("bk" in name) else oracle.DecomposeLDL
+        assert fn(A, p, fl) == 0
+        assert np.array_equal(p, c["piv"])
+    tri = np.tril if fl & LO else np.triu
+    assert rel(tri(A), tri(c["LDL"])) <= 1e-12
+    if "X" in c:
+        X = F(c["B"])
+        if name.startswith("np_"):
+            oracle.SolveLDLnoPiv(X, A, fl)
+        elif "bk" in name:
+            oracle.SolveBK(X, A, c["piv"].copy(), fl)
+        else:
+            oracle.SolveLDL(X, A, c["piv"].copy(), fl)
+        assert rel(X, c["X"]) <= 1e-10
