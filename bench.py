@@ -274,6 +274,63 @@ def qr_leg(mo, dev, n, fp64_peak, nrhs=64, reps=3):
                      "reflector T that DecomposeQRT returns"}
 
 
+def ldl_leg(mo, dev, n=4096, nrhs=64, reps=2):
+    """DecomposeLDLnoPiv / DecomposeLDL / DecomposeBK (ldlnp.go:211, ldl.go:439,
+    ldlbk.go:1114) of an n x n symmetric matrix (uniform, + 2n I for the unpivoted form) and
+    the matching solves of nrhs right-hand sides; CUDA events, residual checked with Mult."""
+    import torch
+    g = torch.Generator(device=dev).manual_seed(11)
+    S = mo.matrix(n, n)
+    S.uniform_(-1.0, 1.0, generator=g)
+    S.copy_(S + S.t())
+    B0 = mo.matrix(n, nrhs)
+    B0.uniform_(-1.0, 1.0, generator=g)
+    A, B = mo.matrix(n, n), mo.matrix(n, nrhs)
+    piv = torch.zeros(n, dtype=torch.int64, device=dev)
+    W = mo.matrix(n, 2)
+    out = {"n": n, "nrhs": nrhs}
+    for kind in ("nopiv", "ldl", "bk"):
+        Sk = S.clone() if kind != "nopiv" else S + 2.0 * n * torch.eye(n, dtype=torch.float64, device=dev)
+        Sc = mo.matrix(n, n)
+        Sc.copy_(Sk)
+        del Sk
+        fts, sts = [], []
+        for it in range(reps + 1):
+            A.copy_(Sc)
+            B.copy_(B0)
+            torch.cuda.synchronize()
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            ev[0].record()
+            if kind == "nopiv":
+                assert mo.DecomposeLDLnoPiv(A, None, LOWER, 0)[1] is None
+            elif kind == "ldl":
+                assert mo.DecomposeLDL(A, None, piv, LOWER, 0)[1] is None
+            else:
+                assert mo.DecomposeBK(A, W, piv, LOWER, 0)[1] is None
+            ev[1].record()
+            if kind == "nopiv":
+                assert mo.SolveLDLnoPiv(B, A, LOWER) is None
+            elif kind == "ldl":
+                assert mo.SolveLDL(B, A, piv, LOWER) is None
+            else:
+                assert mo.SolveBK(B, A, piv, LOWER) is None
+            ev[2].record()
+            torch.cuda.synchronize()
+            if it:
+                fts.append(ev[0].elapsed_time(ev[1]))
+                sts.append(ev[1].elapsed_time(ev[2]))
+        R = B0.clone()
+        assert mo.Mult(R, Sc, B, -1.0, 1.0, 0) is None
+        berr = float(torch.linalg.norm(R) / (torch.linalg.norm(Sc) * torch.linalg.norm(B)
+                                             + torch.linalg.norm(B0)))
+        out[kind] = {"factor_ms": min(fts), "solve_ms": min(sts),
+                     "factor_tflops": n ** 3 / 3.0 / (min(fts) * 1e-3) / 1e12, "solve_berr": berr}
+        if kind == "bk":
+            out[kind]["two_by_two_blocks"] = int((piv < 0).sum().item()) // 2
+        del Sc
+    return out
+
+
 def mixed_leg(mo, n, nrhs, kappas, precs, dev, reps=2):
     """Mixed-precision + FP64-refined Cholesky solve against the FP64 path on the same
     A = Q diag(s) Q^T (seed 6) and B ~ N(0,1) (seed 7): time, iterations, backward and
@@ -1016,6 +1073,8 @@ def main():
                     "identical": bool(d.size == 0), "differing": int(d.size),
                     "reference": "tests/golden/n16384.npz (oracle/_ref DecomposeLU, nb=64)"}
         del L0, Lb0, LA, LB
+        torch.cuda.empty_cache()
+        extras["ldl"] = ldl_leg(mo, dev)
         torch.cuda.empty_cache()
         extras["qr"] = {}
         for nq in sorted({min(8192, n), n}):
