@@ -34,6 +34,15 @@ def test_strerror_matches_go_errors():
     assert L.mo_strerror(-3) == b"pivot array < min(A.Rows(),A.Cols())"
     assert L.mo_strerror(-4) == b"C not a square matrix"
     assert L.mo_strerror(-5) == b"A, B size mismatch"
+    # QR (qrwy.go:526, qrwym.go:652, :656, qrwy.go:550) and LDL^T (ldlnp.go:224, ldl.go:62,
+    # ldlbk.go:1121)
+    assert L.mo_strerror(-13) == b"work space too small"
+    assert L.mo_strerror(-14) == b"workspace not defined"
+    assert L.mo_strerror(-15) == b"C*Q: C.Cols != A.Rows"
+    assert L.mo_strerror(-16) == b"reflector matrix T too small"
+    assert L.mo_strerror(-17) == b"No workspace for blocking invocation"
+    assert L.mo_strerror(-18) == b"zero value on diagonal"
+    assert L.mo_strerror(-19) == b"Workspace too small"
 
 
 def test_null_context_is_rejected_without_gpu():
