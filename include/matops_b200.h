@@ -1,8 +1,9 @@
 /*
  * matops_b200.h -- C ABI of the B200 (sm_100a) implementation of hrautila/matops's
- * level-3 hot path: GEMM, SYRK and TRSM, and the blocked Cholesky / LU factorizations and
- * solves built on them, all in IEEE double precision on device-resident column-major
- * matrices.
+ * level-3 hot path: GEMM, SYRK and TRSM, the rest of the level-3 surface, and the Cholesky /
+ * LU / QR (compact WY) / symmetric indefinite LDL^T factorizations and solves built on
+ * them, all in IEEE double precision on device-resident column-major matrices; plus a
+ * mixed-precision Cholesky solve, batched small systems and the Cholesky adjoints.
  *
  * Every operation entry point mirrors one exported Go function of the reference package
  * (file:line in its source tree) with the same argument meaning, flag bits and error
