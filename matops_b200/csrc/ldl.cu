@@ -19,7 +19,7 @@
 //
 // Solves: SolveLDLnoPiv / SolveLDL as the reference composes them (row interchanges, two
 // unit-triangular solves on the TRSM engine, the diagonal scaling); SolveBK by a
-// cooperative kernel that follows ldlbks.go's two sweeps (interchange, rank-1 / rank-2
+// kernel that follows ldlbks.go's two sweeps (interchange, rank-1 / rank-2
 // update of the rows of B below, 1 x 1 / 2 x 2 diagonal solve; then the transposed sweep
 // back up), on the reversed problem for UPPER.
 #include <algorithm>
@@ -383,13 +383,29 @@ __global__ void __launch_bounds__(kLdlThreads, 1)
   flush();
 }
 
-// ldlbks.go:15-156 (unblkSolveBKLower, both sweeps) for the columns of B, one warp per
+constexpr int kBkSolveThreads = 256;
+
+// sum over the CTA in a fixed order (every thread gets the result)
+__device__ double bk_block_sum(double v, double *red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+#pragma unroll
+  for (int w = 0; w < kBkSolveThreads / 32; ++w) t += red[w];
+  return t;
+}
+
+// ldlbks.go:15-156 (unblkSolveBKLower, both sweeps) for the columns of B, one CTA per
 // column (the columns are independent; no grid-wide synchronization), on the working
 // (reversed for UPPER) indices.  ipiv holds the reference's values at ORIGINAL positions.
-__global__ void __launch_bounds__(128) ldl_bk_solve_kernel(SymView A, double *B, int64_t ldb,
-                                                           int nrhs, const int64_t *ipiv) {
-  const int n = A.n, rev = A.rev, lane = threadIdx.x & 31;
-  const int c = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+__global__ void __launch_bounds__(kBkSolveThreads) ldl_bk_solve_kernel(SymView A, double *B,
+                                                                       int64_t ldb, int nrhs,
+                                                                       const int64_t *ipiv) {
+  __shared__ double red[2][kBkSolveThreads / 32];
+  const int n = A.n, rev = A.rev, tid = threadIdx.x, c = blockIdx.x;
   if (c >= nrhs) return;
   double *bc = B + (int64_t)c * ldb;
   auto brow = [&](int i) -> double * { return bc + (rev ? n - 1 - i : i); };
@@ -401,12 +417,12 @@ __global__ void __launch_bounds__(128) ldl_bk_solve_kernel(SymView A, double *B,
     return -((rev ? (int64_t)n - 1 - q : q) + 1);
   };
   auto swap_rows = [&](int x, int y) {
-    if (lane == 0 && x != y && x >= 0 && x < n && y >= 0 && y < n) {
+    if (tid == 0 && x != y && x >= 0 && x < n && y >= 0 && y < n) {
       const double t = *brow(x);
       *brow(x) = *brow(y);
       *brow(y) = t;
     }
-    __syncwarp();
+    __syncthreads();
   };
   // sweep 1: D^-1 L^-1 with the interchanges of each step (ldlbks.go:72-118)
   for (int k = 0; k < n;) {
@@ -414,10 +430,11 @@ __global__ void __launch_bounds__(128) ldl_bk_solve_kernel(SymView A, double *B,
     if (pk > 0) {
       if (pk != k + 1) swap_rows(k, (int)pk - 1);
       const double bk = *brow(k);
-      for (int i = k + 1 + lane; i < n; i += 32) *brow(i) = __dadd_rn(*brow(i), -(*A.at(i, k) * bk));
-      __syncwarp();
-      if (lane == 0) *brow(k) = bk / *A.at(k, k);
-      __syncwarp();
+      for (int i = k + 1 + tid; i < n; i += kBkSolveThreads)
+        *brow(i) = __dadd_rn(*brow(i), -(*A.at(i, k) * bk));
+      __syncthreads();
+      if (tid == 0) *brow(k) = bk / *A.at(k, k);
+      __syncthreads();
       k += 1;
     } else {
       if (k + 1 >= n) return;  // a 2 x 2 block cannot start at the last row
@@ -427,14 +444,14 @@ __global__ void __launch_bounds__(128) ldl_bk_solve_kernel(SymView A, double *B,
       double scale = __dadd_rn(__dmul_rn(apb, dpb), -1.0);
       scale *= b;
       const double s0 = *brow(k), s1 = *brow(k + 1);
-      for (int i = k + 2 + lane; i < n; i += 32)
+      for (int i = k + 2 + tid; i < n; i += kBkSolveThreads)
         *brow(i) = __dadd_rn(*brow(i), -__dadd_rn(__dmul_rn(*A.at(i, k), s0), __dmul_rn(*A.at(i, k + 1), s1)));
-      __syncwarp();
-      if (lane == 0) {
+      __syncthreads();
+      if (tid == 0) {
         *brow(k) = __dadd_rn(__dmul_rn(dpb, s0), -s1) / scale;
         *brow(k + 1) = __dadd_rn(__dmul_rn(apb, s1), -s0) / scale;
       }
-      __syncwarp();
+      __syncthreads();
       k += 2;
     }
   }
@@ -444,32 +461,29 @@ __global__ void __launch_bounds__(128) ldl_bk_solve_kernel(SymView A, double *B,
     if (pl > 0) {
       const int k = nc - 1;
       double acc = 0.0;
-      for (int i = k + 1 + lane; i < n; i += 32) acc = __dadd_rn(acc, __dmul_rn(*A.at(i, k), *brow(i)));
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-      if (lane == 0) *brow(k) = __dadd_rn(*brow(k), -acc);
-      __syncwarp();
+      for (int i = k + 1 + tid; i < n; i += kBkSolveThreads)
+        acc = __dadd_rn(acc, __dmul_rn(*A.at(i, k), *brow(i)));
+      acc = bk_block_sum(acc, red[0]);
+      if (tid == 0) *brow(k) = __dadd_rn(*brow(k), -acc);
+      __syncthreads();
       if (pl != nc) swap_rows(k, (int)pl - 1);
       nc -= 1;
     } else {
       const int k = nc - 2;
       if (k < 0) return;
       double a0 = 0.0, a1 = 0.0;
-      for (int i = k + 2 + lane; i < n; i += 32) {
+      for (int i = k + 2 + tid; i < n; i += kBkSolveThreads) {
         const double bi = *brow(i);
         a0 = __dadd_rn(a0, __dmul_rn(*A.at(i, k), bi));
         a1 = __dadd_rn(a1, __dmul_rn(*A.at(i, k + 1), bi));
       }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
-        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
-      }
-      if (lane == 0) {
+      a0 = bk_block_sum(a0, red[0]);
+      a1 = bk_block_sum(a1, red[1]);
+      if (tid == 0) {
         *brow(k) = __dadd_rn(*brow(k), -a0);
         *brow(k + 1) = __dadd_rn(*brow(k + 1), -a1);
       }
-      __syncwarp();
+      __syncthreads();
       if (piv(k) != -nc) swap_rows(k + 1, (int)(-piv(k)) - 1);
       nc -= 2;
     }
@@ -544,9 +558,7 @@ int ldl_factor(mo_ctx *ctx, View A, int64_t *ipiv, int mode, bool upper) {
 int ldl_bk_solve(mo_ctx *ctx, View B, View A, const int64_t *ipiv, bool upper) {
   if (B.rows == 0 || B.cols == 0) return MO_OK;
   SymView v{A.d, A.ld, A.rows, upper ? 1 : 0};
-  const int warps = 4;
-  ldl_bk_solve_kernel<<<(B.cols + warps - 1) / warps, 32 * warps, 0, ctx->stream>>>(v, B.d, B.ld,
-                                                                                    B.cols, ipiv);
+  ldl_bk_solve_kernel<<<B.cols, kBkSolveThreads, 0, ctx->stream>>>(v, B.d, B.ld, B.cols, ipiv);
   MO_CUDA_TRY(cudaGetLastError());
   return MO_OK;
 }
