@@ -520,14 +520,16 @@ __global__ void ldl_solve_diag_kernel(double *B, int64_t ldb, int n, int nrhs, c
 
 // DecomposeLDLnoPiv / DecomposeLDL / DecomposeBK on the device: one cooperative sweep.
 // Returns MO_OK, or k + 1 for DecomposeLDL's zero pivot at step k (synchronizes then).
-int ldl_factor(mo_ctx *ctx, View A, int64_t *ipiv, int mode, bool upper) {
+size_t ldl_scratch_bytes(int sms) { return (size_t)2 * sms * (sizeof(double) + sizeof(int)) + 512; }
+
+int ldl_factor(mo_ctx *ctx, View A, int64_t *ipiv, int mode, bool upper, char *scratch = nullptr) {
   const int n = A.rows;
   if (n == 0) return MO_OK;
   const int grid = std::max(1, std::min(ctx->sms, n / 32));
-  const size_t bytes = (size_t)2 * grid * (sizeof(double) + sizeof(int)) + 512;
-  char *ws = nullptr;
-  int rc = workspace(ctx, bytes, (void **)&ws);
-  if (rc) return rc;
+  const size_t bytes = ldl_scratch_bytes(grid);
+  char *ws = scratch;
+  int rc = MO_OK;
+  if (!ws && (rc = workspace(ctx, bytes, (void **)&ws))) return rc;
   LdlScratch sc;
   sc.val = (double *)ws;
   sc.idx = (int *)(ws + (size_t)2 * grid * sizeof(double));
@@ -586,6 +588,78 @@ int ldl_solve(mo_ctx *ctx, View B, View A, const int64_t *ipiv, bool upper) {
   return pivots(upper);
 }
 
+namespace {
+
+// X(:, c) *= 1 / d_c (SolveDiag RIGHT, diag.go:97-102) or, with W, W(:, c) = X(:, c) d_c
+// (MultDiag RIGHT, diag.go:38-44); d the diagonal of the factored block (stride ldd + 1)
+__global__ void ldl_cols_kernel(double *X, int64_t ldx, int rows, const double *D, int64_t ldd,
+                                double *W, int64_t ldw) {
+  const int i = blockIdx.x * 256 + threadIdx.x, c = blockIdx.y;
+  if (i >= rows) return;
+  const double d = D[c + (int64_t)c * ldd];
+  if (W)
+    W[i + (int64_t)c * ldw] = X[i + (int64_t)c * ldx] * d;
+  else
+    X[i + (int64_t)c * ldx] *= 1.0 / d;
+}
+
+}  // namespace
+
+// DecomposeLDLnoPiv blocked as ldlnp.go:104-205 does it with nb = 128: the diagonal block by
+// the sweep, the block column by a unit-triangular solve and D^-1, the rest of the matrix
+// by one engine update in its triangle mode (UpdateTrm's A22 -= L21 (L21 D)^T)
+int ldl_nopiv_blocked(mo_ctx *ctx, View A, bool upper) {
+  const int n = A.rows, NB = 128;
+  const size_t wbytes = ((size_t)n * NB * 8 + 255) & ~(size_t)255;
+  const size_t ibytes = (size_t)NB * NB * 8;
+  char *ws = nullptr;
+  int rc = workspace(ctx, wbytes + ibytes + ldl_scratch_bytes(ctx->sms), (void **)&ws);
+  if (rc) return rc;
+  double *W = (double *)ws, *inv = (double *)(ws + wbytes);
+  char *scr = ws + wbytes + ibytes;
+  auto cols = [&](View X, const View &D, double *w) -> int {
+    if (X.rows == 0 || X.cols == 0) return MO_OK;
+    ldl_cols_kernel<<<dim3((X.rows + 255) / 256, X.cols), 256, 0, ctx->stream>>>(
+        X.d, X.ld, X.rows, D.d, D.ld, w, X.rows);
+    MO_CUDA_TRY(cudaGetLastError());
+    return MO_OK;
+  };
+  GemmOpts o;
+  o.mode = upper ? kSyrkUpper : kSyrkLower;
+  if (!upper) {
+    for (int kb = 0; kb < n; kb += NB) {
+      const int bo = std::min(NB, n - kb), rest = n - kb - bo;
+      const View A11 = A.sub(kb, kb, bo, bo);
+      if ((rc = ldl_factor(ctx, A11, nullptr, kLdlNoPiv, false, scr))) return rc;
+      if (rest == 0) break;
+      const View A21 = A.sub(kb + bo, kb, rest, bo);
+      if ((rc = trsm_with_scratch(ctx, A21, A11, MO_RIGHT | MO_LOWER | MO_UNIT | MO_TRANSA, 1.0,
+                                  inv)))
+        return rc;
+      if ((rc = cols(A21, A11, nullptr)) || (rc = cols(A21, A11, W))) return rc;
+      if ((rc = gemm_ex(ctx, A.sub(kb + bo, kb + bo, rest, rest), A21, false,
+                        View{W, rest, bo, rest}, true, -1.0, 1.0, o)))
+        return rc;
+    }
+  } else {
+    for (int e = n; e > 0; e -= NB) {
+      const int bo = std::min(NB, e), s0 = e - bo;
+      const View A11 = A.sub(s0, s0, bo, bo);
+      if ((rc = ldl_factor(ctx, A11, nullptr, kLdlNoPiv, true, scr))) return rc;
+      if (s0 == 0) break;
+      const View A01 = A.sub(0, s0, s0, bo);
+      if ((rc = trsm_with_scratch(ctx, A01, A11, MO_RIGHT | MO_UPPER | MO_UNIT | MO_TRANSA, 1.0,
+                                  inv)))
+        return rc;
+      if ((rc = cols(A01, A11, nullptr)) || (rc = cols(A01, A11, W))) return rc;
+      if ((rc = gemm_ex(ctx, A.sub(0, 0, s0, s0), A01, false, View{W, s0, bo, s0}, true, -1.0,
+                        1.0, o)))
+        return rc;
+    }
+  }
+  return MO_OK;
+}
+
 }  // namespace mo
 
 using mo::View;
@@ -612,7 +686,8 @@ int mo_decompose_ldl_nopiv(mo_ctx *ctx, mo_matrix Am, mo_matrix Wm, int flags, i
   if (!(A.cols < nb || nb == 0) && Wm.data == nullptr) return MO_ELDLWORK;
   bool upper;
   ldl_tri(flags, &upper);
-  return mo::ldl_factor(ctx, A, nullptr, 0, upper);
+  // one sweep for small orders, the blocked form (ldlnp.go:104) above
+  return A.rows > 256 ? mo::ldl_nopiv_blocked(ctx, A, upper) : mo::ldl_factor(ctx, A, nullptr, 0, upper);
 }
 
 // ldlnp.go:251-266
