@@ -18,10 +18,11 @@
 //     tau, beta and update row.  CTA 0 builds the panel's 32 x 32 T block.  The kernel also
 //     writes the reflectors as an explicit unit lower trapezoid Y (zeros above) and the T
 //     block with zeros below its diagonal, so that every later product is a plain GEMM;
-//   * after each panel: T's rows above the panel, -T(0:kp,0:kp) (Y_prev^T Y_p) T_p, and the
-//     rest of the 128-column block updated with the panel's reflector (three GEMMs each);
-//   * after each block: the columns to its right take Q_b^T in three GEMMs with K = 128
-//     (W = C^T Y_b, W = W T_b, C -= Y_b W^T).
+//   * after each panel: the rest of the 128-column block takes the panel's reflectors
+//     (W = C^T Y_p by a split-K kernel pair, W = W T_p, C -= Y_p W^T);
+//   * after each block: its T (the four panel T blocks joined through Y_b^T Y_b by one CTA),
+//     T's rows above it, -T(0:kb,0:kb) (Y(:,0:kb)^T Y_b) T_b, and the columns to its right
+//     take Q_b^T in three products with K = 128 (W = C^T Y_b, W = W T_b, C -= Y_b W^T).
 // The products run on the FP64 DMMA engine.  T is kept dense (zeros below the diagonal)
 // in workspace and copied to the caller's upper triangle at the end.
 //
