@@ -1442,6 +1442,72 @@ void or_solve_bk_fm(fm B, fm A, const int64_t *ipiv, int flags) {
   }
 }
 
+/* house.go:152-183 (applyHHTo2x1, side RIGHT) with the caller's w1: [a1 A2] = [a1 A2] H,
+ * w1 = tau (a1 + A2 v), a1 -= w1, A2 -= w1 v^T */
+static void applyHHTo2x1Right(double tval, fm v, fm a1, fm A2, fm w1) {
+  if (tval == 0.0) return;
+  const int n = a1.r * a1.c;
+  for (int k = 0; k < n; k++) *vel(w1, k) = *vel(a1, k);
+  MVMult(w1, A2, v, 1.0, 1.0, MTX_NOTRANS);
+  Scale(w1, tval);
+  for (int k = 0; k < n; k++) *vel(a1, k) -= *vel(w1, k);
+  MVRankUpdate(A2, w1, v, -1.0);
+}
+
+/* qrwym.go:28-106 (unblockedMultQLeft) and :114-190 (unblockedMultQRight): one reflector at a
+ * time, forward for Q^T C and C Q, backward for Q C and C Q^T; tau(j) is the j-th entry */
+static void unblockedMultQ(fm C, fm A, fm tau, int flags) {
+  const int k = A.r < A.c ? A.r : A.c;
+  const int right = (flags & MTX_RIGHT) != 0, trans = (flags & MTX_TRANS) != 0;
+  const int forward = right ? !trans : trans;
+  const int wl = right ? C.r : C.c;
+  double *wb = (double *)calloc((size_t)(wl > 0 ? wl : 1), sizeof(double));
+  for (int t = 0; t < k && t < tau.r * tau.c; t++) {
+    const int j = forward ? t : k - 1 - t;
+    const double tj = *vel(tau, j);
+    fm v = sub(A, j + 1, j, A.r - j - 1, 1);
+    if (!right) {
+      double tv = tj;
+      applyHouseholderLeft((fm){&tv, 1, 1, 1}, v, sub(C, j, 0, 1, C.c),
+                           sub(C, j + 1, 0, C.r - j - 1, C.c));
+    } else {
+      fm w = {wb, C.r, 1, C.r > 0 ? C.r : 1};
+      applyHHTo2x1Right(tj, v, sub(C, 0, j, C.r, 1), sub(C, 0, j + 1, C.r, C.c - j - 1), w);
+    }
+  }
+  free(wb);
+}
+
+/* qrwym.go:573-630 (MultQ): the unblocked path for any nb (the blocked one builds its T
+ * blocks with the per-68-row-block GEMV of BuildT); W is checked as the reference checks it */
+int or_mult_q_fm(fm C, fm A, fm tau, fm W, int flags, int nb) {
+  if (nb != 0 && W.d == NULL) return OR_ENOWORK;
+  if (flags & MTX_RIGHT) {
+    if (C.c != A.r) return OR_ECQSIZE;
+    if (nb != 0 && (W.c < nb || W.r < C.r)) return OR_EWORKSMALL;
+  } else if (nb != 0 && (W.c < nb || W.r < C.c)) {
+    return OR_EWORKSMALL;
+  }
+  unblockedMultQ(C, A, tau, flags);
+  return OR_OK;
+}
+
+/* qrwym.go:717-760 (SolveQR); with MTX_TRANS the minimum-norm solution as SolveQRT computes
+ * it (the reference rebinds B to an empty view there, qrwym.go:735) */
+int or_solve_qr_fm(fm B, fm A, fm tau, fm W, int flags, int nb) {
+  fm R = sub(A, 0, 0, A.c, A.c), BT = sub(B, 0, 0, A.c, B.c);
+  if (flags & MTX_TRANS) {
+    or_solve_trm_fm(BT, R, 1.0, MTX_LEFT | MTX_UPPER | MTX_TRANSA);
+    fm BB = sub(B, A.c, 0, B.r - A.c, B.c);
+    for (int j = 0; j < BB.c; j++)
+      for (int i = 0; i < BB.r; i++) BB.d[i + (intptr_t)j * BB.ld] = 0.0;
+    return or_mult_q_fm(B, A, tau, W, MTX_LEFT, nb);
+  }
+  int rc = or_mult_q_fm(B, A, tau, W, MTX_LEFT | MTX_TRANS, nb);
+  if (rc) return rc;
+  return or_solve_trm_fm(BT, R, 1.0, MTX_LEFT | MTX_UPPER);
+}
+
 /* ---------------- flat C entry points for the ctypes harness ---------------- */
 
 #define FM(p, r, c, ld) ((fm){(p), (r), (c), (ld)})
@@ -1571,4 +1637,14 @@ int or_decompose_bk(double *A, int ar, int ac, int lda, int64_t *piv, int npiv, 
 void or_solve_bk(double *B, int br, int bc, int ldb, double *A, int ar, int ac, int lda,
                  const int64_t *piv, int flags) {
   or_solve_bk_fm(FM(B, br, bc, ldb), FM(A, ar, ac, lda), piv, flags);
+}
+int or_mult_q(double *C, int cr, int cc, int ldc, double *A, int ar, int ac, int lda, double *tau,
+              int taur, double *W, int wr, int wc, int ldw, int flags, int nb) {
+  return or_mult_q_fm(FM(C, cr, cc, ldc), FM(A, ar, ac, lda), FM(tau, taur, 1, taur > 0 ? taur : 1),
+                      FM(W, wr, wc, ldw), flags, nb);
+}
+int or_solve_qr(double *B, int br, int bc, int ldb, double *A, int ar, int ac, int lda, double *tau,
+                int taur, double *W, int wr, int wc, int ldw, int flags, int nb) {
+  return or_solve_qr_fm(FM(B, br, bc, ldb), FM(A, ar, ac, lda), FM(tau, taur, 1, taur > 0 ? taur : 1),
+                        FM(W, wr, wc, ldw), flags, nb);
 }

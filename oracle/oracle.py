@@ -103,6 +103,8 @@ class Oracle:
         L.or_decompose_bk.argtypes = M + [p, i, i]
         L.or_solve_bk.argtypes = M + M + [p, i]
         L.or_solve_bk.restype = None
+        L.or_mult_q.argtypes = M + M + [p, i] + [p, i, i, i] + [i, i]
+        L.or_solve_qr.argtypes = M + M + [p, i] + [p, i, i, i] + [i, i]
         L.or_build_q.argtypes = M + [p, i] + [p, i, i, i] + [i]
         L.or_build_qt.argtypes = M + M + M + [i]
 
@@ -180,6 +182,18 @@ class Oracle:
     def SolveQRT(self, B, A, T, W, flags, nb):
         """qrwym.go:784: least squares min ||A X - B|| or (MO_TRANS) min-norm A^T X = B"""
         return self.lib.or_solve_qrt(*view(B), *view(A), *view(T), *self._wview(W), flags, nb)
+
+    def MultQ(self, C, A, tau: np.ndarray, W, flags, nb):
+        """qrwym.go:573 (the unblocked path): C = Q C, Q^T C, C Q, C Q^T from A and tau"""
+        assert tau.dtype == np.float64 and tau.flags.c_contiguous
+        return self.lib.or_mult_q(*view(C), *view(A), ctypes.c_void_p(tau.ctypes.data), len(tau),
+                                  *self._wview(W), flags, nb)
+
+    def SolveQR(self, B, A, tau: np.ndarray, W, flags, nb):
+        """qrwym.go:717: least squares (or, TRANS, minimum norm) with Q from tau"""
+        assert tau.dtype == np.float64 and tau.flags.c_contiguous
+        return self.lib.or_solve_qr(*view(B), *view(A), ctypes.c_void_p(tau.ctypes.data), len(tau),
+                                    *self._wview(W), flags, nb)
 
     def BuildQ(self, A, tau: np.ndarray, W, nb):
         """qrwyk.go:232: A := the first A.cols columns of Q = H(0)...H(k-1) (DORGQR)"""

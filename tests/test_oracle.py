@@ -416,3 +416,27 @@ def test_golden_ldl(oracle, name):
         else:
             oracle.SolveLDL(X, A, c["piv"].copy(), fl)
         assert rel(X, c["X"]) <= 1e-10
+
+
+@pytest.mark.parametrize("flags", [LEFT, LEFT | 0x80, RIGHT, RIGHT | 0x80])
+def test_port_vs_ref_mult_q(oracle, ref_oracle, flags):
+    """MultQ's unblocked path (qrwym.go:28-190): port and reference kernels agree and give
+    the product of the reflectors"""
+    rng = np.random.default_rng(77)
+    m, n = 150, 90
+    A = colmajor(rng.uniform(-1, 1, (m, n)))
+    QR, tau = colmajor(A), np.zeros(n)
+    assert oracle.DecomposeQR(QR, tau, None, 0) == 0
+    Y = np.tril(QR, -1) + np.eye(m, n)
+    Q = np.eye(m)
+    for j in range(n):
+        Q = Q - tau[j] * np.outer(Q @ Y[:, j], Y[:, j])
+    C0 = rng.uniform(-1, 1, (5, m) if flags & RIGHT else (m, 5))
+    outs = []
+    for o in (oracle, ref_oracle):
+        C = colmajor(C0)
+        assert o.MultQ(C, QR, tau.copy(), None, flags, 0) == 0
+        outs.append(C)
+    exp = ((C0 @ Q.T if flags & 0x80 else C0 @ Q) if flags & RIGHT
+           else (Q.T @ C0 if flags & 0x80 else Q @ C0))
+    assert rel(outs[0], exp) <= 1e-13 and rel(outs[1], outs[0]) <= 1e-13

@@ -173,6 +173,33 @@ def test_solve_qrt(gpu, ref, lapack, rng, m, n, p, flags):
         assert fro(A0.T @ (A0 @ X - B0)) <= 64 * m * EPS * cond * fro(A0) * fro(B0)
 
 
+@pytest.mark.parametrize("m,n", [(90, 60), (700, 450)])
+@pytest.mark.parametrize("flags", [LEFT, LEFT | TRANS, RIGHT, RIGHT | TRANS])
+def test_mult_q_vs_reference(gpu, ref, rng, m, n, flags):
+    """MultQ (tau form) against the reference kernels' unblocked MultQ (qrwym.go:28-190, no
+    GEMV with beta != 1 on that path), the same reflectors on both sides"""
+    import torch
+    A0 = colmajor(rng.uniform(-1, 1, (m, n)))
+    Ag = dev(gpu, A0)
+    tau = torch.zeros(n, dtype=torch.float64, device="cuda")
+    assert gpu.DecomposeQR(Ag, tau, None, 0)[1] is None
+    Ah, th = host(Ag), tau.cpu().numpy().copy()
+    p = 21
+    C0 = colmajor(rng.uniform(-1, 1, (p, m) if flags & RIGHT else (m, p)))
+    Cg = dev(gpu, C0)
+    assert gpu.MultQ(Cg, Ag, tau, None, flags, 0) is None
+    Cr = C0.copy(order="F")
+    assert ref.MultQ(Cr, Ah, th, None, flags, 0) == 0
+    assert fro(host(Cg) - Cr) <= 16 * m * EPS * fro(C0)
+    # SolveQR least squares on the same factorization
+    B0 = colmajor(A0 @ rng.uniform(-1, 1, (n, 3)) + 1e-3 * rng.uniform(-1, 1, (m, 3)))
+    Bg = dev(gpu, B0)
+    assert gpu.SolveQR(Bg, Ag, tau, None, 0, 0) is None
+    Br = B0.copy(order="F")
+    assert ref.SolveQR(Br, Ah, th, None, 0, 0) == 0
+    assert fro(host(Bg) - Br) <= 64 * m * EPS * np.linalg.cond(A0) * max(fro(Br), 1.0)
+
+
 @pytest.mark.parametrize("flags", [LEFT | TRANS, RIGHT])
 def test_mult_q_and_solve_qr(gpu, ref, lapack, rng, flags):
     import torch
