@@ -514,18 +514,13 @@ int t_columns(mo_ctx *ctx, int k, int kp, int bp, View Zsrc, QrWork &q) {
 
 // C = alpha * A^T B + beta * C: split-K kernels when C is small and K long, else the
 // engine (its stream-K scratch doubles as the partial-tile buffer: same stream, in order)
-int tn_product(mo_ctx *ctx, View C, View A, View B, double alpha, double beta,
-               double *part = nullptr) {
+int tn_product(mo_ctx *ctx, View C, View A, View B, double alpha, double beta) {
   const int M = C.rows, N = C.cols, K = A.rows;
   if (M <= 0 || N <= 0) return MO_OK;
   const int tiles = ((M + kTnTile - 1) / kTnTile) * ((N + kTnTile - 1) / kTnTile);
   const size_t cap = gemm_partial_bytes(ctx->sms) / sizeof(double) / (kTnTile * kTnTile);
-  if (K < 1024 || tiles > 16 || K <= 0) {
-    GemmOpts o;
-    o.stream_k = part == nullptr;  // a caller's buffer: the product may overlap another
-    return gemm_ex(ctx, C, A, true, B, false, alpha, beta, o);
-  }
-  if (!part) part = ctx->sk_partial;
+  if (K < 1024 || tiles > 16 || K <= 0) return gemm(ctx, C, A, true, B, false, alpha, beta);
+  double *part = ctx->sk_partial;
   // chunks of at least 128 rows, about two CTAs per SM, within the partial buffer
   int chunks = std::max(1, std::min<int>(K / 128, (2 * ctx->sms + tiles - 1) / tiles));
   chunks = std::min<int>(chunks, (int)(cap / tiles));
@@ -545,16 +540,13 @@ int tn_product(mo_ctx *ctx, View C, View A, View B, double alpha, double beta,
 
 // C (rows s.. of A's columns right of a block) = Q_b^T C for the block's reflectors:
 // W = C^T Y_b, W = W T_b, C -= Y_b W^T (qrwy.go:266-303 with transpose)
-int apply_left_t(mo_ctx *ctx, View C, const View &Yb, const View &Tb, QrWork &q,
-                 int max_ctas = 0) {
+int apply_left_t(mo_ctx *ctx, View C, const View &Yb, const View &Tb, QrWork &q) {
   const int nc = C.cols, b = Yb.cols;
   if (nc <= 0 || b <= 0) return MO_OK;
   const View W{q.W, nc, b, nc}, W2{q.W2, nc, b, nc};
-  GemmOpts o;
-  o.max_ctas = max_ctas;
   int rc = tn_product(ctx, W, C, Yb, 1.0, 0.0);
-  if (!rc) rc = gemm_ex(ctx, W2, W, false, Tb, false, 1.0, 0.0, o);
-  if (!rc) rc = gemm_ex(ctx, C, Yb, false, W2, true, -1.0, 1.0, o);
+  if (!rc) rc = gemm(ctx, W2, W, false, Tb, false, 1.0, 0.0);
+  if (!rc) rc = gemm(ctx, C, Yb, false, W2, true, -1.0, 1.0);
   return rc;
 }
 
